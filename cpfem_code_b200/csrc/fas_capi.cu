@@ -1,0 +1,1157 @@
+// fas_capi.cu -- host side of libfasgpu.so: the handle, one-time set-up of
+// the device layout, state transfer, the NRITER / FACSLS orchestration and
+// the exported C ABI of include/fasolt_gpu.h.
+//
+// Everything runs on one CUDA stream per handle.  Host synchronisation
+// happens once per global Newton iteration (to read the error key and the
+// norms that decide the loop) and once per chunk of SOR sweeps (to read the
+// convergence flag); nothing else waits for the device.
+
+#include "../../include/fasolt_gpu.h"
+#include "fas_kernels.cuh"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+using namespace fasdev;
+
+namespace {
+
+template <class T> struct DVec {
+    T *p = nullptr;
+    size_t n = 0;
+    DVec() = default;
+    DVec(const DVec &) = delete;
+    DVec &operator=(const DVec &) = delete;
+    ~DVec() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t alloc(size_t m)
+    {
+        release();
+        n = m;
+        if (!m) return cudaSuccess;
+        cudaError_t e = cudaMalloc((void **)&p, m * sizeof(T));
+        if (e != cudaSuccess) { p = nullptr; n = 0; }
+        return e;
+    }
+    cudaError_t zero(cudaStream_t s) { return n ? cudaMemsetAsync(p, 0, n * sizeof(T), s) : cudaSuccess; }
+    cudaError_t put(const T *h, size_t m, cudaStream_t s)
+    {
+        return m ? cudaMemcpyAsync(p, h, m * sizeof(T), cudaMemcpyHostToDevice, s) : cudaSuccess;
+    }
+};
+
+inline double rdv(const void *p, int rb, size_t i)
+{
+    return rb == 4 ? (double)((const float *)p)[i] : ((const double *)p)[i];
+}
+
+inline unsigned nblocks(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+struct HostCtl {                 // pinned mirror of the small device results
+    unsigned long long ekey[2];
+    int flags[4];                // 0 bad_bc, 1 tflag, 2 overflow, 3 nev
+    SorCtl sor;
+    double sums[8];
+};
+
+}  // namespace
+
+struct fas_handle {
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t mode = 0;
+    int nlmnt = 0, nnod = 0, ngps = 0;
+    int maxns = 0, nsvld = 0, nsv = 0, ns_tmpl = 12;
+    bool point_mode = false, have_state = false;
+    int last_mat = 1;            // mat_code the last element leaves behind
+    // host copies used by the set-up
+    std::vector<int> h_ln, h_gpe, h_le, h_ib, h_gp_iel, h_colour;
+    std::vector<int> ne_ptr, ne_list, ne_locl;   // node -> elements CSR
+    std::vector<double> h_tiem;
+    int ninc1 = 0, nxs = 0, nfs = 0;
+    // device mesh
+    DVec<int> ln, gpe, le, ib, gp_iel, ne_elem, ne_loc, ne_cnt;
+    // materials / control
+    DVec<double> m_e, m_ssang, m_ab, m_an, m_ampar, m_sm;
+    DevMat M{};
+    DevCtrl C{};
+    DVec<double> xspec, fspec;
+    // nodal vectors
+    DVec<double> x, dx, fc, ddx, rhs;
+    // Gauss-point state (SoA)
+    DVec<double> eps, dep, st, ep, ds, de, rt, dr, sv, dsv, srate, cumslip, erepmd, ops, chi_pts;
+    DVec<int> timestwinned, twinsys, cp_iters;
+    // element records
+    DVec<double> rec;
+    // block layout
+    int ncol = 0;
+    std::vector<int> col_start;
+    std::vector<double> col_bytes;
+    DVec<int> perm, rowof, nslot, bcol;
+    DVec<unsigned> bloc;
+    DVec<double> blk;
+    // reductions and control
+    std::vector<int> sor_boff, sor_nblk;
+    int sor_nblk_tot = 0, nr_nblk = 0;
+    DVec<double> part_sor, part_nr, sums;
+    DVec<unsigned long long> ekey;
+    DVec<int> flags;
+    DVec<SorCtl> sorctl;
+    HostCtl *hc = nullptr;
+    // staging for state transfer
+    DVec<unsigned char> stage;
+    DVec<TwinEv> events;
+    // profiling
+    bool prof = false;
+    fas_profile P{};
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<std::pair<cudaEvent_t, cudaEvent_t>, double *>> pending;
+    cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;
+    double asm_bytes = 0.0;      // algorithmic bytes of one assembly launch
+    int64_t launches = 0;
+
+    ~fas_handle()
+    {
+        for (auto e : ev_pool) cudaEventDestroy(e);
+        if (ev_t0) cudaEventDestroy(ev_t0);
+        if (ev_t1) cudaEventDestroy(ev_t1);
+        if (hc) cudaFreeHost(hc);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    DevGp gp()
+    {
+        DevGp G;
+        G.ngps = ngps;
+        G.ldsv = nsvld;
+        G.ldsl = maxns;
+        G.eps = eps.p; G.dep = dep.p; G.st = st.p; G.ep = ep.p; G.ds = ds.p; G.de = de.p;
+        G.rt = rt.p; G.dr = dr.p; G.sv = sv.p; G.dsv = dsv.p; G.srate = srate.p;
+        G.cumslip = cumslip.p; G.timestwinned = timestwinned.p; G.twinsys = twinsys.p;
+        G.tflag = flags.p + 1; G.cp_iters = cp_iters.p; G.erepmd = erepmd.p; G.ops = ops.p;
+        return G;
+    }
+    MeshDev mesh()
+    {
+        MeshDev m;
+        m.nlmnt = nlmnt; m.nnod = nnod; m.ln = ln.p; m.gpe = gpe.p; m.le = le.p; m.ib = ib.p;
+        m.ne_elem = ne_elem.p; m.ne_loc = ne_loc.p; m.ne_cnt = ne_cnt.p;
+        return m;
+    }
+    BlockDev block()
+    {
+        BlockDev b;
+        b.R = nnod; b.perm = perm.p; b.nslot = nslot.p; b.bcol = bcol.p; b.bloc = bloc.p; b.blk = blk.p;
+        return b;
+    }
+};
+
+#define CK(expr)                                      \
+    do {                                              \
+        cudaError_t e_ = (expr);                      \
+        if (e_ != cudaSuccess) {                      \
+            std::fprintf(stderr, "fasgpu: %s: %s\n", #expr, cudaGetErrorString(e_)); \
+            return FAS_E_CUDA;                        \
+        }                                             \
+    } while (0)
+#define CKA(expr)                                     \
+    do {                                              \
+        cudaError_t e_ = (expr);                      \
+        if (e_ != cudaSuccess) return e_ == cudaErrorMemoryAllocation ? FAS_E_NOMEM : FAS_E_CUDA; \
+    } while (0)
+#define LAUNCHED(h)                                   \
+    do {                                              \
+        ++(h)->launches;                              \
+        CK(cudaGetLastError());                       \
+    } while (0)
+
+namespace {
+
+// ---------------------------------------------------------------- profiling
+cudaEvent_t take_event(fas_handle *h)
+{
+    cudaEvent_t e;
+    if (!h->ev_pool.empty()) {
+        e = h->ev_pool.back();
+        h->ev_pool.pop_back();
+    } else {
+        cudaEventCreate(&e);
+    }
+    return e;
+}
+struct Span {                    // event pair around one launch while profiling
+    fas_handle *h;
+    cudaEvent_t a = nullptr, b = nullptr;
+    double *acc;
+    explicit Span(fas_handle *hh, double *accum) : h(hh), acc(accum)
+    {
+        if (h->prof) {
+            a = take_event(h);
+            b = take_event(h);
+            cudaEventRecord(a, h->stream);
+        }
+    }
+    void end()
+    {
+        if (a) cudaEventRecord(b, h->stream);
+    }
+};
+void keep(fas_handle *h, const Span &sp)
+{
+    if (sp.a) h->pending.push_back({{sp.a, sp.b}, sp.acc});
+}
+void settle_spans(fas_handle *h)
+{
+    for (auto &q : h->pending) {
+        float ms = 0.f;
+        cudaEventSynchronize(q.first.second);
+        cudaEventElapsedTime(&ms, q.first.first, q.first.second);
+        *q.second += ms;
+        h->ev_pool.push_back(q.first.first);
+        h->ev_pool.push_back(q.first.second);
+    }
+    h->pending.clear();
+}
+
+// ---------------------------------------------------------------- set-up
+int greedy_colouring(fas_handle *h, const std::vector<double> &xyz)
+{
+    // Same rule as the checker: nodes visited in ascending (z, y, x, id)
+    // order take the smallest colour unused by nodes sharing an element.
+    const int nn = h->nnod;
+    std::vector<int> order(nn);
+    for (int i = 0; i < nn; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int b) {
+        for (int c = 2; c >= 0; --c) {
+            const double xa = xyz[3 * (size_t)a + c], xb = xyz[3 * (size_t)b + c];
+            if (xa != xb) return xa < xb;
+        }
+        return a < b;
+    });
+    h->h_colour.assign(nn, -1);
+    int ncol = 0;
+    std::vector<int> used(64, -1);
+    for (int n : order) {
+        for (int k = h->ne_ptr[n]; k < h->ne_ptr[n + 1]; ++k) {
+            const int e = h->ne_list[k];
+            for (int a = 0; a < 8; ++a) {
+                const int c = h->h_colour[h->h_ln[(size_t)e * 8 + a]];
+                if (c >= 0) {
+                    if (c >= (int)used.size()) used.resize(c + 1, -1);
+                    used[c] = n;
+                }
+            }
+        }
+        int c = 0;
+        while (c < (int)used.size() && used[c] == n) ++c;
+        h->h_colour[n] = c;
+        ncol = std::max(ncol, c + 1);
+    }
+    h->ncol = ncol;
+    return 0;
+}
+
+// Row permutation by colour, node block neighbourhoods and the per-slot
+// element-local index words; allocates the block matrix.
+int build_layout(fas_handle *h, const std::vector<double> &xyz)
+{
+    const int nn = h->nnod;
+    greedy_colouring(h, xyz);
+    std::vector<int> perm(nn), rowof(nn);
+    for (int i = 0; i < nn; ++i) perm[i] = i;
+    std::stable_sort(perm.begin(), perm.end(),
+                     [&](int a, int b) { return h->h_colour[a] < h->h_colour[b]; });
+    for (int p = 0; p < nn; ++p) rowof[perm[p]] = p;
+    h->col_start.assign(h->ncol + 1, 0);
+    for (int p = 0; p < nn; ++p) h->col_start[h->h_colour[perm[p]] + 1] = p + 1;
+    for (int c = 1; c <= h->ncol; ++c) h->col_start[c] = std::max(h->col_start[c], h->col_start[c - 1]);
+
+    std::vector<int> nslot(nn), bcol((size_t)SLOTS * nn, 0);
+    std::vector<unsigned> bloc((size_t)SLOTS * nn, 0xFFFFFFFFu);
+    for (int p = 0; p < nn; ++p) {
+        const int n = perm[p];
+        int nb[SLOTS];
+        int cnt = 0;
+        nb[cnt++] = n;
+        std::vector<int> others;
+        for (int k = h->ne_ptr[n]; k < h->ne_ptr[n + 1]; ++k) {
+            const int e = h->ne_list[k];
+            for (int a = 0; a < 8; ++a) {
+                const int m = h->h_ln[(size_t)e * 8 + a];
+                if (m != n && std::find(others.begin(), others.end(), m) == others.end()) others.push_back(m);
+            }
+        }
+        std::sort(others.begin(), others.end());
+        if ((int)others.size() + 1 > SLOTS) return FAS_E_RANGE;
+        for (int m : others) nb[cnt++] = m;
+        nslot[p] = cnt;
+        for (int s = 0; s < cnt; ++s) {
+            bcol[(size_t)s * nn + p] = nb[s];
+            unsigned word = 0xFFFFFFFFu;
+            int k = 0;
+            for (int q = h->ne_ptr[n]; q < h->ne_ptr[n + 1]; ++q, ++k) {
+                const int e = h->ne_list[q];
+                unsigned b = 0xF;
+                for (int a = 0; a < 8; ++a)
+                    if (h->h_ln[(size_t)e * 8 + a] == nb[s]) { b = (unsigned)a; break; }
+                word = (word & ~(0xFu << (4 * k))) | (b << (4 * k));
+            }
+            bloc[(size_t)s * nn + p] = word;
+        }
+    }
+    // algorithmic bytes of one colour launch: blocks and column ids of the
+    // row, perm + nslot, and rhs read + solution read/write of its node
+    h->col_bytes.assign(h->ncol, 0.0);
+    for (int c = 0; c < h->ncol; ++c)
+        for (int p = h->col_start[c]; p < h->col_start[c + 1]; ++p)
+            h->col_bytes[c] += nslot[p] * (72.0 + 4.0) + 8.0 + 72.0;
+    // algorithmic bytes of one assembly launch: each element record read
+    // once (52 used doubles), each block written once, the slot tables and
+    // node adjacency read once, fc and ddx written
+    double ab = (double)h->nlmnt * 52.0 * 8.0 + (double)nn * (48.0 + 8.0 + 12.0 * MAXADJ);
+    for (int p = 0; p < nn; ++p) ab += nslot[p] * (72.0 + 8.0);
+    h->asm_bytes = ab;
+    cudaStream_t s = h->stream;
+    CKA(h->perm.alloc(nn));
+    CKA(h->rowof.alloc(nn));
+    CKA(h->nslot.alloc(nn));
+    CKA(h->bcol.alloc((size_t)SLOTS * nn));
+    CKA(h->bloc.alloc((size_t)SLOTS * nn));
+    CKA(h->blk.alloc((size_t)SLOTS * 9 * nn));
+    CK(h->perm.put(perm.data(), nn, s));
+    CK(h->rowof.put(rowof.data(), nn, s));
+    CK(h->nslot.put(nslot.data(), nn, s));
+    CK(h->bcol.put(bcol.data(), bcol.size(), s));
+    CK(h->bloc.put(bloc.data(), bloc.size(), s));
+    CK(h->blk.zero(s));
+    // SOR reduction partials
+    h->sor_boff.assign(h->ncol, 0);
+    h->sor_nblk.assign(h->ncol, 0);
+    int tot = 0;
+    for (int c = 0; c < h->ncol; ++c) {
+        h->sor_boff[c] = tot;
+        h->sor_nblk[c] = (int)nblocks(h->col_start[c + 1] - h->col_start[c], 256);
+        tot += h->sor_nblk[c];
+    }
+    h->sor_nblk_tot = std::max(tot, 1);
+    CKA(h->part_sor.alloc((size_t)2 * h->sor_nblk_tot));
+    CK(cudaStreamSynchronize(s));
+    return 0;
+}
+
+int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, const fas_ctrl_desc *Cd)
+{
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return FAS_E_NODEVICE;
+    CK(cudaGetDevice(&h->dev));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, h->dev));
+    if (prop.major != 10) return FAS_E_NODEVICE;
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CK(cudaMallocHost((void **)&h->hc, sizeof(HostCtl)));
+    CK(cudaEventCreate(&h->ev_t0));
+    CK(cudaEventCreate(&h->ev_t1));
+    cudaStream_t s = h->stream;
+
+    if (Md->nlmnt < 0 || Md->nnod < 0 || Md->ngps <= 0) return FAS_E_ARG;
+    h->nlmnt = Md->nlmnt;
+    h->nnod = Md->nnod;
+    h->ngps = Md->ngps;
+    h->point_mode = h->nlmnt == 0;
+    h->h_gp_iel.assign(h->ngps, 1);
+    if (!h->point_mode) {
+        if (!Md->le || !Md->lt || !Md->nd || !Md->np || !Md->ln || !Md->lg || !Md->ib) return FAS_E_ARG;
+        if (Md->ld_ln < 8 || Md->ld_lg < 1 || h->nnod < 1) return FAS_E_ARG;
+        const int ne = h->nlmnt;
+        h->h_ln.resize((size_t)ne * 8);
+        h->h_gpe.resize(ne);
+        h->h_le.assign(Md->le, Md->le + ne);
+        std::vector<int> gp_seen(h->ngps, 0);
+        for (int e = 0; e < ne; ++e) {
+            if (Md->lt[e] != 12) return FAS_E_ELTYPE;
+            if (Md->nd[e] != 8 || Md->np[e] != 1) return FAS_E_ARG;
+            for (int a = 0; a < 8; ++a) {
+                const int id = Md->ln[(size_t)e * Md->ld_ln + a];
+                if (id < 1 || id > h->nnod) return FAS_E_ARG;
+                h->h_ln[(size_t)e * 8 + a] = id - 1;
+            }
+            const int g = Md->lg[(size_t)e * Md->ld_lg];
+            if (g < 1 || g > h->ngps || gp_seen[g - 1]) return FAS_E_ARG;
+            gp_seen[g - 1] = 1;
+            h->h_gpe[e] = g - 1;
+            h->h_gp_iel[g - 1] = Md->le[e];
+        }
+        if (std::abs(Md->le[ne - 1]) >= 1) h->last_mat = std::abs(Md->le[ne - 1]);
+        h->h_ib.assign(Md->ib, Md->ib + h->nnod);
+        // node -> element CSR (ascending element ids)
+        h->ne_ptr.assign(h->nnod + 1, 0);
+        for (int e = 0; e < ne; ++e)
+            for (int a = 0; a < 8; ++a) h->ne_ptr[h->h_ln[(size_t)e * 8 + a] + 1]++;
+        for (int n = 0; n < h->nnod; ++n) {
+            if (h->ne_ptr[n + 1] > MAXADJ) return FAS_E_RANGE;
+            h->ne_ptr[n + 1] += h->ne_ptr[n];
+        }
+        h->ne_list.resize(h->ne_ptr[h->nnod]);
+        h->ne_locl.resize(h->ne_ptr[h->nnod]);
+        std::vector<int> fill(h->ne_ptr.begin(), h->ne_ptr.end() - 1);
+        for (int e = 0; e < ne; ++e)
+            for (int a = 0; a < 8; ++a) {
+                const int n = h->h_ln[(size_t)e * 8 + a];
+                h->ne_list[fill[n]] = e;
+                h->ne_locl[fill[n]] = a;
+                fill[n]++;
+            }
+        std::vector<int> lnT((size_t)8 * ne), nee((size_t)MAXADJ * h->nnod, -1),
+            nel((size_t)MAXADJ * h->nnod, 0), nec(h->nnod);
+        for (int e = 0; e < ne; ++e)
+            for (int a = 0; a < 8; ++a) lnT[(size_t)a * ne + e] = h->h_ln[(size_t)e * 8 + a];
+        for (int n = 0; n < h->nnod; ++n) {
+            nec[n] = h->ne_ptr[n + 1] - h->ne_ptr[n];
+            for (int k = 0; k < nec[n]; ++k) {
+                nee[(size_t)k * h->nnod + n] = h->ne_list[h->ne_ptr[n] + k];
+                nel[(size_t)k * h->nnod + n] = h->ne_locl[h->ne_ptr[n] + k];
+            }
+        }
+        CKA(h->ln.alloc(lnT.size()));
+        CKA(h->gpe.alloc(ne));
+        CKA(h->le.alloc(ne));
+        CKA(h->ib.alloc(h->nnod));
+        CKA(h->ne_elem.alloc(nee.size()));
+        CKA(h->ne_loc.alloc(nel.size()));
+        CKA(h->ne_cnt.alloc(nec.size()));
+        CK(h->ln.put(lnT.data(), lnT.size(), s));
+        CK(h->gpe.put(h->h_gpe.data(), ne, s));
+        CK(h->le.put(h->h_le.data(), ne, s));
+        CK(h->ib.put(h->h_ib.data(), h->nnod, s));
+        CK(h->ne_elem.put(nee.data(), nee.size(), s));
+        CK(h->ne_loc.put(nel.data(), nel.size(), s));
+        CK(h->ne_cnt.put(nec.data(), nec.size(), s));
+        CK(cudaStreamSynchronize(s));
+    } else {
+        if (!Md->le) return FAS_E_ARG;
+        for (int g = 0; g < h->ngps; ++g) h->h_gp_iel[g] = Md->le[g];
+    }
+    // ---- materials
+    if (!T || (T->real_bytes != 4 && T->real_bytes != 8)) return FAS_E_ARG;
+    const int rb = T->real_bytes, L = T->ld_ss, nm = T->nmatl;
+    if (nm < 1 || nm > 12 || L < 1 || L > MAXSS) return FAS_E_ARG;
+    std::vector<double> e(9 * nm, 0.0), ssang((size_t)nm * MAXSS, 0.0), ab((size_t)nm * MAXSS * 3, 0.0),
+        an((size_t)nm * MAXSS * 3, 0.0), ampar((size_t)nm * MAXSS * 6, 0.0),
+        sm((size_t)nm * MAXSS * MAXSS, 0.0);
+    h->M = DevMat{};
+    h->M.nmatl = nm;
+    for (int m = 0; m < nm; ++m) {
+        const int ns = T->nss[m];
+        if (ns < 1 || ns > L) return FAS_E_ARG;
+        h->M.ns[m] = ns;
+        h->maxns = std::max(h->maxns, ns);
+        for (int k = 0; k < 9; ++k) e[9 * m + k] = rdv(T->e, rb, (size_t)9 * m + k);
+        double amx = -1e300;
+        for (int i = 0; i < ns; ++i) {
+            ssang[(size_t)m * MAXSS + i] = rdv(T->ssang, rb, (size_t)m * L + i);
+            for (int k = 0; k < 3; ++k) {
+                ab[((size_t)m * MAXSS + i) * 3 + k] = rdv(T->ab, rb, ((size_t)m * L + i) * 3 + k);
+                an[((size_t)m * MAXSS + i) * 3 + k] = rdv(T->an, rb, ((size_t)m * L + i) * 3 + k);
+            }
+            for (int k = 0; k < 6; ++k)
+                ampar[((size_t)m * MAXSS + i) * 6 + k] =
+                    k < T->nmpar ? rdv(T->ampar, rb, ((size_t)m * L + i) * 10 + k) : 0.0;
+            amx = std::max(amx, ampar[((size_t)m * MAXSS + i) * 6]);
+            for (int j = 0; j < ns; ++j)
+                sm[(size_t)m * MAXSS * MAXSS + (size_t)i * ns + j] =
+                    rdv(T->smatrx, rb, (size_t)m * L * L + (size_t)j * L + i);
+        }
+        h->M.amax[m] = amx;
+    }
+    for (int g = 0; g < h->ngps; ++g) {
+        const int mc = std::abs(h->h_gp_iel[g]);
+        if (mc < 1 || mc > nm) return FAS_E_ARG;
+    }
+    h->ns_tmpl = h->maxns <= 12 ? 12 : (h->maxns <= 32 ? 32 : 60);
+    h->nsvld = 3 + h->maxns;
+    CKA(h->m_e.alloc(e.size()));
+    CKA(h->m_ssang.alloc(ssang.size()));
+    CKA(h->m_ab.alloc(ab.size()));
+    CKA(h->m_an.alloc(an.size()));
+    CKA(h->m_ampar.alloc(ampar.size()));
+    CKA(h->m_sm.alloc(sm.size()));
+    CK(h->m_e.put(e.data(), e.size(), s));
+    CK(h->m_ssang.put(ssang.data(), ssang.size(), s));
+    CK(h->m_ab.put(ab.data(), ab.size(), s));
+    CK(h->m_an.put(an.data(), an.size(), s));
+    CK(h->m_ampar.put(ampar.data(), ampar.size(), s));
+    CK(h->m_sm.put(sm.data(), sm.size(), s));
+    h->M.e = h->m_e.p; h->M.ssang = h->m_ssang.p; h->M.ab = h->m_ab.p; h->M.an = h->m_an.p;
+    h->M.ampar = h->m_ampar.p; h->M.sm = h->m_sm.p;
+    h->M.twinlim = T->twinlim;
+    h->M.twinprob = T->twinprob;
+    // ---- control
+    if (!Cd || (Cd->real_bytes != 4 && Cd->real_bytes != 8) || Cd->ninc1 < 1 || !Cd->tiem) return FAS_E_ARG;
+    const int cb = Cd->real_bytes;
+    h->C.toler = Cd->toler; h->C.alpha = Cd->alpha; h->C.afactor = Cd->afactor; h->C.efix = Cd->efix;
+    h->C.smale = Cd->smale; h->C.smalr = Cd->smalr; h->C.maxit = Cd->maxit; h->C.seed = Cd->twin_seed;
+    h->ninc1 = Cd->ninc1; h->nxs = Cd->nxs; h->nfs = Cd->nfs;
+    if (h->nxs < 0 || h->nfs < 0 || (h->nxs > 0 && (!Cd->x_spec || Cd->ld_xs < h->nxs)) ||
+        (h->nfs > 0 && (!Cd->f_spec || Cd->ld_xs < h->nfs)))
+        return FAS_E_ARG;
+    h->h_tiem.resize(h->ninc1);
+    for (int i = 0; i < h->ninc1; ++i) h->h_tiem[i] = rdv(Cd->tiem, cb, i);
+    std::vector<double> xs((size_t)h->ninc1 * std::max(h->nxs, 1) * 15, 0.0),
+        fs((size_t)h->ninc1 * std::max(h->nfs, 1) * 3, 0.0);
+    for (int i = 0; i < h->ninc1; ++i) {
+        for (int j = 0; j < h->nxs; ++j)
+            for (int k = 0; k < 15; ++k)
+                xs[((size_t)i * h->nxs + j) * 15 + k] = rdv(Cd->x_spec, cb, ((size_t)i * Cd->ld_xs + j) * 15 + k);
+        for (int j = 0; j < h->nfs; ++j)
+            for (int k = 0; k < 3; ++k)
+                fs[((size_t)i * h->nfs + j) * 3 + k] = rdv(Cd->f_spec, cb, ((size_t)i * Cd->ld_xs + j) * 3 + k);
+    }
+    CKA(h->xspec.alloc(xs.size()));
+    CKA(h->fspec.alloc(fs.size()));
+    CK(h->xspec.put(xs.data(), xs.size(), s));
+    CK(h->fspec.put(fs.data(), fs.size(), s));
+    // ---- state
+    const size_t nd3 = 3 * (size_t)h->nnod, ng = h->ngps;
+    CKA(h->x.alloc(nd3)); CKA(h->dx.alloc(nd3)); CKA(h->fc.alloc(nd3));
+    CKA(h->ddx.alloc(nd3)); CKA(h->rhs.alloc(nd3));
+    CKA(h->eps.alloc(ng)); CKA(h->dep.alloc(ng));
+    CKA(h->st.alloc(6 * ng)); CKA(h->ep.alloc(6 * ng)); CKA(h->ds.alloc(6 * ng)); CKA(h->de.alloc(6 * ng));
+    CKA(h->rt.alloc(3 * ng)); CKA(h->dr.alloc(3 * ng));
+    CKA(h->sv.alloc((size_t)h->nsvld * ng)); CKA(h->dsv.alloc((size_t)h->nsvld * ng));
+    CKA(h->srate.alloc((size_t)h->maxns * ng)); CKA(h->cumslip.alloc((size_t)h->maxns * ng));
+    CKA(h->erepmd.alloc(ng)); CKA(h->ops.alloc(ng));
+    CKA(h->timestwinned.alloc(ng)); CKA(h->twinsys.alloc(ng)); CKA(h->cp_iters.alloc(ng));
+    CKA(h->gp_iel.alloc(ng));
+    CK(h->gp_iel.put(h->h_gp_iel.data(), ng, s));
+    for (DVec<double> *v : {&h->x, &h->dx, &h->fc, &h->ddx, &h->rhs, &h->eps, &h->dep, &h->st, &h->ep,
+                            &h->ds, &h->de, &h->rt, &h->dr, &h->sv, &h->dsv, &h->srate, &h->cumslip,
+                            &h->erepmd, &h->ops})
+        CK(v->zero(s));
+    CK(h->timestwinned.zero(s));
+    CK(h->twinsys.zero(s));
+    CK(h->cp_iters.zero(s));
+    if (h->point_mode) {
+        CKA(h->chi_pts.alloc(36 * ng));
+        CK(h->chi_pts.zero(s));
+    } else {
+        CKA(h->rec.alloc((size_t)REC * h->nlmnt));
+        CK(h->rec.zero(s));
+    }
+    h->nr_nblk = (int)std::min<long long>(nblocks(std::max<long long>(h->nnod, h->ngps), 256), 1184);
+    h->nr_nblk = std::max(h->nr_nblk, 1);
+    CKA(h->part_nr.alloc((size_t)4 * h->nr_nblk));
+    CKA(h->sums.alloc(8));
+    CKA(h->ekey.alloc(2));
+    CKA(h->flags.alloc(4));
+    CKA(h->sorctl.alloc(1));
+    CK(h->flags.zero(s));
+    CK(cudaStreamSynchronize(s));
+    return 0;
+}
+
+// ---------------------------------------------------------------- state I/O
+int ensure_stage(fas_handle *h, size_t bytes)
+{
+    if (h->stage.n >= bytes) return 0;
+    CKA(h->stage.alloc(bytes));
+    return 0;
+}
+
+// caller array [n][ld] (element size rb): its first nk columns -> device
+// SoA [nk][n] in FP64.  A pitched copy moves only the nk used columns.
+int up_field(fas_handle *h, const void *src, int rb, int ld, int nk, int n, double *dst)
+{
+    if (!src || nk <= 0 || n <= 0) return 0;
+    const size_t bytes = (size_t)n * nk * rb;
+    int rc = ensure_stage(h, bytes);
+    if (rc) return rc;
+    if (ld == nk) CK(cudaMemcpyAsync(h->stage.p, src, bytes, cudaMemcpyHostToDevice, h->stream));
+    else CK(cudaMemcpy2DAsync(h->stage.p, (size_t)nk * rb, src, (size_t)ld * rb, (size_t)nk * rb, n,
+                              cudaMemcpyHostToDevice, h->stream));
+    k_aos_to_soa<<<nblocks((long long)nk * n, 256), 256, 0, h->stream>>>(h->stage.p, rb, nk, nk, n, dst);
+    LAUNCHED(h);
+    return 0;
+}
+
+// device SoA [nk][n] -> the first nk columns of the caller's [n][ld] array;
+// columns beyond nk are left untouched.
+int down_field(fas_handle *h, void *dst, int rb, int ld, int nk, int n, const double *src)
+{
+    if (!dst || nk <= 0 || n <= 0) return 0;
+    const size_t bytes = (size_t)n * nk * rb;
+    int rc = ensure_stage(h, bytes);
+    if (rc) return rc;
+    k_soa_to_aos<<<nblocks((long long)nk * n, 256), 256, 0, h->stream>>>(src, nk, n, h->stage.p, rb, nk);
+    LAUNCHED(h);
+    if (ld == nk) CK(cudaMemcpyAsync(dst, h->stage.p, bytes, cudaMemcpyDeviceToHost, h->stream));
+    else CK(cudaMemcpy2DAsync(dst, (size_t)ld * rb, h->stage.p, (size_t)nk * rb, (size_t)nk * rb, n,
+                              cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int upload_impl(fas_handle *h, const fas_state_desc *S)
+{
+    if (!S || (S->real_bytes != 4 && S->real_bytes != 8)) return FAS_E_ARG;
+    if (S->nsv < 0 || S->nsv > S->ld_sv) return FAS_E_ARG;
+    const int rb = S->real_bytes, nd3 = 3 * h->nnod, ng = h->ngps;
+    if (S->nsv > 0) h->nsv = std::min(S->nsv, h->nsvld);
+    int rc;
+#define UP(ptr, ld, nk, n, dst) if ((rc = up_field(h, ptr, rb, ld, nk, n, dst))) return rc
+    UP(S->x, 1, 1, nd3, h->x.p);
+    UP(S->dx, 1, 1, nd3, h->dx.p);
+    UP(S->fc, 1, 1, nd3, h->fc.p);
+    UP(S->ddx, 1, 1, nd3, h->ddx.p);
+    UP(S->eps, 1, 1, ng, h->eps.p);
+    UP(S->dep, 1, 1, ng, h->dep.p);
+    UP(S->st, 6, 6, ng, h->st.p);
+    UP(S->ep, 6, 6, ng, h->ep.p);
+    UP(S->ds, 6, 6, ng, h->ds.p);
+    UP(S->de, 6, 6, ng, h->de.p);
+    UP(S->rt, 3, 3, ng, h->rt.p);
+    UP(S->dr, 3, 3, ng, h->dr.p);
+    const int nsvk = std::min(S->ld_sv, h->nsvld);
+    UP(S->sv, S->ld_sv, nsvk, ng, h->sv.p);
+    UP(S->dsv, S->ld_sv, nsvk, ng, h->dsv.p);
+    if (S->srate || S->cumslip) {
+        if (S->ld_slip < 1) return FAS_E_ARG;
+        const int nsl = std::min(S->ld_slip, h->maxns);
+        UP(S->srate, S->ld_slip, nsl, ng, h->srate.p);
+        UP(S->cumslip, S->ld_slip, nsl, ng, h->cumslip.p);
+    }
+#undef UP
+    if (S->timestwinned)
+        CK(cudaMemcpyAsync(h->timestwinned.p, S->timestwinned, ng * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    if (S->twinsys)
+        CK(cudaMemcpyAsync(h->twinsys.p, S->twinsys, ng * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    if (!h->have_state && !h->point_mode) {
+        if (!S->x) return FAS_E_STATE;
+        std::vector<double> xyz(nd3);
+        for (int i = 0; i < nd3; ++i) xyz[i] = rdv(S->x, rb, i);
+        rc = build_layout(h, xyz);
+        if (rc) return rc;
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    h->have_state = true;
+    return 0;
+}
+
+int download_impl(fas_handle *h, const fas_state_desc *S)
+{
+    if (!S || (S->real_bytes != 4 && S->real_bytes != 8)) return FAS_E_ARG;
+    const int rb = S->real_bytes, nd3 = 3 * h->nnod, ng = h->ngps;
+    int rc;
+#define DN(ptr, ld, nk, n, src) if ((rc = down_field(h, ptr, rb, ld, nk, n, src))) return rc
+    DN(S->x, 1, 1, nd3, h->x.p);
+    DN(S->dx, 1, 1, nd3, h->dx.p);
+    DN(S->fc, 1, 1, nd3, h->fc.p);
+    DN(S->ddx, 1, 1, nd3, h->ddx.p);
+    DN(S->eps, 1, 1, ng, h->eps.p);
+    DN(S->dep, 1, 1, ng, h->dep.p);
+    DN(S->st, 6, 6, ng, h->st.p);
+    DN(S->ep, 6, 6, ng, h->ep.p);
+    DN(S->ds, 6, 6, ng, h->ds.p);
+    DN(S->de, 6, 6, ng, h->de.p);
+    DN(S->rt, 3, 3, ng, h->rt.p);
+    DN(S->dr, 3, 3, ng, h->dr.p);
+    const int nsvk = std::min(S->ld_sv, h->nsvld);
+    DN(S->sv, S->ld_sv, nsvk, ng, h->sv.p);
+    DN(S->dsv, S->ld_sv, nsvk, ng, h->dsv.p);
+    if (S->srate || S->cumslip) {
+        const int nsl = std::min(S->ld_slip, h->maxns);
+        DN(S->srate, S->ld_slip, nsl, ng, h->srate.p);
+        DN(S->cumslip, S->ld_slip, nsl, ng, h->cumslip.p);
+    }
+#undef DN
+    if (S->timestwinned)
+        CK(cudaMemcpyAsync(S->timestwinned, h->timestwinned.p, ng * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    if (S->twinsys)
+        CK(cudaMemcpyAsync(S->twinsys, h->twinsys.p, ng * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+// ---------------------------------------------------------------- phases
+template <int NS> int launch_elem(fas_handle *h, int inc, int nit)
+{
+    Span sp(h, &h->P.ms_constitutive);
+    k_elem<NS><<<nblocks(h->nlmnt, 128), 128, 0, h->stream>>>(
+        h->mesh(), h->M, h->C, h->gp(), h->x.p, h->dx.p, h->rec.p, h->h_tiem[inc - 1], inc, nit, h->ekey.p);
+    sp.end();
+    keep(h, sp);
+    LAUNCHED(h);
+    h->P.n_constitutive++;
+    h->P.gp_updates += h->ngps;
+    return 0;
+}
+
+// ELVALS (+ SUVALS when bc): element pass then row-gather assembly.
+// Returns the first element's FAFERR code in element order, if any.
+int elvals_impl(fas_handle *h, int inc, int nit, bool bc)
+{
+    cudaStream_t s = h->stream;
+    CK(cudaMemsetAsync(h->ekey.p, 0xFF, sizeof(unsigned long long), s));
+    CK(cudaMemsetAsync(h->flags.p, 0, sizeof(int), s));
+    int rc;
+    switch (h->ns_tmpl) {
+    case 12: rc = launch_elem<12>(h, inc, nit); break;
+    case 32: rc = launch_elem<32>(h, inc, nit); break;
+    default: rc = launch_elem<60>(h, inc, nit); break;
+    }
+    if (rc) return rc;
+    {
+        Span sp(h, &h->P.ms_assembly);
+        const long long nthr = (long long)SLOTS * h->nnod;
+        k_assemble<<<nblocks(nthr, 256), 256, 0, s>>>(
+            h->mesh(), h->block(), h->rec.p, h->x.p, h->dx.p, h->fc.p, h->ddx.p,
+            h->xspec.p + (size_t)(inc - 1) * std::max(h->nxs, 1) * 15,
+            h->fspec.p + (size_t)(inc - 1) * std::max(h->nfs, 1) * 3, h->nxs, h->nfs, h->C.efix,
+            bc ? 1 : 0, h->flags.p);
+        sp.end();
+        keep(h, sp);
+        LAUNCHED(h);
+        h->P.n_assembly++;
+        h->P.assembly_bytes += h->asm_bytes;
+    }
+    CK(cudaMemcpyAsync(h->hc->ekey, h->ekey.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(h->hc->flags, h->flags.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    settle_spans(h);
+    if (h->hc->ekey[0] != ~0ull) return (int)(h->hc->ekey[0] & 0xFFFFull);
+    if (h->hc->flags[0]) return FAS_E_ARG;
+    return 0;
+}
+
+int suvals_impl(fas_handle *h, int inc)
+{
+    cudaStream_t s = h->stream;
+    CK(cudaMemsetAsync(h->flags.p, 0, sizeof(int), s));
+    k_suvals<<<nblocks(h->nnod, 256), 256, 0, s>>>(
+        h->mesh(), h->block(), h->rowof.p, h->x.p, h->dx.p, h->fc.p, h->ddx.p,
+        h->xspec.p + (size_t)(inc - 1) * std::max(h->nxs, 1) * 15,
+        h->fspec.p + (size_t)(inc - 1) * std::max(h->nfs, 1) * 3, h->nxs, h->nfs, h->C.efix, h->flags.p);
+    LAUNCHED(h);
+    CK(cudaMemcpyAsync(h->hc->flags, h->flags.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return h->hc->flags[0] ? FAS_E_ARG : 0;
+}
+
+// FACSLS: rhs <- ddx, ddx <- 0, multicolour SOR sweeps until the relative
+// change drops below toler^2 or 1000 sweeps (Stif_sol.f90:173-213).
+int facsls_impl(fas_handle *h, int *sweeps, double *error)
+{
+    cudaStream_t s = h->stream;
+    const size_t nd3 = 3 * (size_t)h->nnod;
+    CK(cudaMemcpyAsync(h->rhs.p, h->ddx.p, nd3 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemsetAsync(h->ddx.p, 0, nd3 * sizeof(double), s));
+    CK(cudaMemsetAsync(h->ekey.p + 1, 0xFF, sizeof(unsigned long long), s));
+    CK(cudaMemsetAsync(h->sorctl.p, 0, sizeof(SorCtl), s));
+    BlockDev B = h->block();
+    k_diag_check<<<nblocks(h->nnod, 256), 256, 0, s>>>(B, h->ekey.p + 1);
+    LAUNCHED(h);
+    CK(cudaMemcpyAsync(&h->hc->ekey[1], h->ekey.p + 1, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (h->hc->ekey[1] != ~0ull) return 903;
+    const double tolerl = h->C.toler * h->C.toler;
+    int done = 0, chunk = 4;
+    while (done < 1000) {
+        const int k = std::min(chunk, 1000 - done);
+        for (int it = 0; it < k; ++it) {
+            for (int c = 0; c < h->ncol; ++c) {
+                const int p0 = h->col_start[c], p1 = h->col_start[c + 1];
+                if (p1 <= p0) continue;
+                Span sp(h, &h->P.ms_sor_colour);
+                k_sor_colour<<<h->sor_nblk[c], 256, 0, s>>>(B, p0, p1, h->rhs.p, h->ddx.p, h->sorctl.p,
+                                                           h->part_sor.p, h->sor_boff[c], h->sor_nblk_tot);
+                sp.end();
+                keep(h, sp);
+                LAUNCHED(h);
+            }
+            k_sor_check<<<1, 1024, 0, s>>>(h->part_sor.p, h->sor_nblk_tot, h->sorctl.p, tolerl);
+            LAUNCHED(h);
+        }
+        done += k;
+        CK(cudaMemcpyAsync(&h->hc->sor, h->sorctl.p, sizeof(SorCtl), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (h->hc->sor.conv) break;
+        chunk = std::min(chunk * 2, 64);
+    }
+    settle_spans(h);
+    const int nsw = h->hc->sor.sweeps;
+    h->P.sor_sweeps += nsw;
+    h->P.n_sor_colour += (int64_t)nsw * h->ncol;
+    double bytes = 0.0;
+    for (double b : h->col_bytes) bytes += b;
+    h->P.sor_bytes += bytes * nsw;
+    if (sweeps) *sweeps = nsw;
+    if (error) *error = h->hc->sor.err;
+    if (h->hc->sor.err > 10.0 * tolerl) return 904;
+    return 0;
+}
+
+int nriter_impl(fas_handle *h, int inc, fas_iter_report *rep, int cap, int *n_rep)
+{
+    cudaStream_t s = h->stream;
+    const int ndof = 3 * h->nnod;
+    int nit = 0;
+    bool l_conv = true;
+    while (l_conv) {
+        ++nit;
+        if (n_rep) *n_rep = nit;
+        int rc = elvals_impl(h, inc, nit, true);
+        if (rc) return rc;
+        int sweeps = 0;
+        double serr = 0.0;
+        rc = facsls_impl(h, &sweeps, &serr);
+        if (rc) return rc;
+        k_nr_norms<<<h->nr_nblk, 256, 0, s>>>(h->nnod, h->ngps, h->ib.p, h->rhs.p, h->dx.p, h->ddx.p,
+                                              h->erepmd.p, h->part_nr.p, h->nr_nblk);
+        LAUNCHED(h);
+        k_final_sum<4><<<1, 1024, 0, s>>>(h->part_nr.p, h->nr_nblk, h->sums.p);
+        LAUNCHED(h);
+        CK(cudaMemcpyAsync(h->hc->sums, h->sums.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        const double sfc = std::sqrt(h->hc->sums[0]);
+        const double errdx = std::sqrt(h->hc->sums[1]);
+        const double erddx = std::sqrt(h->hc->sums[2]);
+        const double sdx = errdx == 0.0 ? h->C.toler : erddx / errdx;
+        const double alp2 = 1.0 / (1.0 + h->C.alpha * sdx);
+        if (rep && nit <= cap) {
+            fas_iter_report &r = rep[nit - 1];
+            r.nit = nit;
+            r.sor_sweeps = sweeps;
+            r.sdx = sdx;
+            r.sfc = sfc;
+            r.cp_err = h->hc->sums[3] / (double)h->ngps;
+            r.alp2 = alp2;
+            r.sor_error = serr;
+        }
+        k_nr_update<<<nblocks(ndof, 256), 256, 0, s>>>(ndof, alp2, h->ddx.p, h->x.p, h->dx.p);
+        LAUNCHED(h);
+        l_conv = (sdx >= h->C.toler) && (nit < h->C.maxit);
+    }
+    const int nsc = h->M.ns[h->last_mat - 1];
+    k_cumslip<<<nblocks(h->ngps, 256), 256, 0, s>>>(h->gp(), nsc, h->h_tiem[inc - 1]);
+    LAUNCHED(h);
+    CK(cudaStreamSynchronize(s));
+    return 0;
+}
+
+int reorient_impl(fas_handle *h, int inc, fas_twin_event *ev, int cap, int *n_ev)
+{
+    cudaStream_t s = h->stream;
+    if (!h->events.p) CKA(h->events.alloc(std::max(h->ngps, 1)));
+    CK(cudaMemsetAsync(h->flags.p + 3, 0, sizeof(int), s));
+    k_reorient<<<nblocks(h->ngps, 256), 256, 0, s>>>(h->gp(), h->M, h->events.p, h->ngps, h->flags.p + 3);
+    LAUNCHED(h);
+    CK(cudaMemsetAsync(h->flags.p + 1, 0, sizeof(int), s));   // tflag = 0
+    CK(cudaMemcpyAsync(&h->hc->flags[3], h->flags.p + 3, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const int n = h->hc->flags[3];
+    if (n_ev) *n_ev = n;
+    if (ev && n > 0 && cap > 0) {
+        std::vector<TwinEv> tv(n);
+        CK(cudaMemcpy(tv.data(), h->events.p, n * sizeof(TwinEv), cudaMemcpyDeviceToHost));
+        std::sort(tv.begin(), tv.end(), [](const TwinEv &a, const TwinEv &b) { return a.gp < b.gp; });
+        for (int i = 0; i < std::min(n, cap); ++i) {
+            ev[i].inc = inc;
+            ev[i].gp = tv[i].gp + 1;
+            ev[i].sys = tv[i].sys + 1;
+            ev[i].pad = 0;
+            for (int k = 0; k < 3; ++k) {
+                ev[i].euler_old[k] = tv[i].eo[k];
+                ev[i].euler_new[k] = tv[i].en[k];
+            }
+        }
+    }
+    return 0;
+}
+
+int pattern_device(fas_handle *h, int ld, DVec<int> &isd)
+{
+    const size_t ndof = 3 * (size_t)h->nnod;
+    CKA(isd.alloc(ndof * ld));
+    CK(cudaMemsetAsync(h->flags.p + 2, 0, sizeof(int), h->stream));
+    k_setpta<<<nblocks((long long)ndof, 128), 128, 0, h->stream>>>(h->mesh(), ld, isd.p, h->flags.p + 2);
+    LAUNCHED(h);
+    CK(cudaMemcpyAsync(&h->hc->flags[2], h->flags.p + 2, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return h->hc->flags[2] ? 955 : 0;
+}
+
+}  // namespace
+
+// ================================================================ C ABI
+extern "C" {
+
+int32_t fas_gpu_create(const fas_mesh_desc *mesh, const fas_matl_desc *matl, const fas_ctrl_desc *ctrl,
+                       uint32_t mode, fas_handle **out)
+{
+    if (!out || !mesh || !matl || !ctrl) return FAS_E_ARG;
+    *out = nullptr;
+    fas_handle *h = new (std::nothrow) fas_handle;
+    if (!h) return FAS_E_NOMEM;
+    h->mode = mode;
+    const int rc = create_impl(h, mesh, matl, ctrl);
+    if (rc) {
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return 0;
+}
+
+void fas_gpu_destroy(fas_handle *h) { delete h; }
+
+int32_t fas_gpu_set_mode(fas_handle *h, uint32_t mode)
+{
+    if (!h) return FAS_E_ARG;
+    h->mode = mode;
+    return 0;
+}
+
+int32_t fas_gpu_upload_state(fas_handle *h, const fas_state_desc *s)
+{
+    if (!h) return FAS_E_ARG;
+    return upload_impl(h, s);
+}
+
+int32_t fas_gpu_download_state(fas_handle *h, const fas_state_desc *s)
+{
+    if (!h) return FAS_E_ARG;
+    return download_impl(h, s);
+}
+
+int32_t fas_gpu_update_node(fas_handle *h)
+{
+    if (!h) return FAS_E_ARG;
+    if (!h->have_state) return FAS_E_STATE;
+    const int nd3 = 3 * h->nnod;
+    if (nd3 > 0) {
+        k_update_node<<<nblocks(nd3, 256), 256, 0, h->stream>>>(nd3, h->x.p, h->dx.p);
+        LAUNCHED(h);
+    }
+    return 0;
+}
+
+int32_t fas_gpu_elvals(fas_handle *h, int32_t inc, int32_t nit)
+{
+    if (!h) return FAS_E_ARG;
+    if (!h->have_state || h->point_mode) return FAS_E_STATE;
+    if (inc < 1 || inc > h->ninc1) return FAS_E_ARG;
+    return elvals_impl(h, inc, nit, false);
+}
+
+int32_t fas_gpu_suvals(fas_handle *h, int32_t inc)
+{
+    if (!h) return FAS_E_ARG;
+    if (!h->have_state || h->point_mode) return FAS_E_STATE;
+    if (inc < 1 || inc > h->ninc1) return FAS_E_ARG;
+    return suvals_impl(h, inc);
+}
+
+int32_t fas_gpu_facsls(fas_handle *h, int32_t *sweeps, double *error)
+{
+    if (!h) return FAS_E_ARG;
+    if (!h->have_state || h->point_mode) return FAS_E_STATE;
+    return facsls_impl(h, sweeps, error);
+}
+
+int32_t fas_gpu_nriter(fas_handle *h, int32_t inc, fas_iter_report *rep, int32_t cap, int32_t *n_rep)
+{
+    if (!h) return FAS_E_ARG;
+    if (!h->have_state || h->point_mode) return FAS_E_STATE;
+    if (inc < 1 || inc > h->ninc1) return FAS_E_ARG;
+    int n = 0;
+    const int rc = nriter_impl(h, inc, rep, cap, &n);
+    if (n_rep) *n_rep = n;
+    return rc;
+}
+
+int32_t fas_gpu_update_gptv(fas_handle *h)
+{
+    if (!h) return FAS_E_ARG;
+    if (!h->have_state) return FAS_E_STATE;
+    k_update_gptv<<<nblocks(h->ngps, 256), 256, 0, h->stream>>>(h->gp(), h->nsv);
+    LAUNCHED(h);
+    return 0;
+}
+
+int32_t fas_gpu_reorient(fas_handle *h, int32_t inc, fas_twin_event *ev, int32_t cap, int32_t *n_ev)
+{
+    if (!h) return FAS_E_ARG;
+    if (!h->have_state) return FAS_E_STATE;
+    return reorient_impl(h, inc, ev, cap, n_ev);
+}
+
+int32_t fas_gpu_increment(fas_handle *h, int32_t inc, fas_iter_report *rep, int32_t cap, int32_t *n_rep,
+                          fas_twin_event *ev, int32_t ev_cap, int32_t *n_ev)
+{
+    int32_t rc = fas_gpu_update_node(h);
+    if (rc) return rc;
+    rc = fas_gpu_nriter(h, inc, rep, cap, n_rep);
+    if (rc) return rc;
+    rc = fas_gpu_update_gptv(h);
+    if (rc) return rc;
+    if (n_ev) *n_ev = 0;
+    CK(cudaMemcpyAsync(&h->hc->flags[1], h->flags.p + 1, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->hc->flags[1]) rc = reorient_impl(h, inc, ev, ev_cap, n_ev);
+    return rc;
+}
+
+int32_t fas_gpu_get_pattern(fas_handle *h, int32_t *is, int32_t ld_is)
+{
+    if (!h || !is || ld_is < 2) return FAS_E_ARG;
+    if (h->point_mode) return FAS_E_STATE;
+    DVec<int> isd;
+    int rc = pattern_device(h, ld_is, isd);
+    if (rc) return rc;
+    CK(cudaMemcpy(is, isd.p, isd.n * sizeof(int), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int32_t fas_gpu_get_stiffness(fas_handle *h, void *ss, int32_t ld_ss, int32_t real_bytes)
+{
+    if (!h || !ss || ld_ss < 2 || (real_bytes != 4 && real_bytes != 8)) return FAS_E_ARG;
+    if (h->point_mode || !h->have_state) return FAS_E_STATE;
+    DVec<int> isd;
+    int rc = pattern_device(h, ld_ss, isd);
+    if (rc) return rc;
+    const size_t n = 3 * (size_t)h->nnod * ld_ss;
+    DVec<double> ssd;
+    CKA(ssd.alloc(n));
+    k_to_ell<<<nblocks(3LL * h->nnod, 128), 128, 0, h->stream>>>(h->block(), h->rowof.p, h->nnod, ld_ss,
+                                                                 isd.p, ssd.p);
+    LAUNCHED(h);
+    std::vector<double> tmp(n);
+    CK(cudaMemcpyAsync(tmp.data(), ssd.p, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (size_t i = 0; i < n; ++i) {
+        if (real_bytes == 4) ((float *)ss)[i] = (float)tmp[i];
+        else ((double *)ss)[i] = tmp[i];
+    }
+    return 0;
+}
+
+int32_t fas_gpu_get_colouring(fas_handle *h, int32_t *colour, int32_t *ncol)
+{
+    if (!h) return FAS_E_ARG;
+    if (!h->have_state || h->point_mode) return FAS_E_STATE;
+    if (colour) std::copy(h->h_colour.begin(), h->h_colour.end(), colour);
+    if (ncol) *ncol = h->ncol;
+    return 0;
+}
+
+int32_t fas_gpu_constitutive(fas_handle *h, int32_t inc, int32_t nit)
+{
+    if (!h) return FAS_E_ARG;
+    if (!h->have_state) return FAS_E_STATE;
+    if (inc < 1 || inc > h->ninc1) return FAS_E_ARG;
+    if (!h->chi_pts.p) {
+        CKA(h->chi_pts.alloc(36 * (size_t)h->ngps));
+        CK(h->chi_pts.zero(h->stream));
+    }
+    cudaStream_t s = h->stream;
+    CK(cudaMemsetAsync(h->ekey.p, 0xFF, sizeof(unsigned long long), s));
+    Span sp(h, &h->P.ms_constitutive);
+    const double dt = h->h_tiem[inc - 1];
+    const unsigned nb = nblocks(h->ngps, 128);
+    switch (h->ns_tmpl) {
+    case 12: k_points<12><<<nb, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p); break;
+    case 32: k_points<32><<<nb, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p); break;
+    default: k_points<60><<<nb, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p); break;
+    }
+    sp.end();
+    keep(h, sp);
+    LAUNCHED(h);
+    h->P.n_constitutive++;
+    h->P.gp_updates += h->ngps;
+    CK(cudaMemcpyAsync(h->hc->ekey, h->ekey.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    settle_spans(h);
+    if (h->hc->ekey[0] != ~0ull) return (int)(h->hc->ekey[0] & 0xFFFFull);
+    return 0;
+}
+
+int32_t fas_gpu_get_tangent(fas_handle *h, void *chi, int32_t real_bytes)
+{
+    if (!h || !chi || (real_bytes != 4 && real_bytes != 8)) return FAS_E_ARG;
+    const size_t ng = h->ngps;
+    std::vector<double> out(36 * ng, 0.0);
+    if (h->point_mode || !h->rec.p) {
+        if (!h->chi_pts.p) return FAS_E_STATE;
+        std::vector<double> t(36 * ng);
+        CK(cudaMemcpy(t.data(), h->chi_pts.p, t.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for (size_t g = 0; g < ng; ++g)
+            for (int q = 0; q < 36; ++q) out[g * 36 + q] = t[(size_t)q * ng + g];
+    } else {
+        std::vector<double> r((size_t)REC * h->nlmnt);
+        CK(cudaMemcpy(r.data(), h->rec.p, r.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int e = 0; e < h->nlmnt; ++e) {
+            const size_t g = h->h_gpe[e];
+            for (int i = 0; i < 6; ++i)
+                for (int j = i; j < 6; ++j) {
+                    const double v = r[(size_t)e * REC + REC_D + utri(i, j)];
+                    out[g * 36 + i + 6 * j] = v;
+                    out[g * 36 + j + 6 * i] = v;
+                }
+        }
+    }
+    for (size_t i = 0; i < out.size(); ++i) {
+        if (real_bytes == 4) ((float *)chi)[i] = (float)out[i];
+        else ((double *)chi)[i] = out[i];
+    }
+    return 0;
+}
+
+int32_t fas_gpu_get_cp_stats(fas_handle *h, int32_t *iters, double *erepmd)
+{
+    if (!h) return FAS_E_ARG;
+    if (iters) CK(cudaMemcpy(iters, h->cp_iters.p, h->ngps * sizeof(int), cudaMemcpyDeviceToHost));
+    if (erepmd) CK(cudaMemcpy(erepmd, h->erepmd.p, h->ngps * sizeof(double), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int32_t fas_gpu_get_cp_ops(fas_handle *h, double *ops)
+{
+    if (!h || !ops) return FAS_E_ARG;
+    CK(cudaMemcpy(ops, h->ops.p, h->ngps * sizeof(double), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int32_t fas_gpu_profile(fas_handle *h, int32_t enable, fas_profile *out)
+{
+    if (!h) return FAS_E_ARG;
+    if (h->prof) {
+        CK(cudaEventRecord(h->ev_t1, h->stream));
+        CK(cudaEventSynchronize(h->ev_t1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, h->ev_t0, h->ev_t1));
+        h->P.ms_total = ms;
+        settle_spans(h);
+    }
+    h->P.n_launches = h->launches;
+    if (out) *out = h->P;
+    if (enable) {
+        h->P = fas_profile{};
+        h->launches = 0;
+        h->prof = true;
+        CK(cudaEventRecord(h->ev_t0, h->stream));
+    } else {
+        h->prof = false;
+    }
+    return 0;
+}
+
+}  // extern "C"

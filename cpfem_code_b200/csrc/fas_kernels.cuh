@@ -1,0 +1,721 @@
+// fas_kernels.cuh -- the sm_100a kernels of the increment hot path.
+//
+// Data layout in HBM (all FP64 unless noted):
+//   * nodal vectors x, dx, fc, ddx, rhs: reference DOF order 3*node+comp;
+//   * Gauss-point state: structure of arrays field[k * ngps + g];
+//   * element record rec[e * REC + .]: sfd (24), stress (6), weight, tangent
+//     upper triangle (21) -- written once per Newton iteration by the element
+//     kernel and read by the row-gather assembly;
+//   * stiffness: block-ELL of 3x3 node blocks, rows permuted so each SOR
+//     colour is a contiguous row range; blk[(slot*9 + r*3 + c) * R + row],
+//     slot 0 = the diagonal block, bcol[slot * R + row] = column node.
+#pragma once
+
+#include "fas_device.cuh"
+
+namespace fasdev {
+
+constexpr int REC = 56;          // doubles per element record
+constexpr int REC_S = 24, REC_W = 30, REC_D = 32;
+constexpr int SLOTS = 27;        // node blocks per row of an 8-node brick mesh
+constexpr int MAXADJ = 8;        // elements per node
+
+// upper-triangle index of chi(i,j), i <= j (0-based)
+__host__ __device__ __forceinline__ int utri(int i, int j) { return i * 6 - (i * (i - 1)) / 2 + (j - i); }
+
+struct MeshDev {
+    int nlmnt, nnod;
+    const int *ln;       // [8][nlmnt] 0-based node ids
+    const int *gpe;      // [nlmnt] 0-based GP of the element
+    const int *le;       // [nlmnt]
+    const int *ib;       // [nnod]
+    const int *ne_elem;  // [MAXADJ][nnod] adjacent elements, ascending
+    const int *ne_loc;   // [MAXADJ][nnod] local index of the node in it
+    const int *ne_cnt;   // [nnod]
+};
+
+struct BlockDev {
+    int R;               // rows (= nnod)
+    const int *perm;     // row -> node
+    const int *nslot;    // [R]
+    const int *bcol;     // [SLOTS][R] column node of each slot
+    const unsigned *bloc;// [SLOTS][R] 4-bit local index of the column node in
+                         // each adjacent element of the row node (0xF: absent)
+    double *blk;         // [SLOTS*9][R]
+};
+
+// ---------------------------------------------------------------- element pass
+// ELVALS per element (src/fasolt/Elvals.f90:31-126): gather, SHAPE_12,
+// DSTRNS, DSTRSS, store the GP increments and the element record.
+template <int NS>
+__global__ void __launch_bounds__(128) k_elem(MeshDev Mh, DevMat M, DevCtrl C, DevGp G,
+                                              const double *__restrict__ x,
+                                              const double *__restrict__ dx, double *rec,
+                                              double dt, int inc, int nit,
+                                              unsigned long long *errkey)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= Mh.nlmnt) return;
+    const int ne = Mh.nlmnt;
+    double xl[8][3], dxl[8][3];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        const int n = Mh.ln[a * ne + e];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            xl[a][c] = x[3 * n + c];
+            dxl[a][c] = dx[3 * n + c];
+        }
+    }
+    double sfd[8][3];
+    const double w = shape12(xl, sfd);
+    if (w < 1.e-7) {
+        atomicMin(errkey, ((unsigned long long)e << 16) | 920ull);
+        return;
+    }
+    double del[6], r[3], defl;
+    int rc = dstrns(sfd, dxl, C.smalr, C.smale, del, r, defl);
+    if (rc) {
+        atomicMin(errkey, ((unsigned long long)e << 16) | (unsigned long long)rc);
+        return;
+    }
+    const int g = Mh.gpe[e];
+    const int ng = G.ngps;
+    double st[6], ds[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        st[k] = G.st[k * ng + g];
+        ds[k] = G.ds[k * ng + g];
+    }
+    GpOut o;
+    rc = dstrss<NS>(M, C, G, g, Mh.le[e], del, r, st, ds, dt, inc, nit, o);
+    if (rc) {
+        atomicMin(errkey, ((unsigned long long)e << 16) | (unsigned long long)rc);
+        return;
+    }
+    G.dep[g] = o.deff;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        G.de[k * ng + g] = del[k];
+        G.ds[k * ng + g] = ds[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) G.dr[k * ng + g] = r[k];
+    double *R = rec + (size_t)e * REC;
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) R[3 * a + c] = sfd[a][c];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) R[REC_S + k] = o.t[k];
+    R[REC_W] = w;
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int j = i; j < 6; ++j) R[REC_D + utri(i, j)] = o.chi[i][j];
+}
+
+// Constitutive update of independent points (no mesh): DSTRSS with the
+// stored de / dr; the full tangent goes to chi[36][ngps] (column-major 6x6).
+template <int NS>
+__global__ void __launch_bounds__(128) k_points(DevMat M, DevCtrl C, DevGp G, const int *gp_iel,
+                                                double *chi, double dt, int inc, int nit,
+                                                unsigned long long *errkey)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G.ngps) return;
+    const int ng = G.ngps;
+    double de[6], r[3], st[6], ds[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        de[k] = G.de[k * ng + g];
+        st[k] = G.st[k * ng + g];
+        ds[k] = G.ds[k * ng + g];
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) r[k] = G.dr[k * ng + g];
+    GpOut o;
+    const int rc = dstrss<NS>(M, C, G, g, gp_iel[g], de, r, st, ds, dt, inc, nit, o);
+    if (rc) {
+        atomicMin(errkey, ((unsigned long long)g << 16) | (unsigned long long)rc);
+        return;
+    }
+    G.dep[g] = o.deff;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) G.ds[k * ng + g] = ds[k];
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int j = 0; j < 6; ++j) chi[(i + 6 * j) * (size_t)ng + g] = o.chi[i][j];
+}
+
+// gaussm (src/fasolt/Elvals.f90:132-220) for node pair (i, j) of one
+// element: gm[r][c] = gaussm(r+1, c+1).  d is the tangent's upper
+// triangle -- the only entries the reference reads.
+__device__ __forceinline__ void gaussm_block(const double ai[3], const double bj[3],
+                                             const double *d, const double s[6], double gm[9])
+{
+#define D(p, q) d[utri((p)-1, (q)-1)]
+#define SS(p) s[(p)-1]
+    const double i1 = ai[0], i2 = ai[1], i3 = ai[2], j1 = bj[0], j2 = bj[1], j3 = bj[2];
+    gm[0] = (i1 * j1 * (D(1, 1) - SS(1)) + i2 * j2 * (D(6, 6) - (SS(1) - SS(2)) / 2.0) +
+             i3 * j3 * (D(5, 5) - (SS(1) - SS(3)) / 2.0) + i2 * j3 * (D(5, 6) + SS(4) / 2.0) +
+             i3 * j1 * (D(1, 5)) + i1 * j2 * (D(1, 6)) + j2 * i3 * (D(5, 6) + SS(4) / 2.0) +
+             j3 * i1 * (D(1, 5)) + j1 * i2 * (D(1, 6)));
+    gm[3] = (i1 * j1 * (D(1, 6) - SS(6)) + i2 * j2 * (D(2, 6) - SS(6)) +
+             i3 * j3 * (D(4, 5) - SS(6) / 2.0) + i2 * j3 * (D(2, 5) - SS(5) / 4.0) +
+             i3 * j1 * (D(1, 4) - SS(4) / 4.0) + i1 * j2 * (D(6, 6) - (SS(1) + SS(2)) / 4.0) +
+             j2 * i3 * (D(4, 6) - SS(5) / 4.0) + j3 * i1 * (D(5, 6) - SS(4) / 4.0) +
+             j1 * i2 * (D(1, 2) - (SS(1) + SS(2)) / 4.0));
+    gm[6] = (i1 * j1 * (D(1, 5) - SS(5)) + i2 * j2 * (D(4, 6) - SS(5) / 2.0) +
+             i3 * j3 * (D(3, 5) - SS(5)) + i2 * j3 * (D(4, 5) - SS(6) / 4.0) +
+             i3 * j1 * (D(1, 3) - (SS(1) + SS(3)) / 4.0) + i1 * j2 * (D(5, 6) - SS(4) / 4.0) +
+             j2 * i3 * (D(3, 6) - SS(6) / 4.0) + j3 * i1 * (D(5, 5) - (SS(1) + SS(3)) / 4.0) +
+             j1 * i2 * (D(1, 4) - SS(4) / 4.0));
+    gm[1] = (j1 * i1 * (D(1, 6) - SS(6)) + j2 * i2 * (D(2, 6) - SS(6)) +
+             j3 * i3 * (D(4, 5) - SS(6) / 2.0) + j2 * i3 * (D(2, 5) - SS(5) / 4.0) +
+             j3 * i1 * (D(1, 4) - SS(4) / 4.0) + j1 * i2 * (D(6, 6) - (SS(1) + SS(2)) / 4.0) +
+             i2 * j3 * (D(4, 6) - SS(5) / 4.0) + i3 * j1 * (D(5, 6) - SS(4) / 4.0) +
+             i1 * j2 * (D(1, 2) - (SS(1) + SS(2)) / 4.0));
+    gm[4] = (i1 * j1 * (D(6, 6) - (SS(2) - SS(1)) / 2.0) + i2 * j2 * (D(2, 2) - SS(2)) +
+             i3 * j3 * (D(4, 4) - (SS(2) - SS(3)) / 2.0) + i2 * j3 * (D(2, 4)) +
+             i3 * j1 * (D(4, 6) + SS(5) / 2.0) + i1 * j2 * (D(2, 6)) + j2 * i3 * (D(2, 4)) +
+             j3 * i1 * (D(4, 6) + SS(5) / 2.0) + j1 * i2 * (D(2, 6)));
+    gm[7] = (i1 * j1 * (D(5, 6) - SS(4) / 2.0) + i2 * j2 * (D(2, 4) - SS(4)) +
+             i3 * j3 * (D(3, 4) - SS(4)) + i2 * j3 * (D(4, 4) - (SS(2) + SS(3)) / 4.0) +
+             i3 * j1 * (D(3, 6) - SS(6) / 4.0) + i1 * j2 * (D(2, 5) - SS(5) / 4.0) +
+             j2 * i3 * (D(2, 3) - (SS(2) + SS(3)) / 4.0) + j3 * i1 * (D(4, 5) - SS(6) / 4.0) +
+             j1 * i2 * (D(4, 6) - SS(5) / 4.0));
+    gm[2] = (j1 * i1 * (D(1, 5) - SS(5)) + j2 * i2 * (D(4, 6) - SS(5) / 2.0) +
+             j3 * i3 * (D(3, 5) - SS(5)) + j2 * i3 * (D(4, 5) - SS(6) / 4.0) +
+             j3 * i1 * (D(1, 3) - (SS(1) + SS(3)) / 4.0) + j1 * i2 * (D(5, 6) - SS(4) / 4.0) +
+             i2 * j3 * (D(3, 6) - SS(6) / 4.0) + i3 * j1 * (D(5, 5) - (SS(1) + SS(3)) / 4.0) +
+             i1 * j2 * (D(1, 4) - SS(4) / 4.0));
+    gm[5] = (j1 * i1 * (D(5, 6) - SS(4) / 2.0) + j2 * i2 * (D(2, 4) - SS(4)) +
+             j3 * i3 * (D(3, 4) - SS(4)) + j2 * i3 * (D(4, 4) - (SS(2) + SS(3)) / 4.0) +
+             j3 * i1 * (D(3, 6) - SS(6) / 4.0) + j1 * i2 * (D(2, 5) - SS(5) / 4.0) +
+             i2 * j3 * (D(2, 3) - (SS(2) + SS(3)) / 4.0) + i3 * j1 * (D(4, 5) - SS(6) / 4.0) +
+             i1 * j2 * (D(4, 6) - SS(5) / 4.0));
+    gm[8] = (i1 * j1 * (D(5, 5) - (SS(3) - SS(1)) / 2.0) +
+             i2 * j2 * (D(4, 4) - (SS(3) - SS(2)) / 2.0) + i3 * j3 * (D(3, 3) - SS(3)) +
+             i2 * j3 * (D(3, 4)) + i3 * j1 * (D(3, 5)) + i1 * j2 * (D(4, 5) + SS(6) / 2.0) +
+             j2 * i3 * (D(3, 4)) + j3 * i1 * (D(3, 5)) + j1 * i2 * (D(4, 5) + SS(6) / 2.0));
+#undef D
+#undef SS
+}
+
+// Penalty boundary condition of one node (SUVALS, src/fasolt/Bconds.f90:40-109)
+// applied to its diagonal block D (row-major 3x3) and right-hand side f.
+__device__ __forceinline__ int apply_bc(int ibc, int n, const double *x, const double *dx,
+                                        const double *xspec, const double *fspec, int nxs,
+                                        int nfs, double efix, double D[9], double f[3])
+{
+    if (ibc < 100) return 0;
+    const int ikin = (ibc / 100) % 100;
+    if (ikin > 0) {
+        if (ikin > nxs) return 1;
+        const double *xs = xspec + (size_t)(ikin - 1) * 15;
+        double xsp[3];
+        if (ikin < 50) {
+            xsp[0] = xs[6];
+            xsp[1] = xs[10];
+            xsp[2] = xs[14];
+        } else {
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                xsp[j] = xs[6 + 3 * j] * (x[3 * n] + dx[3 * n]) +
+                         xs[7 + 3 * j] * (x[3 * n + 1] + dx[3 * n + 1]) +
+                         xs[8 + 3 * j] * (x[3 * n + 2] + dx[3 * n + 2]);
+        }
+        const int point[3][3] = {{0, 1, 3}, {1, 2, 4}, {3, 4, 5}};
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            double sum = 0.0;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const double pen = efix * xs[point[i][j]];
+                D[3 * i + j] = D[3 * i + j] + pen;
+                sum = sum + pen * (dx[3 * n + j] - xsp[j]);
+            }
+            f[i] = f[i] + sum;
+        }
+    }
+    const int ispf = (ibc / 10000) % 100;
+    if (ispf > 0) {
+        if (ispf > nfs) return 1;
+        const double *fs = fspec + (size_t)(ispf - 1) * 3;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) f[i] = f[i] + fs[i];
+    }
+    return 0;
+}
+
+// Row-gather assembly: thread (slot, row) sums, in ascending element order
+// (the reference's scatter order, Elvals.f90:244-262), w * gaussm over the
+// elements that hold both the row node and the slot's column node, and
+// writes the 3x3 block once -- no atomics, no read-modify-write of the
+// matrix.  The diagonal-slot thread also forms the nodal force
+// (Elvals.f90:122-126,265-271) and, when `bc` is set, applies SUVALS.
+__global__ void __launch_bounds__(256) k_assemble(MeshDev Mh, BlockDev B,
+                                                  const double *__restrict__ rec,
+                                                  const double *__restrict__ x,
+                                                  const double *__restrict__ dx, double *fc,
+                                                  double *ddx, const double *xspec,
+                                                  const double *fspec, int nxs, int nfs,
+                                                  double efix, int bc, int *bad_bc)
+{
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int R = B.R;
+    const int s = (int)(tid / R);
+    const int p = (int)(tid - (long long)s * R);
+    if (s >= SLOTS) return;
+    if (s >= B.nslot[p]) return;
+    const int n = B.perm[p];
+    const unsigned bl = B.bloc[s * R + p];
+    const int cnt = Mh.ne_cnt[n];
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double f[3] = {0, 0, 0};
+    for (int k = 0; k < cnt; ++k) {
+        const int b = (bl >> (4 * k)) & 0xF;
+        if (b == 0xF) continue;
+        const int e = Mh.ne_elem[k * Mh.nnod + n];
+        const int a = Mh.ne_loc[k * Mh.nnod + n];
+        const double *Rr = rec + (size_t)e * REC;
+        double sa[3], sb[3], st[6], d[21];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            sa[c] = __ldg(Rr + 3 * a + c);
+            sb[c] = __ldg(Rr + 3 * b + c);
+        }
+#pragma unroll
+        for (int c = 0; c < 6; ++c) st[c] = __ldg(Rr + REC_S + c);
+        const double w = __ldg(Rr + REC_W);
+#pragma unroll
+        for (int c = 0; c < 21; ++c) d[c] = __ldg(Rr + REC_D + c);
+        double gm[9];
+        gaussm_block(sa, sb, d, st, gm);
+#pragma unroll
+        for (int q = 0; q < 9; ++q) acc[q] = acc[q] + w * gm[q];
+        if (s == 0) {
+            f[0] = f[0] + w * (st[0] * sa[0] + st[5] * sa[1] + st[4] * sa[2]);
+            f[1] = f[1] + w * (st[1] * sa[1] + st[3] * sa[2] + st[5] * sa[0]);
+            f[2] = f[2] + w * (st[2] * sa[2] + st[4] * sa[0] + st[3] * sa[1]);
+        }
+    }
+    if (s == 0) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) fc[3 * n + c] = f[c];
+        if (bc) {
+            if (apply_bc(Mh.ib[n], n, x, dx, xspec, fspec, nxs, nfs, efix, acc, f)) *bad_bc = 1;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) ddx[3 * n + c] = f[c];
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) B.blk[(size_t)(s * 9 + q) * R + p] = acc[q];
+}
+
+// Stand-alone SUVALS (src/fasolt/Bconds.f90:19-113): ddx = fc, then the
+// penalty terms of every constrained node.
+__global__ void k_suvals(MeshDev Mh, BlockDev B, const int *rowof, const double *x,
+                         const double *dx, const double *fc, double *ddx, const double *xspec,
+                         const double *fspec, int nxs, int nfs, double efix, int *bad_bc)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= Mh.nnod) return;
+    double f[3] = {fc[3 * n], fc[3 * n + 1], fc[3 * n + 2]};
+    const int ibc = Mh.ib[n];
+    if (ibc >= 100) {
+        const int p = rowof[n];
+        const int R = B.R;
+        double D[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) D[q] = B.blk[(size_t)q * R + p];
+        if (apply_bc(ibc, n, x, dx, xspec, fspec, nxs, nfs, efix, D, f)) *bad_bc = 1;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) B.blk[(size_t)q * R + p] = D[q];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) ddx[3 * n + c] = f[c];
+}
+
+// ---------------------------------------------------------------- reductions
+// Deterministic block sum of NV values per thread; block b writes
+// part[v * nblk + b].
+template <int NV>
+__device__ __forceinline__ void block_sum_store(double v[NV], double *part, int nblk)
+{
+    __shared__ double red[NV][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double t = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        if (lane == 0) red[k][wid] = t;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double t = lane < nw ? red[k][lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+            if (lane == 0) part[k * nblk + blockIdx.x] = t;
+        }
+    }
+}
+
+// Single-block final sum of NV partial vectors of length nblk.
+template <int NV>
+__global__ void __launch_bounds__(1024) k_final_sum(const double *part, int nblk, double *out)
+{
+    double v[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double t = 0.0;
+        for (int i = threadIdx.x; i < nblk; i += blockDim.x) t += part[k * nblk + i];
+        v[k] = t;
+    }
+    __shared__ double red[NV][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double t = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        if (lane == 0) red[k][wid] = t;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double t = lane < nw ? red[k][lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+            if (lane == 0) out[k] = t;
+        }
+    }
+}
+
+// NRITER's norms (src/fasolt/Stif_sol.f90:46-51,56-58,65): sum of rhs^2
+// over nodes with ib < 10, |dx|^2, |ddx|^2, and the CPSTRS error sum.
+__global__ void __launch_bounds__(256) k_nr_norms(int nnod, int ngps, const int *ib,
+                                                  const double *rhs, const double *dx,
+                                                  const double *ddx, const double *erepmd,
+                                                  double *part, int nblk)
+{
+    double v[4] = {0, 0, 0, 0};
+    const int stride = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nnod; i += stride) {
+        const double a = rhs[3 * i], b = rhs[3 * i + 1], c = rhs[3 * i + 2];
+        if (ib[i] < 10) v[0] += a * a + b * b + c * c;
+        const double d0 = dx[3 * i], d1 = dx[3 * i + 1], d2 = dx[3 * i + 2];
+        v[1] += d0 * d0 + d1 * d1 + d2 * d2;
+        const double e0 = ddx[3 * i], e1 = ddx[3 * i + 1], e2 = ddx[3 * i + 2];
+        v[2] += e0 * e0 + e1 * e1 + e2 * e2;
+    }
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngps; g += stride) v[3] += erepmd[g];
+    block_sum_store<4>(v, part, nblk);
+}
+
+// ---------------------------------------------------------------- SOR
+// FACSLS (src/fasolt/Stif_sol.f90:161-215) in multicolour node order: one
+// launch per colour; each thread updates the x, y, z DOFs of one node with
+// point SOR (omega = 1.2) and adds its share of |dx_sweep|^2 and |x|^2.
+struct SorCtl {
+    int conv;       // set once error < toler^2
+    int sweeps;     // sweeps actually performed
+    double err;     // error of the last sweep
+    double pad;
+};
+
+__global__ void __launch_bounds__(256) k_sor_colour(BlockDev B, int p0, int p1,
+                                                    const double *__restrict__ rhs, double *sol,
+                                                    const SorCtl *ctl, double *part, int boff,
+                                                    int nblk_tot)
+{
+    if (((volatile const SorCtl *)ctl)->conv) return;
+    const int p = p0 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int R = B.R;
+    double v[2] = {0.0, 0.0};
+    if (p < p1) {
+        const int n = B.perm[p];
+        const int ns = B.nslot[p];
+        double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+        for (int s = 1; s < ns; ++s) {
+            const int m = B.bcol[s * R + p];
+            const double x0 = sol[3 * m], x1 = sol[3 * m + 1], x2 = sol[3 * m + 2];
+            const double *b = B.blk + (size_t)s * 9 * R + p;
+            acc0 += b[0] * x0 + b[(size_t)R] * x1 + b[2 * (size_t)R] * x2;
+            acc1 += b[3 * (size_t)R] * x0 + b[4 * (size_t)R] * x1 + b[5 * (size_t)R] * x2;
+            acc2 += b[6 * (size_t)R] * x0 + b[7 * (size_t)R] * x1 + b[8 * (size_t)R] * x2;
+        }
+        double D[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) D[q] = B.blk[(size_t)q * R + p];
+        const double o0 = sol[3 * n], o1 = sol[3 * n + 1], o2 = sol[3 * n + 2];
+        double x0 = o0, x1 = o1, x2 = o2;
+        double t = (rhs[3 * n] - (acc0 + D[1] * x1 + D[2] * x2)) / D[0];
+        x0 = x0 + 1.2 * (t - x0);
+        t = (rhs[3 * n + 1] - (acc1 + D[3] * x0 + D[5] * x2)) / D[4];
+        x1 = x1 + 1.2 * (t - x1);
+        t = (rhs[3 * n + 2] - (acc2 + D[6] * x0 + D[7] * x1)) / D[8];
+        x2 = x2 + 1.2 * (t - x2);
+        sol[3 * n] = x0;
+        sol[3 * n + 1] = x1;
+        sol[3 * n + 2] = x2;
+        v[0] = (x0 - o0) * (x0 - o0) + (x1 - o1) * (x1 - o1) + (x2 - o2) * (x2 - o2);
+        v[1] = x0 * x0 + x1 * x1 + x2 * x2;
+    }
+    block_sum_store<2>(v, part + boff, nblk_tot);
+}
+
+// End of one sweep: error = sum(dx^2) / sum(x^2) (Stif_sol.f90:206-210).
+__global__ void __launch_bounds__(1024) k_sor_check(const double *part, int nblk, SorCtl *ctl,
+                                                    double tolerl)
+{
+    if (ctl->conv) return;
+    double v[2] = {0.0, 0.0};
+    for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
+        v[0] += part[i];
+        v[1] += part[nblk + i];
+    }
+    __shared__ double red[2][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        double t = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        if (lane == 0) red[k][wid] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        double a = 0.0, b = 0.0;
+        for (int i = 0; i < nw; ++i) {
+            a += red[0][i];
+            b += red[1][i];
+        }
+        const double err = a / b;
+        ctl->err = err;
+        ctl->sweeps += 1;
+        if (err < tolerl) ctl->conv = 1;
+    }
+}
+
+// 903 test (Stif_sol.f90:183-185): first DOF whose diagonal entry is zero.
+__global__ void k_diag_check(BlockDev B, unsigned long long *firstbad)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= B.R) return;
+    const int n = B.perm[p];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        if (B.blk[(size_t)(4 * c) * B.R + p] == 0.0) atomicMin(firstbad, (unsigned long long)(3 * n + c));
+}
+
+// ---------------------------------------------------------------- updates
+// NRITER's damped correction (Stif_sol.f90:70-74).
+__global__ void k_nr_update(int ndof, double alp2, const double *ddx, double *x, double *dx)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ndof) return;
+    const double xc = alp2 * ddx[i];
+    x[i] = x[i] - xc;
+    dx[i] = dx[i] - xc;
+}
+
+// UPDATE_NODE (src/fasolt/Fasolt3.f90:231-244)
+__global__ void k_update_node(int ndof, double *x, const double *dx)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < ndof) x[i] = x[i] + dx[i];
+}
+
+// cumslip update after the Newton loop (src/fasolt/Stif_sol.f90:80-84)
+__global__ void k_cumslip(DevGp G, int nsc, double tm)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G.ngps) return;
+    for (int k = 0; k < nsc; ++k)
+        G.cumslip[k * G.ngps + g] = G.cumslip[k * G.ngps + g] + (G.srate[k * G.ngps + g] * tm);
+}
+
+// UPDATE_GPTV (src/fasolt/Fasolt3.f90:254-284)
+__global__ void k_update_gptv(DevGp G, int nsv)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G.ngps) return;
+    const int ng = G.ngps;
+    G.eps[g] = G.eps[g] + G.dep[g];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) G.rt[k * ng + g] = G.rt[k * ng + g] + G.dr[k * ng + g];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        G.ep[k * ng + g] = G.ep[k * ng + g] + G.de[k * ng + g];
+        G.st[k * ng + g] = G.st[k * ng + g] + G.ds[k * ng + g];
+    }
+    for (int k = 0; k < nsv; ++k) G.sv[k * ng + g] = G.sv[k * ng + g] + G.dsv[k * ng + g];
+}
+
+// DoReorient (src/fasolt/Fasolt3.f90:79-178): rotate a twinned GP by ssang
+// about n x d of its twin system, using material 1's tables and
+// pi = 3.14159 as the reference does.  Events are appended unordered; the
+// host sorts them by GP.
+struct TwinEv {
+    int gp, sys;
+    double eo[3], en[3];
+};
+
+__global__ void k_reorient(DevGp G, DevMat M, TwinEv *ev, int cap, int *nev)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= G.ngps) return;
+    const int ts = G.twinsys[j];
+    if (ts == 0) return;
+    const int i = ts - 1;
+    const int ng = G.ngps;
+    const double e1 = G.sv[j], e2 = G.sv[ng + j], e3 = G.sv[2 * ng + j];
+    const double ang = M.ssang[i] * 3.14159 / 180.0;
+    double ss1, c1, s2, c2, s3, c3;
+    sincos(e1, &ss1, &c1);
+    sincos(e2, &s2, &c2);
+    sincos(e3, &s3, &c3);
+    double RM[3][3];
+    RM[0][0] = c1 * c3 - c2 * ss1 * s3;
+    RM[0][1] = -c1 * s3 - c2 * c3 * ss1;
+    RM[0][2] = ss1 * s2;
+    RM[1][0] = c3 * ss1 + c1 * c2 * s3;
+    RM[1][1] = c1 * c2 * c3 - ss1 * s3;
+    RM[1][2] = -c1 * s2;
+    RM[2][0] = s2 * s3;
+    RM[2][1] = c3 * s2;
+    RM[2][2] = c2;
+    double nv[3], dv[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        nv[a] = RM[a][0] * M.an[3 * i] + RM[a][1] * M.an[3 * i + 1] + RM[a][2] * M.an[3 * i + 2];
+        dv[a] = RM[a][0] * M.ab[3 * i] + RM[a][1] * M.ab[3 * i + 1] + RM[a][2] * M.ab[3 * i + 2];
+    }
+    const double u1 = nv[1] * dv[2] - nv[2] * dv[1];
+    const double u2 = nv[2] * dv[0] - nv[0] * dv[2];
+    const double u3 = nv[0] * dv[1] - nv[1] * dv[0];
+    double s, c;
+    sincos(ang, &s, &c);
+    double E[3][3];
+    E[0][0] = c + u1 * u1 * (1.0 - c);
+    E[0][1] = u1 * u2 * (1.0 - c) - u3 * s;
+    E[0][2] = u1 * u3 * (1.0 - c) + u2 * s;
+    E[1][0] = u1 * u2 * (1.0 - c) + u3 * s;
+    E[1][1] = c + u2 * u2 * (1.0 - c);
+    E[1][2] = u2 * u3 * (1.0 - c) - u1 * s;
+    E[2][0] = u1 * u3 * (1.0 - c) - u2 * s;
+    E[2][1] = u2 * u3 * (1.0 - c) + u1 * s;
+    E[2][2] = c + u3 * u3 * (1.0 - c);
+    double F[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) F[a][b] = E[a][0] * RM[0][b] + E[a][1] * RM[1][b] + E[a][2] * RM[2][b];
+    const double e1n = atan2(F[0][2], -F[1][2]);
+    double f33 = F[2][2];
+    if (fabs(f33) > 1.0) f33 = f33 / fabs(f33);
+    const double e2n = acos(f33);
+    const double e3n = atan2(F[2][0], F[2][1]);
+    G.sv[j] = e1n;
+    G.sv[ng + j] = e2n;
+    G.sv[2 * ng + j] = e3n;
+    const int slot = atomicAdd(nev, 1);
+    if (slot < cap) {
+        TwinEv &t = ev[slot];
+        t.gp = j;
+        t.sys = i;
+        t.eo[0] = e1; t.eo[1] = e2; t.eo[2] = e3;
+        t.en[0] = e1n; t.en[1] = e2n; t.en[2] = e3n;
+    }
+    G.twinsys[j] = 0;
+    G.timestwinned[j] = G.timestwinned[j] + 1;
+}
+
+// ---------------------------------------------------------------- exports
+// SETPTA (src/fasolt/Stif_sol.f90:98-149) per DOF row: columns in the order
+// of first touch over ascending elements and their local DOFs.  Writes the
+// 1-based reference layout is[row * ld + k]; overflow raises 955.
+__global__ void k_setpta(MeshDev Mh, int ld, int *is, int *overflow)
+{
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= 3 * Mh.nnod) return;
+    const int n = row / 3;
+    int *out = is + (size_t)row * ld;
+    int cnt = 0;
+    for (int k = 0; k < Mh.ne_cnt[n]; ++k) {
+        const int e = Mh.ne_elem[k * Mh.nnod + n];
+        for (int a = 0; a < 8; ++a) {
+            const int m = Mh.ln[a * Mh.nlmnt + e];
+            for (int c = 0; c < 3; ++c) {
+                const int col = 3 * m + c + 1;
+                if (col == row + 1) continue;
+                bool found = false;
+                for (int q = 1; q <= cnt; ++q)
+                    if (out[q] == col) { found = true; break; }
+                if (!found) {
+                    if (cnt + 1 >= ld) { *overflow = 1; return; }
+                    out[++cnt] = col;
+                }
+            }
+        }
+    }
+    out[0] = cnt;
+    for (int q = cnt + 1; q < ld; ++q) out[q] = 0;
+}
+
+// Values of the block matrix in the reference layout ss(ld, ndof).
+__global__ void k_to_ell(BlockDev B, const int *rowof, int nnod, int ld, const int *is, double *ss)
+{
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= 3 * nnod) return;
+    const int n = row / 3, r = row % 3;
+    const int p = rowof[n];
+    const int R = B.R;
+    const int *ir = is + (size_t)row * ld;
+    double *out = ss + (size_t)row * ld;
+    out[0] = B.blk[(size_t)(r * 3 + r) * R + p];
+    for (int k = 1; k <= ir[0]; ++k) {
+        const int col = ir[k] - 1;
+        const int m = col / 3, c = col % 3;
+        int slot = -1;
+        for (int s = 0; s < B.nslot[p]; ++s)
+            if (B.bcol[s * R + p] == m) { slot = s; break; }
+        out[k] = slot >= 0 ? B.blk[(size_t)(slot * 9 + r * 3 + c) * R + p] : 0.0;
+    }
+    for (int k = ir[0] + 1; k < ld; ++k) out[k] = 0.0;
+}
+
+// ---------------------------------------------------------------- state I/O
+// Gather a caller array laid out [g][k] (leading dimension ld, element size
+// rb) into the structure-of-arrays [k][g] FP64 layout, and back.
+__global__ void k_aos_to_soa(const void *src, int rb, int ld, int nk, int n, double *dst)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nk * n) return;
+    const int k = (int)(t / n), g = (int)(t - (long long)k * n);
+    const size_t si = (size_t)g * ld + k;
+    dst[(size_t)k * n + g] = rb == 4 ? (double)((const float *)src)[si] : ((const double *)src)[si];
+}
+
+__global__ void k_soa_to_aos(const double *src, int nk, int n, void *dst, int rb, int ld)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nk * n) return;
+    const int g = (int)(t / nk), k = (int)(t - (long long)g * nk);
+    const double v = src[(size_t)k * n + g];
+    const size_t di = (size_t)g * ld + k;
+    if (rb == 4) ((float *)dst)[di] = (float)v;
+    else ((double *)dst)[di] = v;
+}
+
+}  // namespace fasdev

@@ -1,0 +1,363 @@
+"""Structured-brick problem generator with fs3pre's semantics.
+
+The reference builds its input with the interactive pre-processor ``fs3pre``
+(src/prepro/fs3pre.f90) and writes a ``.fsd`` file.  This module produces the
+same tables directly, for 8-node one-Gauss-point bricks (``lt = 12``):
+
+* elements in (z, y, x) loop order with ADDEL_8NQ's local node order
+  (src/prepro/fs3pre.f90:183-233);
+* node numbers in first-occurrence order, which is what SWEEP's duplicate
+  removal leaves (src/prepro/fs3p-swp.f90:53-109), computed with one sort
+  instead of the O(nnod^2) sweep;
+* SETBOUNDS codes for the four ``xfree`` options (src/prepro/fs3p-bkc.f90:9-174);
+* SETKINC loading tables (src/prepro/fs3p-bkc.f90:182-308);
+* random orientations per grain with fs3pre's uniform-SO(3) formulas
+  (src/prepro/fs3p-gps.f90:105-110), seeded; grains are g x g x g blocks;
+* SETMATC's equal initial slip resistance (src/prepro/fs3p-matl.f90:106-125).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import abi
+from .problem import Control, Problem
+
+# ADDEL_8NQ local node offsets (fs3pre.f90:193-196)
+BRICK8 = np.array([(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0),
+                   (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)], dtype=np.int64)
+
+
+# ----------------------------------------------------------------- materials
+def cubic_compliance(c11: float, c12: float, c44: float) -> np.ndarray:
+    """e(1:9) = S11,S22,S33,S23,S31,S12,S44,S55,S66 (1/MPa) of a cubic crystal
+    from stiffnesses in MPa (the .fmt compliance line, ela-plas.f90:56-74)."""
+    d = (c11 - c12) * (c11 + 2.0 * c12)
+    s11 = (c11 + c12) / d
+    s12 = -c12 / d
+    s44 = 1.0 / c44
+    return np.array([s11, s11, s11, s12, s12, s12, s44, s44, s44])
+
+
+def fcc_systems() -> tuple[np.ndarray, np.ndarray]:
+    """The 12 {111}<110> systems in the order of src/prepro/crysdat.f90 and
+    sample_input_files/aluminium2.fmt: three directions on each of the
+    planes (111), (11-1), (-111), (1-11)."""
+    planes = [(1, 1, 1), (1, 1, -1), (-1, 1, 1), (1, -1, 1)]
+    dirs = [[(0, 1, -1), (-1, 0, 1), (1, -1, 0)],
+            [(0, 1, 1), (-1, 0, -1), (1, -1, 0)],
+            [(0, 1, -1), (1, 0, 1), (-1, -1, 0)],
+            [(0, -1, -1), (-1, 0, 1), (1, 1, 0)]]
+    ab, an = [], []
+    for p, ds in zip(planes, dirs):
+        for d in ds:
+            assert sum(a * b for a, b in zip(p, d)) == 0
+            ab.append(np.array(d, float) / math.sqrt(2.0))
+            an.append(np.array(p, float) / math.sqrt(3.0))
+    return np.array(ab), np.array(an)
+
+
+def fcc_aluminium(m: float = 0.05, h0: float = 150.0, tau_sat: float = 80.0,
+                  c11=108.2e3, c12=61.3e3, c44=28.5e3) -> dict:
+    """FCC aluminium: power-law flow with exponent 1/m, Voce hardening
+    theta = h0 (1 - s/tau_sat) (PLASTC with A3 = 0, A4 = 1, A6 = 0,
+    ela-plas.f90:127-170) and a latent matrix of ones."""
+    ab, an = fcc_systems()
+    ns = 12
+    ampar = np.zeros((ns, 10))
+    ampar[:, 0] = m
+    ampar[:, 1] = h0
+    ampar[:, 2] = 0.0
+    ampar[:, 3] = 1.0
+    ampar[:, 4] = tau_sat
+    ampar[:, 5] = 0.0
+    return dict(name="fcc-al", ns=ns, e=cubic_compliance(c11, c12, c44),
+                ssang=np.zeros(ns), ab=ab, an=an, ampar=ampar,
+                smatrx=np.ones((ns, ns)))
+
+
+def pack_materials(mats: list[dict]):
+    """Material tables in the FAS_CPL layout (ld_ss = 60)."""
+    nm = len(mats)
+    L = abi.FAS_MAXSS
+    nss = np.array([m["ns"] for m in mats], np.int32)
+    e = np.zeros((nm, 9))
+    ssang = np.zeros((nm, L))
+    ab = np.zeros((nm, L, 3))
+    an = np.zeros((nm, L, 3))
+    ampar = np.zeros((nm, L, 10))
+    smatrx = np.zeros((nm, L, L))
+    for k, m in enumerate(mats):
+        ns = m["ns"]
+        e[k] = m["e"]
+        ssang[k, :ns] = m["ssang"]
+        ab[k, :ns] = m["ab"]
+        an[k, :ns] = m["an"]
+        ampar[k, :ns] = m["ampar"]
+        # smatrx(i, j, k) lives at [k, j, i]
+        smatrx[k, :ns, :ns] = np.asarray(m["smatrx"]).T
+    return nss, e, ssang, ab, an, ampar, smatrx
+
+
+# ----------------------------------------------------------------- boundary codes
+_FULL = {1: 100, 4: 200, 16: 300, 5: 400, 17: 500, 20: 600, 21: 700,
+         2: 800, 8: 900, 32: 1000, 10: 1100, 34: 1200, 40: 1300, 42: 1400,
+         9: 1500, 33: 1600, 6: 1700, 36: 1800, 18: 1900, 24: 2000,
+         26: 2100, 38: 2200, 41: 2300, 37: 2400, 25: 2500, 22: 2600}
+_FREEX = {1: 1, 2: 1, 5: 200, 6: 200, 9: 900, 10: 900, 17: 300, 18: 300,
+          33: 1000, 34: 1000, 22: 600, 25: 2000, 26: 2000, 37: 1800, 38: 1800,
+          41: 1300, 42: 1300}
+_JUSTX = {**{k: 1 for k in (4, 8, 16, 20, 24, 32, 36, 40)},
+          **{k: 100 for k in (1, 5, 9, 17, 25, 33, 37, 41)},
+          **{k: 800 for k in (6, 10, 18, 22, 26, 34, 38, 42)}}
+
+
+def setbounds(x: np.ndarray, tolerance: float, xfree: int) -> np.ndarray:
+    """SETBOUNDS, src/prepro/fs3p-bkc.f90:9-174."""
+    xyz = x.reshape(-1, 3)
+    lo, hi = xyz.min(axis=0), xyz.max(axis=0)
+    ib = np.zeros(xyz.shape[0], np.int32)
+    for i in range(xyz.shape[0]):
+        side = 0
+        for j in range(3):
+            if abs(xyz[i, j] - lo[j]) < tolerance:
+                side += 2 ** (2 * j)
+            if abs(xyz[i, j] - hi[j]) < tolerance:
+                side += 2 ** (2 * j + 1)
+        if side == 0:
+            continue
+        code = _FULL.get(side, 1)
+        if xfree == 0:
+            code = 5000
+        elif xfree == 2:
+            code = _FREEX.get(side, code)
+        elif xfree == 3:
+            code = _JUSTX.get(side, code)
+        ib[i] = code
+    return ib
+
+
+def setkinc(xl, xfree: int, eps_inc, ninc1: int):
+    """SETKINC, src/prepro/fs3p-bkc.f90:182-308: tiem and x_spec tables.
+    `eps_inc` = (e11, e22, e33) increments; components the chosen `xfree`
+    does not read are ignored as fs3pre ignores them."""
+    ex, ey, ez = (float(v) for v in eps_inc)
+    if xfree == 2:
+        ex = 0.0
+    elif xfree == 3:
+        ey = ez = 0.0
+    tiem = np.zeros(ninc1)
+    xs = np.zeros((ninc1, abi.XSLD, 15))
+    masks = {1: (1, 0, 0, 0, 0, 0), 2: (0, 0, 1, 0, 0, 0), 3: (0, 0, 0, 0, 0, 1),
+             4: (1, 0, 1, 0, 0, 0), 5: (1, 0, 0, 0, 0, 1), 6: (0, 0, 1, 0, 0, 1),
+             7: (1, 0, 1, 0, 0, 1)}
+    for k in range(8, 15):
+        masks[k] = masks[k - 7]
+    for k, mk in zip(range(15, 21), (4, 5, 4, 6, 5, 6)):
+        masks[k] = masks[mk]
+    for k in range(21, 27):
+        masks[k] = masks[7]
+    xc, yc, zc = (float(v) for v in xl)
+    for i in range(ninc1):
+        tiem[i] = math.sqrt(ex ** 2 + ey ** 2 + ez ** 2)
+        for code, mk in masks.items():
+            xs[i, code - 1, :6] = mk
+        dxs, dys, dzs = ex * xc, ey * yc, ez * zc
+        xc, yc, zc = xc + dxs, yc + dys, zc + dzs
+        for code in (8, 11, 12, 14, 17, 19, 21, 22, 26):
+            xs[i, code - 1, 6] = dxs
+        for code in (9, 11, 13, 14, 15, 20, 21, 23, 25):
+            xs[i, code - 1, 10] = dys
+        for code in (10, 12, 13, 14, 16, 18, 22, 23, 24):
+            xs[i, code - 1, 14] = dzs
+        xs[i, 49, :6] = (1, 0, 1, 0, 0, 1)
+        xs[i, 49, 6] = ex
+        xs[i, 49, 8] = 0.0
+        xs[i, 49, 10] = ey
+        xs[i, 49, 14] = ez
+    return tiem, xs
+
+
+# ----------------------------------------------------------------- the cube
+def structured_cube(n=(8, 8, 8), lengths=(1.0, 1.0, 1.0), xfree: int = 3,
+                    eps_inc=(1.0e-3, 0.0, 0.0), ninc: int = 10, grain: int = 1,
+                    materials: list[dict] | None = None, fractions=None,
+                    tau0: float | list[float] = 25.0, seed: int = 0,
+                    twinlim: int = 0, twinprob: float = 0.0,
+                    ctrl: Control | None = None) -> Problem:
+    """An nx x ny x nz brick of 8-node bricks with fs3pre's numbering, boundary
+    codes, loading and per-grain random orientations (see module docstring).
+
+    `grain` = edge of the cubic grains in elements.  With several materials,
+    each grain draws its material from `fractions` (fs3p-matl.f90:33-57
+    draws per element; here per grain so grains stay single-phase)."""
+    nx, ny, nz = (int(v) for v in n)
+    materials = materials or [fcc_aluminium()]
+    nel = nx * ny * nz
+    dxl = np.array([lengths[0] / nx, lengths[1] / ny, lengths[2] / nz])
+    iz, iy, ix = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    ix, iy, iz = ix.ravel(), iy.ravel(), iz.ravel()          # element order: x fastest
+    gx = ix[:, None] + BRICK8[None, :, 0]
+    gy = iy[:, None] + BRICK8[None, :, 1]
+    gz = iz[:, None] + BRICK8[None, :, 2]
+    key = (gx + (nx + 1) * (gy + (ny + 1) * gz)).ravel()
+    uniq, first, inv = np.unique(key, return_index=True, return_inverse=True)
+    order = np.argsort(first, kind="stable")
+    rank = np.empty_like(order)
+    rank[order] = np.arange(order.size)
+    ln = (rank[inv].reshape(nel, 8) + 1).astype(np.int32)
+    nnod = uniq.size
+    # coordinates from the first-occurrence element: x0 + delx * xyz
+    fo = first[order]
+    fe, fa = fo // 8, fo % 8
+    x0 = np.stack([dxl[0] * ix[fe], dxl[1] * iy[fe], dxl[2] * iz[fe]], axis=1)
+    xyz = x0 + dxl[None, :] * BRICK8[fa]
+    x = np.ascontiguousarray(xyz.reshape(-1))
+    tolerance = 0.5 * float(dxl.min())       # SETSWTOL: 0.5 * shortest distance
+    ib = setbounds(x, tolerance, xfree)
+
+    rng = np.random.default_rng(seed)
+    gxn, gyn, gzn = -(-nx // grain), -(-ny // grain), -(-nz // grain)
+    ngr = gxn * gyn * gzn
+    grain_id = (ix // grain) + gxn * ((iy // grain) + gyn * (iz // grain))
+    u = rng.random((ngr, 3))
+    euler = np.stack([6.2832 * u[:, 0], np.arccos(2.0 * u[:, 1] - 1.0), 6.2832 * u[:, 2]], axis=1)
+    nm = len(materials)
+    if nm > 1:
+        fr = np.asarray(fractions if fractions is not None else [1.0] * nm, float)
+        cum = np.cumsum(fr / fr.sum())
+        r = rng.random(ngr)
+        grain_mat = 1 + np.sum(r[:, None] > cum[None, :-1], axis=1)
+    else:
+        grain_mat = np.ones(ngr, np.int64)
+    le = grain_mat[grain_id].astype(np.int32)
+
+    nss, e, ssang, ab, an, ampar, smatrx = pack_materials(materials)
+    tiem, x_spec = setkinc(lengths, xfree, eps_inc, ninc)
+    nsv = 3 + int(nss.max())
+    prob = Problem(
+        nlmnt=nel, nnod=nnod, ngps=nel, le=le, lt=np.full(nel, 12, np.int32),
+        nd=np.full(nel, 8, np.int32), np_=np.ones(nel, np.int32), ln=ln,
+        lg=np.arange(1, nel + 1, dtype=np.int32).reshape(nel, 1), ib=ib,
+        nss=nss, e=e, ssang=ssang, ab=ab, an=an, ampar=ampar, smatrx=smatrx,
+        nmpar=6, twinlim=twinlim, twinprob=twinprob, tiem=tiem, x_spec=x_spec,
+        f_spec=np.zeros((ninc, abi.XSLD, 3)), nxs=50, nfs=0,
+        ctrl=ctrl or Control(), nsv=nsv)
+    prob.zero_state()
+    prob.x[:] = x
+    prob.sv[:, 0:3] = euler[grain_id]
+    t0 = np.broadcast_to(np.asarray(tau0, float), (nm,))
+    for k in range(nm):
+        sel = le == k + 1
+        prob.sv[sel, 3:3 + nss[k]] = t0[k]
+    prob.meta.update(dict(n=(nx, ny, nz), lengths=tuple(lengths), xfree=xfree, grain=grain,
+                          seed=seed, grain_id=grain_id.astype(np.int32),
+                          materials=[m["name"] for m in materials]))
+    return prob
+
+
+def point_batch(npts: int, seed: int = 1, tau0: float = 25.0, strain_norm: float = 1.0e-3,
+                material: dict | None = None, ctrl: Control | None = None) -> Problem:
+    """Mesh-free batch of independent FCC material points (the constitutive
+    micro-benchmark): uniform-SO(3) orientations, Gaussian strain increments
+    rescaled to Frobenius norm `strain_norm`, CRSS uniform in [tau0, 2 tau0],
+    zero spin and start stress, and the stress increment seeded with the
+    elastic predictor S^-1 de so the plastic branch of DSTRSS runs."""
+    material = material or fcc_aluminium()
+    rng = np.random.default_rng(seed)
+    nss, e, ssang, ab, an, ampar, smatrx = pack_materials([material])
+    ns = int(nss[0])
+    u = rng.random((npts, 3))
+    euler = np.stack([6.2832 * u[:, 0], np.arccos(2.0 * u[:, 1] - 1.0), 6.2832 * u[:, 2]], axis=1)
+    g = rng.standard_normal((npts, 3, 3))
+    g = 0.5 * (g + g.transpose(0, 2, 1))
+    g *= strain_norm / np.linalg.norm(g, axis=(1, 2))[:, None, None]
+    de = np.stack([g[:, 0, 0], g[:, 1, 1], g[:, 2, 2],
+                   2 * g[:, 1, 2], 2 * g[:, 2, 0], 2 * g[:, 0, 1]], axis=1)
+    tiem = np.full(1, strain_norm)
+    prob = Problem(
+        nlmnt=0, nnod=0, ngps=npts, le=np.ones(npts, np.int32), lt=np.zeros(0, np.int32),
+        nd=np.zeros(0, np.int32), np_=np.zeros(0, np.int32), ln=np.zeros((0, 8), np.int32),
+        lg=np.zeros((0, 1), np.int32), ib=np.zeros(0, np.int32),
+        nss=nss, e=e, ssang=ssang, ab=ab, an=an, ampar=ampar, smatrx=smatrx,
+        nmpar=6, twinlim=0, twinprob=0.0, tiem=tiem,
+        x_spec=np.zeros((1, abi.XSLD, 15)), f_spec=np.zeros((1, abi.XSLD, 3)),
+        nxs=0, nfs=0, ctrl=ctrl or Control(), nsv=3 + ns)
+    prob.zero_state()
+    prob.sv[:, 0:3] = euler
+    prob.sv[:, 3:3 + ns] = tau0 * (1.0 + rng.random((npts, ns)))
+    prob.de[:] = de
+    # elastic predictor in the rotated crystal frame
+    prob.ds[:] = elastic_predictor(e[0], euler, de)
+    return prob
+
+
+def rotated_compliance(e9: np.ndarray, euler: np.ndarray) -> np.ndarray:
+    """Vectorised ELASTC (ela-plas.f90:12-86) for many orientations:
+    [n, 6, 6] compliances with engineering shears."""
+    ph1, phi, ph2 = euler[:, 0], euler[:, 1], euler[:, 2]
+    c1, s1, c2, s2, c, s = np.cos(ph1), np.sin(ph1), np.cos(ph2), np.sin(ph2), np.cos(phi), np.sin(phi)
+    a = np.zeros((euler.shape[0], 3, 3))
+    a[:, 0, 0] = c1 * c2 - s1 * s2 * c
+    a[:, 1, 0] = -c1 * s2 - s1 * c2 * c
+    a[:, 2, 0] = s1 * s
+    a[:, 0, 1] = s1 * c2 + c1 * s2 * c
+    a[:, 1, 1] = -s1 * s2 + c1 * c2 * c
+    a[:, 2, 1] = -c1 * s
+    a[:, 0, 2] = s2 * s
+    a[:, 1, 2] = c2 * s
+    a[:, 2, 2] = c
+    at = a.transpose(0, 2, 1)
+    pi = [0, 1, 2, 1, 2, 0]
+    pj = [0, 1, 2, 2, 0, 1]
+    S = np.zeros((euler.shape[0], 6, 6))
+    for I in range(6):
+        i, j = pi[I], pj[I]
+        mult = 1.0 if I < 3 else 2.0
+        for J in range(6):
+            k, l = pi[J], pj[J]
+            A = lambda p, q: at[:, p, q]
+            t1 = (A(i, 0) * A(j, 0) * A(k, 0) * A(l, 0) * e9[0] + A(i, 1) * A(j, 1) * A(k, 1) * A(l, 1) * e9[1]
+                  + A(i, 2) * A(j, 2) * A(k, 2) * A(l, 2) * e9[2])
+            t2 = (A(i, 1) * A(j, 1) * A(k, 2) * A(l, 2) * e9[3] + A(i, 2) * A(j, 2) * A(k, 1) * A(l, 1) * e9[3]
+                  + A(i, 2) * A(j, 2) * A(k, 0) * A(l, 0) * e9[4] + A(i, 0) * A(j, 0) * A(k, 2) * A(l, 2) * e9[4]
+                  + A(i, 0) * A(j, 0) * A(k, 1) * A(l, 1) * e9[5] + A(i, 1) * A(j, 1) * A(k, 0) * A(l, 0) * e9[5])
+            t3 = (A(i, 1) * A(j, 2) * A(k, 1) * A(l, 2) * e9[6] + A(i, 2) * A(j, 1) * A(k, 2) * A(l, 1) * e9[6]
+                  + A(i, 2) * A(j, 0) * A(k, 2) * A(l, 0) * e9[7] + A(i, 0) * A(j, 2) * A(k, 0) * A(l, 2) * e9[7]
+                  + A(i, 0) * A(j, 1) * A(k, 0) * A(l, 1) * e9[8] + A(i, 1) * A(j, 0) * A(k, 1) * A(l, 0) * e9[8])
+            S[:, I, J] = mult * (t1 + t2 + 0.5 * t3)
+    iu = np.triu_indices(6, 1)
+    S[:, iu[1], iu[0]] = S[:, iu[0], iu[1]]
+    return S
+
+
+def elastic_predictor(e9: np.ndarray, euler: np.ndarray, de: np.ndarray) -> np.ndarray:
+    S = rotated_compliance(e9, euler)
+    return np.linalg.solve(S, de[:, :, None])[:, :, 0]
+
+
+# ----------------------------------------------------------------- named workloads
+def cube_config(n: int, ninc: int, grain: int, seed: int, eps: float = 1.0e-3,
+                ctrl: Control | None = None) -> Problem:
+    """FCC aluminium n^3 cube in uniaxial tension along x ("just x faces",
+    xfree = 3), strain increment `eps` per increment, grains of grain^3
+    elements with seeded uniform-SO(3) orientations."""
+    return structured_cube(n=(n, n, n), xfree=3, eps_inc=(eps, 0.0, 0.0), ninc=ninc,
+                           grain=grain, seed=seed, ctrl=ctrl)
+
+
+WORKLOADS = {
+    # 8^3 FCC, one grain per element, 10 increments to 1 %
+    "cube8": dict(n=8, ninc=10, grain=1, seed=8),
+    # 16^3 FCC, 20 increments to 2 %
+    "cube16": dict(n=16, ninc=20, grain=1, seed=16),
+    # 64^3 FCC, grains of 2^3 elements, 50 increments to 5 %
+    "cube64": dict(n=64, ninc=50, grain=2, seed=64),
+}
+
+
+def workload(name: str, **over) -> Problem:
+    kw = dict(WORKLOADS[name])
+    kw.update(over)
+    return cube_config(**kw)

@@ -1,0 +1,206 @@
+"""Python face of the C ABI, with the reference's routine names.
+
+:class:`GpuSolver` drives ``libfasgpu.so`` (the sm_100a implementation) the
+way the Fortran driver (src/fasolt/Fasolt3.f90:38-60) drives its routines:
+``update_node``, ``nriter``, ``update_gptv``, ``do_reorient`` per increment,
+or the finer ``elvals`` / ``suvals`` / ``facsls`` steps of NRITER
+(src/fasolt/Stif_sol.f90:10-88).  A non-zero status raises
+:class:`~cpfem_code_b200.abi.FasError` carrying the FAFERR code the reference
+would have raised.  There is no CPU fallback: without the built library or
+without a B200 the constructor raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from .problem import Problem
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libfasgpu.so")
+_lib = None
+
+
+def load_library(path: str | None = None) -> C.CDLL:
+    """Load the device library once.  Raises if it has not been built."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(
+            f"{p} is missing: build it with `python -m cpfem_code_b200.build` "
+            "(the GPU path has no CPU fallback)")
+    lib = C.CDLL(p)
+    abi.declare(lib, "fas_gpu")
+    if path is None:
+        _lib = lib
+    return lib
+
+
+class _SolverBase:
+    """Shared driver logic over a library with the fasolt_gpu.h signatures."""
+
+    prefix = "fas_gpu"
+
+    def __init__(self, lib: C.CDLL, prob: Problem, handle: C.c_void_p):
+        self._lib = lib
+        self.prob = prob
+        self._h = handle
+        self._fn = lambda name: getattr(self._lib, f"{self.prefix}_{name}")
+
+    # ---- lifecycle
+    def close(self) -> None:
+        if self._h:
+            self._fn("destroy")(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _call(self, name: str, *args) -> int:
+        if not self._h:
+            raise abi.FasError(abi.FAS_E_STATE, name)
+        return abi.check(self._fn(name)(self._h, *args), f"{self.prefix}_{name}")
+
+    def set_mode(self, mode: int) -> None:
+        self._call("set_mode", C.c_uint32(mode))
+
+    # ---- state transfer
+    def upload(self, prob: Problem | None = None) -> None:
+        p = prob or self.prob
+        self._call("upload_state", C.byref(p.state_descriptor()))
+
+    def download(self, prob: Problem | None = None) -> Problem:
+        p = prob or self.prob
+        self._call("download_state", C.byref(p.state_descriptor()))
+        return p
+
+    # ---- reference routines
+    def update_node(self) -> None:
+        self._call("update_node")
+
+    def elvals(self, inc: int, nit: int = 1) -> None:
+        self._call("elvals", inc, nit)
+
+    def suvals(self, inc: int) -> None:
+        self._call("suvals", inc)
+
+    def facsls(self) -> tuple[int, float]:
+        sweeps, err = C.c_int32(0), C.c_double(0.0)
+        self._call("facsls", C.byref(sweeps), C.byref(err))
+        return sweeps.value, err.value
+
+    def nriter(self, inc: int, cap: int = 128) -> list[dict]:
+        rep = (abi.FasIterReport * cap)()
+        n = C.c_int32(0)
+        try:
+            self._call("nriter", inc, rep, cap, C.byref(n))
+        finally:
+            self.last_report = _report(rep, min(n.value, cap))
+        return self.last_report
+
+    def update_gptv(self) -> None:
+        self._call("update_gptv")
+
+    def do_reorient(self, inc: int, cap: int = 65536) -> list[dict]:
+        ev = (abi.FasTwinEvent * cap)()
+        n = C.c_int32(0)
+        self._call("reorient", inc, ev, cap, C.byref(n))
+        return _events(ev, min(n.value, cap))
+
+    def increment(self, inc: int, cap: int = 128, ev_cap: int = 65536):
+        """UPDATE_NODE -> NRITER -> UPDATE_GPTV -> DoReorient (when a twin
+        fired): one pass of the driver loop, src/fasolt/Fasolt3.f90:38-46."""
+        rep = (abi.FasIterReport * cap)()
+        ev = (abi.FasTwinEvent * ev_cap)()
+        n, nev = C.c_int32(0), C.c_int32(0)
+        try:
+            self._call("increment", inc, rep, cap, C.byref(n), ev, ev_cap, C.byref(nev))
+        finally:
+            self.last_report = _report(rep, min(n.value, cap))
+        return self.last_report, _events(ev, min(nev.value, ev_cap))
+
+    def constitutive(self, inc: int = 1, nit: int = 1) -> None:
+        self._call("constitutive", inc, nit)
+
+    # ---- inspection
+    def pattern(self, ld: int = 96) -> np.ndarray:
+        """SETPTA's `is` array, [3*nnod, ld] (== is(ld, 3*nnod)), 1-based."""
+        out = np.zeros((3 * self.prob.nnod, ld), np.int32)
+        self._call("get_pattern", abi.iptr(out), ld)
+        return out
+
+    def stiffness(self, ld: int = 96) -> np.ndarray:
+        out = np.zeros((3 * self.prob.nnod, ld), np.float64)
+        self._call("get_stiffness", abi.ptr(out), ld, 8)
+        return out
+
+    def colouring(self) -> tuple[np.ndarray, int]:
+        col = np.zeros(self.prob.nnod, np.int32)
+        n = C.c_int32(0)
+        self._call("get_colouring", abi.iptr(col), C.byref(n))
+        return col, n.value
+
+    def tangent(self) -> np.ndarray:
+        """chi(6,6,ngps) as [ngps, 6(col), 6(row)]."""
+        out = np.zeros((self.prob.ngps, 6, 6), np.float64)
+        self._call("get_tangent", abi.ptr(out), 8)
+        return out
+
+    def cp_ops(self) -> np.ndarray:
+        out = np.zeros(self.prob.ngps, np.float64)
+        self._call("get_cp_ops", out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out
+
+    def cp_stats(self) -> tuple[np.ndarray, np.ndarray]:
+        it = np.zeros(self.prob.ngps, np.int32)
+        er = np.zeros(self.prob.ngps, np.float64)
+        self._call("get_cp_stats", abi.iptr(it),
+                   er.ctypes.data_as(C.POINTER(C.c_double)))
+        return it, er
+
+
+def _report(rep, n) -> list[dict]:
+    return [dict(nit=r.nit, sor_sweeps=r.sor_sweeps, sdx=r.sdx, sfc=r.sfc,
+                 cp_err=r.cp_err, alp2=r.alp2, sor_error=r.sor_error) for r in rep[:n]]
+
+
+def _events(ev, n) -> list[dict]:
+    return [dict(inc=e.inc, gp=e.gp, sys=e.sys, euler_old=tuple(e.euler_old),
+                 euler_new=tuple(e.euler_new)) for e in ev[:n]]
+
+
+class GpuSolver(_SolverBase):
+    """One problem resident on the B200 (state uploaded on construction)."""
+
+    prefix = "fas_gpu"
+
+    def __init__(self, prob: Problem, mode: int = abi.FAS_MODE_PLAIN, upload: bool = True):
+        lib = load_library()
+        mesh, matl, ctrl = prob.descriptors()
+        h = C.c_void_p()
+        abi.check(lib.fas_gpu_create(C.byref(mesh), C.byref(matl), C.byref(ctrl),
+                                     C.c_uint32(mode), C.byref(h)), "fas_gpu_create")
+        super().__init__(lib, prob, h)
+        if upload:
+            self.upload()
+
+    def profile(self, enable: bool) -> dict:
+        """Start (True) or stop (False) device-side phase timing; returns the
+        counters gathered since the last start."""
+        out = abi.FasProfile()
+        self._call("profile", 1 if enable else 0, C.byref(out))
+        return out.as_dict()

@@ -1,0 +1,257 @@
+/*
+ * fasolt_gpu.h -- C ABI of the B200 (sm_100a) implementation of FASOLT3's
+ * per-increment hot path: the crystal-plasticity Gauss-point update, element
+ * assembly, penalty boundary conditions, SOR solve and the increment commit.
+ *
+ * The Fortran driver (src/fasolt/Fasolt3.f90) keeps its module arrays
+ * (FAS_COM / FAS_CPL in src/fasolt/fas-com-mod.f90:9-43,54-80) and reaches
+ * this library through ISO_C_BINDING.  Every pointer below may point straight
+ * at a Fortran module array: arrays are column-major with explicit leading
+ * dimensions, index arrays are 1-based, and reals are REAL(4) or REAL(8) as
+ * the caller says in `real_bytes`.  Nothing crosses this boundary as a C++ or
+ * torch type.
+ *
+ * Return codes of every `int32_t` entry point:
+ *    0                 success
+ *  > 0                 the reference's own FAFERR code, raised at the point
+ *                      where the reference would raise it (first failing
+ *                      element / DOF in the reference's loop order):
+ *                      903 zero SOR diagonal, 904 SOR not converged,
+ *                      905 rotation increment too large, 906 strain increment
+ *                      too large, 910 singular local Jacobian, 920 element
+ *                      weight too small, 987 slip Newton failed (tauerr>0.5)
+ *  < 0                 FAS_E_* errors of this ABI (bad argument, no sm_100
+ *                      device, CUDA failure, unsupported element type).
+ * There is no CPU fallback: without an sm_100 device fas_gpu_create returns
+ * FAS_E_NODEVICE.
+ */
+#ifndef FASOLT_GPU_H
+#define FASOLT_GPU_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FAS_API __attribute__((visibility("default")))
+#else
+#define FAS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes of the ABI itself (reference FAFERR codes are > 0) ---- */
+#define FAS_OK              0
+#define FAS_E_ARG          (-1)  /* null / inconsistent argument            */
+#define FAS_E_NODEVICE     (-2)  /* no sm_100 (B200) device visible          */
+#define FAS_E_CUDA         (-3)  /* a CUDA runtime call failed               */
+#define FAS_E_ELTYPE       (-4)  /* element type not implemented (lt != 12) */
+#define FAS_E_NOMEM        (-5)  /* device allocation failed                 */
+#define FAS_E_RANGE        (-6)  /* size beyond a documented maximum         */
+#define FAS_E_STATE        (-7)  /* call out of order (e.g. no state yet)    */
+
+#define FAS_MAXSS  60            /* maxss, src/fasolt/fas-com-mod.f90:57     */
+
+/* ---- mode flags for fas_gpu_create / fas_gpu_set_mode ------------------ */
+#define FAS_MODE_PLAIN        0u  /* FP64 everywhere, reference tangent      */
+#define FAS_MODE_SOR_FP32     1u  /* SOR sweeps on an FP32 copy of the
+                                     matrix with FP64 residual refinement   */
+#define FAS_MODE_SOR_NATURAL  2u  /* (oracle only) natural-order SOR        */
+
+/*
+ * Mesh: the FAS_COM element and node tables.
+ * Replaces the element/node arrays read by RDDATA
+ * (src/fasolt/Faslt_io_nowin.f90:36-53).  ln(1:ld_ln,1:nlmnt) and
+ * lg(1:ld_lg,1:nlmnt) are Fortran column-major with 1-based ids.
+ * nlmnt == 0 makes a mesh-free "point batch" of ngps independent Gauss
+ * points; `le` then holds one material code per point (length ngps).
+ */
+typedef struct fas_mesh_desc {
+    int32_t nlmnt, nnod, ngps;
+    const int32_t *le, *lt, *nd, *np;    /* [nlmnt]                        */
+    const int32_t *ln;  int32_t ld_ln;   /* node ids, ln(ld_ln, nlmnt)     */
+    const int32_t *lg;  int32_t ld_lg;   /* GP ids,   lg(ld_lg, nlmnt)     */
+    const int32_t *ib;                   /* [nnod] boundary codes ccbbaa   */
+} fas_mesh_desc;
+
+/*
+ * Materials: the FAS_CPL tables (src/fasolt/fas-com-mod.f90:59-78), as read
+ * by RDDATA (src/fasolt/Faslt_io_nowin.f90:66-116).
+ */
+typedef struct fas_matl_desc {
+    int32_t real_bytes;                  /* 4 (REAL(4)) or 8 (REAL(8))     */
+    int32_t nmatl, nmpar;
+    int32_t ld_ss;                       /* leading dim of the ss tables
+                                            (maxss = 60 in the reference)  */
+    const int32_t *nss;                  /* [nmatl]                        */
+    const void *e;                       /* e(9, nmatl) compliances 1/MPa  */
+    const void *ssang;                   /* ssang(ld_ss, nmatl) degrees    */
+    const void *ab, *an;                 /* (3, ld_ss, nmatl)              */
+    const void *ampar;                   /* ampar(10, ld_ss, nmatl)        */
+    const void *smatrx;                  /* smatrx(ld_ss, ld_ss, nmatl)    */
+    int32_t twinlim;
+    double  twinprob;
+} fas_matl_desc;
+
+/*
+ * Control: fafcdf.dat scalars read by FSINIT (src/fasolt/Fasolt3.f90:216-218)
+ * and the per-increment loading read by RDDATA
+ * (src/fasolt/Faslt_io_nowin.f90:123-138).
+ */
+typedef struct fas_ctrl_desc {
+    int32_t real_bytes;                  /* element size of tiem/x/f_spec  */
+    int32_t maxit;
+    double  toler, alpha, afactor, efix, smale, smalr;
+    int32_t ninc1, nxs, nfs;
+    int32_t ld_xs;                       /* 2nd dim of x_spec/f_spec (99)  */
+    const void *tiem;                    /* [ninc1]                        */
+    const void *x_spec;                  /* x_spec(15, ld_xs, ninc1)       */
+    const void *f_spec;                  /* f_spec(3,  ld_xs, ninc1) or 0  */
+    uint64_t twin_seed;                  /* key of the counter-based twin
+                                            RNG (stands in for RANDOM_NUMBER,
+                                            src/fasolt/crys-cons.f90:169)  */
+} fas_ctrl_desc;
+
+/*
+ * Nodal and Gauss-point state (FAS_COM / FAS_CPL arrays).  Used for upload
+ * (read) and download (written).  Any pointer may be null to skip it.
+ */
+typedef struct fas_state_desc {
+    int32_t real_bytes;
+    int32_t nsv;                         /* state variables per GP used    */
+    int32_t ld_sv;                       /* leading dim of sv/dsv (63)     */
+    int32_t ld_slip;                     /* leading dim of srate/cumslip   */
+    void *x, *dx, *fc, *ddx;             /* [3*nnod]                       */
+    void *eps, *dep;                     /* [ngps]                         */
+    void *st, *ep, *ds, *de;             /* (6, ngps)                      */
+    void *rt, *dr;                       /* (3, ngps)                      */
+    void *sv, *dsv;                      /* (ld_sv, ngps)                  */
+    int32_t *timestwinned, *twinsys;     /* [ngps]                         */
+    void *srate, *cumslip;               /* (ld_slip, ngps)                */
+} fas_state_desc;
+
+/* One line of the NRITER progress report (ITEREP,
+ * src/fasolt/Faslt_io_nowin.f90:309-344), plus the SOR statistics. */
+typedef struct fas_iter_report {
+    int32_t nit;
+    int32_t sor_sweeps;
+    double  sdx, sfc, cp_err, alp2;
+    double  sor_error;
+} fas_iter_report;
+
+/* One twin reorientation (the unit-55 "twins" record written by DoReorient,
+ * src/fasolt/Fasolt3.f90:164).  gp and sys are 1-based. */
+typedef struct fas_twin_event {
+    int32_t inc, gp, sys, pad;
+    double  euler_old[3], euler_new[3];
+} fas_twin_event;
+
+typedef struct fas_handle fas_handle;
+
+/* Creates a device problem: uploads mesh, materials and loading, builds the
+ * node adjacency, the node colouring for SOR and the block-ELL stiffness
+ * layout.  Replaces the set-up half of SETPTA (src/fasolt/Stif_sol.f90:98-149)
+ * and the table reads of RDDATA.  `mode` is a FAS_MODE_* mask. */
+FAS_API int32_t fas_gpu_create(const fas_mesh_desc *mesh, const fas_matl_desc *matl,
+                       const fas_ctrl_desc *ctrl, uint32_t mode,
+                       fas_handle **out);
+FAS_API void    fas_gpu_destroy(fas_handle *h);
+FAS_API int32_t fas_gpu_set_mode(fas_handle *h, uint32_t mode);
+
+/* Copies Fortran-side state to the device (promoted to FP64) / back. */
+FAS_API int32_t fas_gpu_upload_state(fas_handle *h, const fas_state_desc *s);
+FAS_API int32_t fas_gpu_download_state(fas_handle *h, const fas_state_desc *s);
+
+/* UPDATE_NODE, src/fasolt/Fasolt3.f90:231-244:  x += dx. */
+FAS_API int32_t fas_gpu_update_node(fas_handle *h);
+
+/* ELVALS, src/fasolt/Elvals.f90:11-275 (with fc zeroed first, as
+ * NRITER does at src/fasolt/Stif_sol.f90:38-39).  `nit` is the global
+ * Newton iteration number (keys the twin RNG). */
+FAS_API int32_t fas_gpu_elvals(fas_handle *h, int32_t inc, int32_t nit);
+
+/* SUVALS, src/fasolt/Bconds.f90:19-113. */
+FAS_API int32_t fas_gpu_suvals(fas_handle *h, int32_t inc);
+
+/* FACSLS, src/fasolt/Stif_sol.f90:161-215: SOR on the assembled system,
+ * right-hand side taken from ddx, solution left in ddx.  Multicolour node
+ * order (see fas_gpu_get_colouring). */
+FAS_API int32_t fas_gpu_facsls(fas_handle *h, int32_t *sweeps, double *error);
+
+/* NRITER, src/fasolt/Stif_sol.f90:10-88: the damped global Newton loop of
+ * increment `inc` including the cumslip update.  Up to `cap` report lines
+ * are written to `rep` (may be null); *n_rep receives the iteration count. */
+FAS_API int32_t fas_gpu_nriter(fas_handle *h, int32_t inc, fas_iter_report *rep,
+                       int32_t cap, int32_t *n_rep);
+
+/* UPDATE_GPTV, src/fasolt/Fasolt3.f90:254-284. */
+FAS_API int32_t fas_gpu_update_gptv(fas_handle *h);
+
+/* DoReorient, src/fasolt/Fasolt3.f90:79-178.  Events are returned in
+ * ascending GP order; *n_ev may exceed cap (then only cap are written). */
+FAS_API int32_t fas_gpu_reorient(fas_handle *h, int32_t inc, fas_twin_event *ev,
+                         int32_t cap, int32_t *n_ev);
+
+/* One whole increment of the driver loop (src/fasolt/Fasolt3.f90:38-46):
+ * UPDATE_NODE, NRITER, UPDATE_GPTV and, when a twin fired, DoReorient. */
+FAS_API int32_t fas_gpu_increment(fas_handle *h, int32_t inc, fas_iter_report *rep,
+                          int32_t cap, int32_t *n_rep, fas_twin_event *ev,
+                          int32_t ev_cap, int32_t *n_ev);
+
+/* The compact stiffness pattern of SETPTA (src/fasolt/Stif_sol.f90:98-149),
+ * rebuilt on the device: is(1,row) = off-diagonal count, is(2..,row) = 1-based
+ * columns in first-touch order.  `is` is (ld_is, 3*nnod), column-major. */
+FAS_API int32_t fas_gpu_get_pattern(fas_handle *h, int32_t *is, int32_t ld_is);
+
+/* The assembled stiffness (after ELVALS [+ SUVALS]) in the reference layout
+ * ss(ld_ss, 3*nnod): ss(1,row) = diagonal, ss(k,row) = value of column
+ * is(k,row).  Replaces reading the module array ss. */
+FAS_API int32_t fas_gpu_get_stiffness(fas_handle *h, void *ss, int32_t ld_ss,
+                              int32_t real_bytes);
+
+/* Node colour of every node (0-based colours, [nnod]) and the colour count:
+ * the SOR visits colours in ascending order, nodes of one colour in any
+ * order, and the three DOFs of a node in x, y, z order. */
+FAS_API int32_t fas_gpu_get_colouring(fas_handle *h, int32_t *colour, int32_t *ncol);
+
+/* DSTRSS, src/fasolt/Sig_eps.f90:84-151, for every GP of the handle, taking
+ * the strain increment de(:,j) and spin dr(:,j) from the uploaded state
+ * (the constitutive micro-benchmark).  Updates ds, dsv, dep, srate and the
+ * twin flags on the device; the 6x6 tangent is kept for fas_gpu_get_tangent. */
+FAS_API int32_t fas_gpu_constitutive(fas_handle *h, int32_t inc, int32_t nit);
+
+/* The symmetrised tangent chi(6,6,ngps) of the last constitutive pass
+ * (upper triangle mirrored), column-major. */
+FAS_API int32_t fas_gpu_get_tangent(fas_handle *h, void *chi, int32_t real_bytes);
+
+/* Per-GP diagnostics of the last constitutive pass: outer (CPSTRS) iteration
+ * count and final erepmd.  Either pointer may be null. */
+FAS_API int32_t fas_gpu_get_cp_stats(fas_handle *h, int32_t *iters, double *erepmd);
+
+/* Per-GP algorithmic operation count of the last constitutive pass (the
+ * formulas of fas_flops.h summed over the iterations each GP took). */
+FAS_API int32_t fas_gpu_get_cp_ops(fas_handle *h, double *ops);
+
+/* Device time per phase, measured with CUDA events on the handle's stream
+ * while profiling is on, plus launch counts and algorithmic work. */
+typedef struct fas_profile {
+    double  ms_constitutive;   /* element kernel (kinematics + DSTRSS)      */
+    double  ms_assembly;       /* row-gather assembly (+ fused SUVALS)      */
+    double  ms_sor_colour;     /* multicolour SOR colour-phase kernels      */
+    double  ms_total;          /* everything on the stream while profiling  */
+    int64_t n_constitutive, n_assembly, n_sor_colour;
+    int64_t n_launches;        /* all kernels this library launched         */
+    int64_t gp_updates;        /* DSTRSS evaluations                        */
+    int64_t sor_sweeps;
+    double  sor_bytes;         /* algorithmic bytes of the colour kernels   */
+    double  assembly_bytes;    /* algorithmic bytes of the assembly kernel  */
+} fas_profile;
+
+/* enable != 0 starts (and zeroes) profiling, 0 stops it.  When `out` is
+ * non-null the counters so far are written to it first. */
+FAS_API int32_t fas_gpu_profile(fas_handle *h, int32_t enable, fas_profile *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FASOLT_GPU_H */

@@ -1,0 +1,109 @@
+"""The structured-brick generator against brute-force restatements of
+fs3pre's ADDEL_8NQ + SWEEP, SETBOUNDS and SETKINC."""
+import numpy as np
+import pytest
+
+from cpfem_code_b200 import generator
+
+
+def _addel_sweep(nx, ny, nz, dxl):
+    """ADDEL_8NQ (fs3pre.f90:183-233) then SWEEP (fs3p-swp.f90:53-109),
+    literally: append 8 nodes per element, then remove every node that lies
+    within the tolerance of an earlier one, renumbering the topology."""
+    xs, ln = [], []
+    for iz in range(nz):
+        for iy in range(ny):
+            for ix in range(nx):
+                x0 = np.array([dxl[0] * ix, dxl[1] * iy, dxl[2] * iz])
+                el = []
+                for off in generator.BRICK8:
+                    xs.append(x0 + dxl * off)
+                    el.append(len(xs))
+                ln.append(el)
+    x = np.array(xs)
+    ln = np.array(ln)
+    tol = 0.5 * dxl.min()
+    i_test = 1
+    while i_test < len(x):
+        i_test += 1
+        j = 1
+        common = False
+        while j < i_test - 1 and not common:
+            j += 1
+            common = np.sqrt(((x[i_test - 1] - x[j - 1]) ** 2).sum()) < tol
+        if common:
+            x = np.delete(x, i_test - 1, axis=0)
+            ln = np.where(ln == i_test, j, ln)
+            ln = np.where(ln > i_test, ln - 1, ln)
+            i_test -= 1
+    return x.reshape(-1), ln
+
+
+@pytest.mark.parametrize("n", [(1, 1, 1), (2, 2, 2), (3, 2, 1), (2, 3, 4)])
+def test_numbering_matches_sweep(n):
+    p = generator.structured_cube(n=n, lengths=(1.0, 2.0, 0.5), ninc=1)
+    dxl = np.array([1.0 / n[0], 2.0 / n[1], 0.5 / n[2]])
+    x, ln = _addel_sweep(*n, dxl)
+    assert p.nnod == len(x) // 3 == np.prod(np.array(n) + 1)
+    np.testing.assert_array_equal(p.ln, ln)
+    np.testing.assert_array_equal(p.x, x)
+    np.testing.assert_array_equal(p.lg[:, 0], np.arange(1, p.nlmnt + 1))
+
+
+def test_bounds_xfree3_uniaxial():
+    p = generator.structured_cube(n=(2, 2, 2), xfree=3, ninc=1)
+    xyz = p.x.reshape(-1, 3)
+    lo = np.isclose(xyz[:, 0], 0.0)
+    hi = np.isclose(xyz[:, 0], 1.0)
+    origin = np.all(np.isclose(xyz, 0.0), axis=1)
+    inner = np.all((xyz > 0) & (xyz < 1), axis=1)
+    assert (p.ib[origin] == 700).all()            # l_side 21 keeps the 'all fixed' default
+    assert (p.ib[lo & ~origin] == 100).all()
+    assert (p.ib[hi] == 800).all()
+    assert (p.ib[inner] == 0).all()
+    assert (p.ib[~lo & ~hi & ~inner] == 1).all()
+
+
+@pytest.mark.parametrize("xfree", [0, 1, 2])
+def test_bounds_other_options(xfree):
+    p = generator.structured_cube(n=(2, 2, 2), xfree=xfree, ninc=1)
+    xyz = p.x.reshape(-1, 3)
+    surf = ~np.all((xyz > 0) & (xyz < 1), axis=1)
+    if xfree == 0:
+        assert (p.ib[surf] == 5000).all()
+    if xfree == 1:
+        corner = np.all(np.isclose(xyz, 1.0), axis=1)
+        assert (p.ib[corner] == 1400).all()
+    if xfree == 2:
+        # x faces free, y and z faces specified
+        xlo_only = np.isclose(xyz[:, 0], 0) & (xyz[:, 1] > 0) & (xyz[:, 1] < 1) & (xyz[:, 2] > 0) & (xyz[:, 2] < 1)
+        assert (p.ib[xlo_only] == 1).all()
+    assert (p.ib[~surf] == 0).all()
+
+
+def test_setkinc_tables():
+    tiem, xs = generator.setkinc((1.0, 1.0, 1.0), 3, (1e-3, 5.0, 5.0), 3)
+    np.testing.assert_allclose(tiem, 1e-3)
+    # x-spec code 8: mask xx, target = e11 * current length, compounding
+    L = 1.0
+    for i in range(3):
+        np.testing.assert_array_equal(xs[i, 7, :6], [1, 0, 0, 0, 0, 0])
+        assert xs[i, 7, 6] == pytest.approx(1e-3 * L)
+        L += 1e-3 * L
+        assert xs[i, 0, 6] == 0.0
+        np.testing.assert_array_equal(xs[i, 49, :6], [1, 0, 1, 0, 0, 1])
+        assert xs[i, 49, 6] == 1e-3 and xs[i, 49, 10] == 0.0
+
+
+def test_grains_and_materials():
+    a = generator.fcc_aluminium()
+    b = dict(a, name="fcc-b")
+    p = generator.structured_cube(n=(4, 4, 4), grain=2, materials=[a, b], fractions=[0.5, 0.5], seed=3)
+    gid = p.meta["grain_id"]
+    assert gid.max() == 7
+    for g in range(8):
+        sel = gid == g
+        assert len(np.unique(p.le[sel])) == 1
+        assert np.unique(p.sv[sel, :3], axis=0).shape[0] == 1
+    assert set(np.unique(p.le)) <= {1, 2}
+    assert (p.sv[:, 3:15] == 25.0).all()
