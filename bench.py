@@ -1,0 +1,341 @@
+#!/usr/bin/env python
+"""Benchmark of the FASOLT3 increment hot path on B200.
+
+Workload: the 64^3 FCC aluminium cube (262,144 one-point bricks = GPs,
+274,625 nodes, 823,875 DOF), grains of 2^3 elements with seeded uniform-SO(3)
+orientations, uniaxial tension at 1e-3 strain per increment.  A *step* is one
+increment of the driver loop: UPDATE_NODE -> NRITER -> UPDATE_GPTV ->
+DoReorient.  W untimed increments, then K timed ones.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Metric: Gauss-point updates per second -- one DSTRSS evaluation of one GP in
+one global Newton iteration -- over the whole increment (elements, assembly,
+SOR, norms, commit), i.e. ngps * Newton iterations / time.  The seconds per
+increment are reported beside it.  `value` is device time of the timed
+increments with all inputs resident in HBM (CUDA events on the library's
+stream); `e2e` repeats the same increments through the C ABI with the state
+copied from pinned host memory before and back after every increment.
+
+N > 1 (torchrun): independent replicas, one per GPU (the path is one
+problem on one GPU); time is the max over ranks, value the sum of work.
+`--impl reference` times the CPU restatement of the reference on the host
+cores instead (each step one complete Newton iteration of increment 1).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "cube64"
+METRIC = "GP updates/s at 64^3 (DSTRSS evaluations per second of whole Newton iterations)"
+DESC = ("64^3 FCC Al one-point bricks (262,144 GPs, 823,875 DOF), 2^3-element grains, "
+        "uniaxial tension 1e-3 per increment")
+
+
+def peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return dict(hbm_gbs=float(d["hbm_gbs"]), source="measured")
+    except Exception:
+        return dict(hbm_gbs=6650.0, source="fallback")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=["nvidia-smi unavailable"])
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for k, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(k)
+        return dict(sm_mhz=float(np.median(sm)) if sm else None,
+                    sm_max_mhz=float(max(smax)) if smax else None,
+                    reasons=sorted(reasons), samples=len(sm))
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def init_dist(ws: int, backend: str):
+    if ws <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
+def reduce_max_sum(dist, t: float, work: float, device=None):
+    """(max of t, sum of work) over ranks -- the only collective of the
+    benchmark (replicas share nothing on the data path)."""
+    if dist is None:
+        return t, work
+    import torch
+    a = torch.tensor([t], dtype=torch.float64, device=device)
+    b = torch.tensor([work], dtype=torch.float64, device=device)
+    dist.all_reduce(a, op=dist.ReduceOp.MAX)
+    dist.all_reduce(b, op=dist.ReduceOp.SUM)
+    return float(a.item()), float(b.item())
+
+
+# ------------------------------------------------------------------ CPU leg
+def cpu_sample(prob, inc: int, warm_iters: int, timed_iters: int, threads: int) -> dict:
+    """The checker (oracle/, the C++ restatement of the reference) on the
+    host cores: complete Newton iterations of increment `inc` of the
+    workload, starting from the state held in `prob`."""
+    from oracle import OracleSolver
+    o = OracleSolver(prob.copy(), 8, threads=threads)
+    o.update_node()
+    nit = 0
+    for _ in range(warm_iters):
+        nit += 1
+        o.nr_step(inc, nit)
+    t0 = time.perf_counter()
+    sweeps = 0
+    for _ in range(timed_iters):
+        nit += 1
+        r, more = o.nr_step(inc, nit)
+        sweeps += r["sor_sweeps"]
+    dt = time.perf_counter() - t0
+    o.close()
+    return dict(value=prob.ngps * timed_iters / dt, seconds=dt, iters=timed_iters, sweeps=sweeps,
+                first_iter=warm_iters + 1)
+
+
+def run_reference(args):
+    ws, rank, local = dist_env()
+    dist = init_dist(ws, "gloo")
+    if rank != 0:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
+    from cpfem_code_b200 import generator
+    prob = generator.workload(WORKLOAD)
+    threads = os.cpu_count() or 1
+    # iterations 1-2 of increment 1 are elastic (dx and ds start at zero);
+    # the warm-up covers at least those
+    s = cpu_sample(prob, 1, max(args.warmup, 2), args.steps, threads)
+    line = {
+        "impl": "reference", "metric": METRIC,
+        "value": s["value"], "unit": "GP-updates/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * s["seconds"] / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, fs3pre semantics)",
+        "config": {"workload": WORKLOAD, "desc": DESC, "step": "one complete Newton iteration of increment 1"},
+        "cpu_baseline": {"value": s["value"], "unit": "GP-updates/s", "cores": threads, "kind": "port",
+                         "sample": f"Newton iterations {s['first_iter']}..{s['first_iter'] + s['iters'] - 1} "
+                                   f"of increment 1 ({s['sweeps']} SOR sweeps) on {threads} threads"},
+        "e2e": {"value": s["value"], "unit": "GP-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+# ------------------------------------------------------------------ GPU leg
+def pinned_like(prob):
+    """Re-back the state arrays of `prob` with pinned host memory."""
+    import torch
+    for name in ("x", "dx", "fc", "ddx", "eps", "dep", "st", "ep", "ds", "de", "rt", "dr",
+                 "sv", "dsv", "srate", "cumslip", "timestwinned", "twinsys"):
+        a = getattr(prob, name)
+        t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+        b = t.numpy()
+        b[...] = a
+        setattr(prob, name, b)
+        prob.meta.setdefault("_pinned", []).append(t)
+
+
+def moved_bytes(prob, ns: int) -> int:
+    """Bytes one upload (or download) moves: the nodal vectors and the used
+    columns of every GP field."""
+    nsv = 3 + ns
+    per_gp = 8 * (2 + 24 + 6 + 2 * nsv + 2 * ns) + 8
+    return 4 * 3 * prob.nnod * 8 + prob.ngps * per_gp
+
+
+def run_gpu(args):
+    import torch
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = init_dist(ws, "nccl")
+    dev = torch.device("cuda", local)
+    from cpfem_code_b200 import GpuSolver, generator
+
+    prob = generator.workload(WORKLOAD)
+    ninc_needed = args.warmup + 2 * args.steps + 1
+    if prob.ninc1 < ninc_needed:
+        prob = generator.workload(WORKLOAD, ninc=ninc_needed)
+    g = GpuSolver(prob)
+    inc = 0
+    for _ in range(args.warmup):
+        inc += 1
+        g.increment(inc)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    g.profile(True)
+    nit = 0
+    sweeps = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        inc += 1
+        rep, _ = g.increment(inc)
+        nit += len(rep)
+        sweeps += sum(r["sor_sweeps"] for r in rep)
+    prof = g.profile(False)
+    wall = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    dev_s = prof["ms_total"] / 1e3
+    t_max, work = reduce_max_sum(dist, dev_s, float(prob.ngps * nit), dev)
+    value = work / t_max
+
+    # e2e: the same kind of increments through the ABI with host state
+    g.download()
+    nit_e, e2e_s = 0, 0.0
+    if not args.no_e2e:
+        pinned_like(prob)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            inc += 1
+            g.upload(prob)
+            rep, _ = g.increment(inc)
+            g.download(prob)
+            nit_e += len(rep)
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+    te, work_e = reduce_max_sum(dist, e2e_s, float(prob.ngps * nit_e), dev)
+    mb = moved_bytes(prob, int(prob.nss.max()))
+
+    if rank == 0:
+        pk = peaks()
+        achieved = prof["sor_bytes"] / (prof["ms_sor_colour"] / 1e3) / 1e9 if prof["ms_sor_colour"] else 0.0
+        launch_ms = prof["ms_sor_colour"] / max(prof["n_sor_colour"], 1)
+        line = {
+            "metric": METRIC,
+            "value": value, "unit": "GP-updates/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator, fs3pre semantics)",
+            "config": {"workload": WORKLOAD, "desc": DESC, "parallelism": f"replicas{ws}",
+                       "increments": [args.warmup + 1, args.warmup + args.steps],
+                       "newton_iters": nit, "sor_sweeps": sweeps,
+                       "l2": "inputs larger than L2 (534 MB block matrix re-read every sweep)"},
+            "s_per_increment": t_max / args.steps,
+            "wall_s": wall,
+            "phases_ms": {"constitutive": prof["ms_constitutive"], "assembly": prof["ms_assembly"],
+                          "sor_colour": prof["ms_sor_colour"], "total": prof["ms_total"]},
+            "constitutive_gp_updates_per_s": prof["gp_updates"] / (prof["ms_constitutive"] / 1e3)
+            if prof["ms_constitutive"] else None,
+            "gpu_launches": int(prof["n_launches"]),
+            "roofline": {"kernel": "k_sor_colour", "bound": "hbm", "achieved": achieved,
+                         "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
+                         "peak_source": pk["source"], "traffic": None,
+                         "launch_ms": launch_ms,
+                         "bytes_per_launch": prof["sor_bytes"] / max(prof["n_sor_colour"], 1)},
+            "clocks": clk,
+            "e2e": {"value": work_e / te if te > 0 else None, "unit": "GP-updates/s",
+                    "h2d_bytes_per_step": mb, "d2h_bytes_per_step": mb,
+                    "s_per_increment": te / args.steps if te > 0 else None},
+        }
+        if ws == 1 and not args.no_cpu:
+            # the state after the e2e increments is plastic: time the first
+            # Newton iteration of the next increment on the host cores
+            s = cpu_sample(prob, inc + 1, 0, 1, os.cpu_count() or 1)
+            line["cpu_baseline"] = {
+                "value": s["value"], "unit": "GP-updates/s", "cores": os.cpu_count() or 1,
+                "kind": "port",
+                "sample": f"Newton iteration 1 of increment {inc + 1} ({s['sweeps']} SOR sweeps) "
+                          f"by the C++ restatement from the same state, {s['seconds']:.1f} s"}
+        print(json.dumps(line), flush=True)
+    g.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer (e2e) leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -729,35 +729,47 @@ void gaussm_block(const R ai[3], const R bj[3], const R d[6][6], const R s[6], R
 }
 
 // ================================================================ assembly
-// SETPTA, src/fasolt/Stif_sol.f90:98-149 (first-touch column order).
+// SETPTA, src/fasolt/Stif_sol.f90:98-149 (first-touch column order).  The
+// reference appends, element by element, each new column of every row of the
+// element in local DOF order; for one row that is the order of its elements
+// (ascending) and their local DOFs, which is how it is built here -- one row
+// at a time, with a stamp array instead of the reference's linear search.
 template <class R> void setpta(Problem<R> &P)
 {
     const int ndof = 3 * P.nnod;
-    // first pass: row lengths to size the compact rows
-    std::vector<std::vector<int>> cols(ndof);
-    for (int e = 0; e < P.nlmnt; ++e) {
-        int nn = P.nd[e];
-        int loc[60];
-        for (int i = 0; i < nn; ++i)
-            for (int c = 0; c < 3; ++c) loc[3 * i + c] = 3 * P.ln[e * P.ldn + i] + c;
-        for (int i = 0; i < 3 * nn; ++i) {
-            int row = loc[i];
-            for (int j = 0; j < 3 * nn; ++j) {
-                int col = loc[j];
-                if (row == col) continue;
-                auto &v = cols[row];
-                if (std::find(v.begin(), v.end(), col) == v.end()) v.push_back(col);
-            }
-        }
-    }
+    std::vector<int> ptr(P.nnod + 1, 0);
+    for (int e = 0; e < P.nlmnt; ++e)
+        for (int i = 0; i < P.nd[e]; ++i) ptr[P.ln[e * P.ldn + i] + 1]++;
+    for (int n = 0; n < P.nnod; ++n) ptr[n + 1] += ptr[n];
+    std::vector<int> adj(ptr[P.nnod]), fill(ptr.begin(), ptr.end() - 1);
+    for (int e = 0; e < P.nlmnt; ++e)
+        for (int i = 0; i < P.nd[e]; ++i) adj[fill[P.ln[e * P.ldn + i]]++] = e;
+    std::vector<int> stamp(ndof, -1), cnt(ndof, 0);
     int mx = 0;
-    for (auto &v : cols) mx = std::max<int>(mx, (int)v.size());
-    P.ld = mx + 1;
-    P.is.assign((size_t)ndof * P.ld, 0);
-    P.ss.assign((size_t)ndof * P.ld, R(0));
-    for (int r = 0; r < ndof; ++r) {
-        P.is[(size_t)r * P.ld] = (int)cols[r].size();
-        for (size_t k = 0; k < cols[r].size(); ++k) P.is[(size_t)r * P.ld + 1 + k] = cols[r][k];
+    for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1) {
+            P.ld = mx + 1;
+            P.is.assign((size_t)ndof * P.ld, 0);
+            P.ss.assign((size_t)ndof * P.ld, R(0));
+            std::fill(stamp.begin(), stamp.end(), -1);
+        }
+        for (int row = 0; row < ndof; ++row) {
+            const int n = row / 3;
+            int c = 0;
+            for (int k = ptr[n]; k < ptr[n + 1]; ++k) {
+                const int e = adj[k];
+                for (int i = 0; i < P.nd[e]; ++i)
+                    for (int q = 0; q < 3; ++q) {
+                        const int col = 3 * P.ln[e * P.ldn + i] + q;
+                        if (col == row || stamp[col] == row) continue;
+                        stamp[col] = row;
+                        ++c;
+                        if (pass == 1) P.is[(size_t)row * P.ld + c] = col;
+                    }
+            }
+            if (pass == 0) mx = std::max(mx, c);
+            else P.is[(size_t)row * P.ld] = c;
+        }
     }
 }
 
@@ -1063,52 +1075,64 @@ template <class R> int facsls(Problem<R> &P, int maxitl, int *sweeps, double *er
     return 0;
 }
 
+// One pass of NRITER's loop body (src/fasolt/Stif_sol.f90:32-77): ELVALS,
+// SUVALS, the residual norm, FACSLS, the damping factor and the correction.
+// *more = the reference's loop condition for another pass.
+template <class R> int nr_step(Problem<R> &P, int inc, int nit, fas_iter_report *r, bool *more)
+{
+    const int ndof = 3 * P.nnod;
+    int rc = elvals(P, inc, nit);
+    if (rc) return rc;
+    rc = suvals(P, inc);
+    if (rc) return rc;
+    R sfc = 0;
+    for (int i = 0; i < P.nnod; ++i)
+        if (P.ib[i] < 10)
+            sfc = sfc + P.ddx[3 * i] * P.ddx[3 * i] + P.ddx[3 * i + 1] * P.ddx[3 * i + 1] +
+                  P.ddx[3 * i + 2] * P.ddx[3 * i + 2];
+    sfc = std::sqrt(sfc);
+    int sweeps = 0;
+    double serr = 0;
+    rc = facsls(P, 1000, &sweeps, &serr);
+    if (rc) return rc;
+    R a = 0, b = 0;
+    for (int i = 0; i < ndof; ++i) a = a + P.dx[i] * P.dx[i];
+    for (int i = 0; i < ndof; ++i) b = b + P.ddx[i] * P.ddx[i];
+    R errdx = std::sqrt(a), erddx = std::sqrt(b);
+    R sdx = errdx == R(0) ? P.toler : erddx / errdx;
+    R alp2 = R(1.0) / (R(1.0) + P.alpha * sdx);
+    R cperr = P.sumcpiter / (R)P.ngps;
+    if (r) {
+        r->nit = nit;
+        r->sor_sweeps = sweeps;
+        r->sdx = sdx;
+        r->sfc = sfc;
+        r->cp_err = cperr;
+        r->alp2 = alp2;
+        r->sor_error = serr;
+    }
+    for (int i = 0; i < ndof; ++i) {
+        R xc = alp2 * P.ddx[i];
+        P.x[i] = P.x[i] - xc;
+        P.dx[i] = P.dx[i] - xc;
+    }
+    if (more) *more = (sdx >= P.toler) && (nit < P.maxit);
+    return 0;
+}
+
 // NRITER, src/fasolt/Stif_sol.f90:10-88 (ITEREP lines go to `rep`).
 template <class R>
 int nriter(Problem<R> &P, int inc, fas_iter_report *rep, int cap, int *n_rep)
 {
-    const int ndof = 3 * P.nnod;
     int nit = 0;
     bool l_conv = true;
     while (l_conv) {
         ++nit;
-        int rc = elvals(P, inc, nit);
-        if (rc) { if (n_rep) *n_rep = nit; return rc; }
-        rc = suvals(P, inc);
-        if (rc) { if (n_rep) *n_rep = nit; return rc; }
-        R sfc = 0;
-        for (int i = 0; i < P.nnod; ++i)
-            if (P.ib[i] < 10)
-                sfc = sfc + P.ddx[3 * i] * P.ddx[3 * i] + P.ddx[3 * i + 1] * P.ddx[3 * i + 1] +
-                      P.ddx[3 * i + 2] * P.ddx[3 * i + 2];
-        sfc = std::sqrt(sfc);
-        int sweeps = 0;
-        double serr = 0;
-        rc = facsls(P, 1000, &sweeps, &serr);
-        if (rc) { if (n_rep) *n_rep = nit; return rc; }
-        R a = 0, b = 0;
-        for (int i = 0; i < ndof; ++i) a = a + P.dx[i] * P.dx[i];
-        for (int i = 0; i < ndof; ++i) b = b + P.ddx[i] * P.ddx[i];
-        R errdx = std::sqrt(a), erddx = std::sqrt(b);
-        R sdx = errdx == R(0) ? P.toler : erddx / errdx;
-        R alp2 = R(1.0) / (R(1.0) + P.alpha * sdx);
-        R cperr = P.sumcpiter / (R)P.ngps;
-        if (rep && nit <= cap) {
-            fas_iter_report &r = rep[nit - 1];
-            r.nit = nit;
-            r.sor_sweeps = sweeps;
-            r.sdx = sdx;
-            r.sfc = sfc;
-            r.cp_err = cperr;
-            r.alp2 = alp2;
-            r.sor_error = serr;
-        }
-        for (int i = 0; i < ndof; ++i) {
-            R xc = alp2 * P.ddx[i];
-            P.x[i] = P.x[i] - xc;
-            P.dx[i] = P.dx[i] - xc;
-        }
-        l_conv = (sdx >= P.toler) && (nit < P.maxit);
+        if (n_rep) *n_rep = nit;
+        fas_iter_report r;
+        int rc = nr_step(P, inc, nit, &r, &l_conv);
+        if (rc) return rc;
+        if (rep && nit <= cap) rep[nit - 1] = r;
     }
     if (n_rep) *n_rep = nit;
     // cumslip over nss(mat_code) of the last material touched (Stif_sol.f90:80-84)
@@ -1525,6 +1549,17 @@ int32_t ora_nriter(ora_problem *p, int32_t inc, fas_iter_report *rep, int32_t ca
         if (!P.have_state || P.nlmnt == 0) return FAS_E_STATE;
         if (inc < 1 || inc > P.ninc1) return FAS_E_ARG;
         return nriter(P, inc, rep, cap, n_rep);
+    });
+}
+int32_t ora_nr_step(ora_problem *p, int32_t inc, int32_t nit, fas_iter_report *rep, int32_t *more)
+{
+    DISPATCH(p, {
+        if (!P.have_state || P.nlmnt == 0) return FAS_E_STATE;
+        if (inc < 1 || inc > P.ninc1) return FAS_E_ARG;
+        bool m = false;
+        int rc = nr_step(P, inc, nit, rep, &m);
+        if (more) *more = m ? 1 : 0;
+        return rc;
     });
 }
 int32_t ora_update_gptv(ora_problem *p)
