@@ -14,8 +14,9 @@ one global Newton iteration -- over the whole increment (elements, assembly,
 SOR, norms, commit), i.e. ngps * Newton iterations / time.  The seconds per
 increment are reported beside it.  `value` is device time of the timed
 increments with all inputs resident in HBM (CUDA events on the library's
-stream); `e2e` repeats the same increments through the C ABI with the state
-copied from pinned host memory before and back after every increment.
+stream); `e2e` replays the same increments from the same start state through
+the C ABI with the whole state copied from pinned host memory before and
+back after every increment.
 
 N > 1 (torchrun): independent replicas, one per GPU (the path is one
 problem on one GPU); time is the max over ranks, value the sum of work.
@@ -233,6 +234,11 @@ def run_gpu(args):
     for _ in range(args.warmup):
         inc += 1
         g.increment(inc)
+    # the state at the start of the timed increments, kept on the host so the
+    # e2e leg can replay exactly the same increments
+    g.download()
+    start = prob.copy()
+    inc0 = inc
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
@@ -255,23 +261,26 @@ def run_gpu(args):
     t_max, work = reduce_max_sum(dist, dev_s, float(prob.ngps * nit), dev)
     value = work / t_max
 
-    # e2e: the same kind of increments through the ABI with host state
-    g.download()
+    # e2e: the same increments again through the ABI, the whole state copied
+    # from pinned host memory before and back after every increment
     nit_e, e2e_s = 0, 0.0
     if not args.no_e2e:
-        pinned_like(prob)
+        host = start
+        pinned_like(host)
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
         t0 = time.perf_counter()
-        for _ in range(args.steps):
-            inc += 1
-            g.upload(prob)
-            rep, _ = g.increment(inc)
-            g.download(prob)
+        for k in range(args.steps):
+            g.upload(host)
+            rep, _ = g.increment(inc0 + 1 + k)
+            g.download(host)
             nit_e += len(rep)
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
+        prob = host
+    else:
+        g.download()
     te, work_e = reduce_max_sum(dist, e2e_s, float(prob.ngps * nit_e), dev)
     mb = moved_bytes(prob, int(prob.nss.max()))
 
@@ -304,7 +313,8 @@ def run_gpu(args):
             "clocks": clk,
             "e2e": {"value": work_e / te if te > 0 else None, "unit": "GP-updates/s",
                     "h2d_bytes_per_step": mb, "d2h_bytes_per_step": mb,
-                    "s_per_increment": te / args.steps if te > 0 else None},
+                    "s_per_increment": te / args.steps if te > 0 else None,
+                    "newton_iters": nit_e, "increments": [inc0 + 1, inc0 + args.steps]},
         }
         if ws == 1 and not args.no_cpu:
             # the state after the e2e increments is plastic: time the first

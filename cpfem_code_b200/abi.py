@@ -28,6 +28,7 @@ XSLD = 99          # second dimension of x_spec / f_spec (fas-com-mod.f90:30-31)
 FAS_MODE_PLAIN = 0
 FAS_MODE_SOR_FP32 = 1
 FAS_MODE_SOR_NATURAL = 2
+FAS_MODE_SOR_GRID = 4
 
 #: FAFERR codes the hot path raises, with the reference's meaning.
 FAFERR_TEXT = {

@@ -68,7 +68,7 @@ struct HostCtl {                 // pinned mirror of the small device results
 }  // namespace
 
 struct fas_handle {
-    int dev = 0;
+    int dev = 0, nsm = 148;
     cudaStream_t stream = nullptr;
     uint32_t mode = 0;
     int nlmnt = 0, nnod = 0, ngps = 0;
@@ -103,6 +103,8 @@ struct fas_handle {
     DVec<double> blk;
     // reductions and control
     std::vector<int> sor_boff, sor_nblk;
+    DVec<int> d_cstart;          // colour ranges for the one-CTA SOR
+    bool sor_small = false;      // whole solve in one CTA (small meshes)
     int sor_nblk_tot = 0, nr_nblk = 0;
     DVec<double> part_sor, part_nr, sums;
     DVec<unsigned long long> ekey;
@@ -155,6 +157,9 @@ struct fas_handle {
         return b;
     }
 };
+
+// meshes with at most this many nodes run each SOR solve in one CTA
+constexpr int SOR_SMALL_ROWS = 8192;
 
 #define CK(expr)                                      \
     do {                                              \
@@ -296,7 +301,7 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
         for (int m : others) nb[cnt++] = m;
         nslot[p] = cnt;
         for (int s = 0; s < cnt; ++s) {
-            bcol[(size_t)s * nn + p] = nb[s];
+            bcol[sidx(p, s)] = nb[s];
             unsigned word = 0xFFFFFFFFu;
             int k = 0;
             for (int q = h->ne_ptr[n]; q < h->ne_ptr[n + 1]; ++q, ++k) {
@@ -306,7 +311,7 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
                     if (h->h_ln[(size_t)e * 8 + a] == nb[s]) { b = (unsigned)a; break; }
                 word = (word & ~(0xFu << (4 * k))) | (b << (4 * k));
             }
-            bloc[(size_t)s * nn + p] = word;
+            bloc[sidx(p, s)] = word;
         }
     }
     // algorithmic bytes of one colour launch: blocks and column ids of the
@@ -340,11 +345,16 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
     int tot = 0;
     for (int c = 0; c < h->ncol; ++c) {
         h->sor_boff[c] = tot;
-        h->sor_nblk[c] = (int)nblocks(h->col_start[c + 1] - h->col_start[c], 256);
+        // warp per row, 8 rows per block, at most 8 blocks per SM resident
+        h->sor_nblk[c] = (int)std::min<long long>(nblocks(h->col_start[c + 1] - h->col_start[c], 8),
+                                                   (long long)h->nsm * 8);
         tot += h->sor_nblk[c];
     }
     h->sor_nblk_tot = std::max(tot, 1);
     CKA(h->part_sor.alloc((size_t)2 * h->sor_nblk_tot));
+    CKA(h->d_cstart.alloc(h->ncol + 1));
+    CK(h->d_cstart.put(h->col_start.data(), h->ncol + 1, s));
+    h->sor_small = nn <= SOR_SMALL_ROWS;
     CK(cudaStreamSynchronize(s));
     return 0;
 }
@@ -357,6 +367,7 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
     cudaDeviceProp prop;
     CK(cudaGetDeviceProperties(&prop, h->dev));
     if (prop.major != 10) return FAS_E_NODEVICE;
+    h->nsm = prop.multiProcessorCount;
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     CK(cudaMallocHost((void **)&h->hc, sizeof(HostCtl)));
     CK(cudaEventCreate(&h->ev_t0));
@@ -711,7 +722,7 @@ int elvals_impl(fas_handle *h, int inc, int nit, bool bc)
     if (rc) return rc;
     {
         Span sp(h, &h->P.ms_assembly);
-        const long long nthr = (long long)SLOTS * h->nnod;
+        const long long nthr = (long long)SLOTS * h->nnod;   // thread (row, slot), row-major
         k_assemble<<<nblocks(nthr, 256), 256, 0, s>>>(
             h->mesh(), h->block(), h->rec.p, h->x.p, h->dx.p, h->fc.p, h->ddx.p,
             h->xspec.p + (size_t)(inc - 1) * std::max(h->nxs, 1) * 15,
@@ -763,7 +774,17 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
     CK(cudaStreamSynchronize(s));
     if (h->hc->ekey[1] != ~0ull) return 903;
     const double tolerl = h->C.toler * h->C.toler;
-    int done = 0, chunk = 4;
+    const bool small = h->sor_small && !(h->mode & FAS_MODE_SOR_GRID);
+    if (small) {
+        Span sp(h, &h->P.ms_sor_colour);
+        k_sor_small<<<1, 1024, 0, s>>>(B, h->d_cstart.p, h->ncol, h->rhs.p, h->ddx.p, h->sorctl.p, tolerl, 1000);
+        sp.end();
+        keep(h, sp);
+        LAUNCHED(h);
+        CK(cudaMemcpyAsync(&h->hc->sor, h->sorctl.p, sizeof(SorCtl), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    int done = small ? 1000 : 0, chunk = 4;
     while (done < 1000) {
         const int k = std::min(chunk, 1000 - done);
         for (int it = 0; it < k; ++it) {
@@ -789,7 +810,7 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
     settle_spans(h);
     const int nsw = h->hc->sor.sweeps;
     h->P.sor_sweeps += nsw;
-    h->P.n_sor_colour += (int64_t)nsw * h->ncol;
+    h->P.n_sor_colour += small ? 1 : (int64_t)nsw * h->ncol;
     double bytes = 0.0;
     for (double b : h->col_bytes) bytes += b;
     h->P.sor_bytes += bytes * nsw;

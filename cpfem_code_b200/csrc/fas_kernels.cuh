@@ -7,8 +7,9 @@
 //     upper triangle (21) -- written once per Newton iteration by the element
 //     kernel and read by the row-gather assembly;
 //   * stiffness: block-ELL of 3x3 node blocks, rows permuted so each SOR
-//     colour is a contiguous row range; blk[(slot*9 + r*3 + c) * R + row],
-//     slot 0 = the diagonal block, bcol[slot * R + row] = column node.
+//     colour is a contiguous row range, row-major: the 27 blocks of a row
+//     are 1944 contiguous bytes, blk[((row*27 + slot)*9 + r*3 + c)];
+//     slot 0 = the diagonal block, bcol[row*27 + slot] = column node.
 #pragma once
 
 #include "fas_device.cuh"
@@ -19,6 +20,10 @@ constexpr int REC = 56;          // doubles per element record
 constexpr int REC_S = 24, REC_W = 30, REC_D = 32;
 constexpr int SLOTS = 27;        // node blocks per row of an 8-node brick mesh
 constexpr int MAXADJ = 8;        // elements per node
+
+// block matrix addressing (row-major rows of SLOTS 3x3 blocks)
+__host__ __device__ __forceinline__ size_t sidx(int p, int s) { return (size_t)p * 27 + s; }
+__host__ __device__ __forceinline__ size_t bidx(int p, int s, int q) { return ((size_t)p * 27 + s) * 9 + q; }
 
 // upper-triangle index of chi(i,j), i <= j (0-based)
 __host__ __device__ __forceinline__ int utri(int i, int j) { return i * 6 - (i * (i - 1)) / 2 + (j - i); }
@@ -38,10 +43,10 @@ struct BlockDev {
     int R;               // rows (= nnod)
     const int *perm;     // row -> node
     const int *nslot;    // [R]
-    const int *bcol;     // [SLOTS][R] column node of each slot
-    const unsigned *bloc;// [SLOTS][R] 4-bit local index of the column node in
+    const int *bcol;     // [R][SLOTS] column node of each slot
+    const unsigned *bloc;// [R][SLOTS] 4-bit local index of the column node in
                          // each adjacent element of the row node (0xF: absent)
-    double *blk;         // [SLOTS*9][R]
+    double *blk;         // [R][SLOTS][9]
 };
 
 // ---------------------------------------------------------------- element pass
@@ -265,13 +270,12 @@ __global__ void __launch_bounds__(256) k_assemble(MeshDev Mh, BlockDev B,
                                                   double efix, int bc, int *bad_bc)
 {
     const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int R = B.R;
-    const int s = (int)(tid / R);
-    const int p = (int)(tid - (long long)s * R);
-    if (s >= SLOTS) return;
+    const int p = (int)(tid / SLOTS);
+    const int s = (int)(tid - (long long)p * SLOTS);
+    if (p >= B.R) return;
     if (s >= B.nslot[p]) return;
     const int n = B.perm[p];
-    const unsigned bl = B.bloc[s * R + p];
+    const unsigned bl = B.bloc[sidx(p, s)];
     const int cnt = Mh.ne_cnt[n];
     double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     double f[3] = {0, 0, 0};
@@ -312,7 +316,7 @@ __global__ void __launch_bounds__(256) k_assemble(MeshDev Mh, BlockDev B,
         }
     }
 #pragma unroll
-    for (int q = 0; q < 9; ++q) B.blk[(size_t)(s * 9 + q) * R + p] = acc[q];
+    for (int q = 0; q < 9; ++q) B.blk[bidx(p, s, q)] = acc[q];
 }
 
 // Stand-alone SUVALS (src/fasolt/Bconds.f90:19-113): ddx = fc, then the
@@ -327,13 +331,12 @@ __global__ void k_suvals(MeshDev Mh, BlockDev B, const int *rowof, const double 
     const int ibc = Mh.ib[n];
     if (ibc >= 100) {
         const int p = rowof[n];
-        const int R = B.R;
         double D[9];
 #pragma unroll
-        for (int q = 0; q < 9; ++q) D[q] = B.blk[(size_t)q * R + p];
+        for (int q = 0; q < 9; ++q) D[q] = B.blk[bidx(p, 0, q)];
         if (apply_bc(ibc, n, x, dx, xspec, fspec, nxs, nfs, efix, D, f)) *bad_bc = 1;
 #pragma unroll
-        for (int q = 0; q < 9; ++q) B.blk[(size_t)q * R + p] = D[q];
+        for (int q = 0; q < 9; ++q) B.blk[bidx(p, 0, q)] = D[q];
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) ddx[3 * n + c] = f[c];
@@ -432,45 +435,138 @@ struct SorCtl {
     double pad;
 };
 
+// One warp per row: lane s (1 <= s < nslot) multiplies the off-diagonal
+// block of slot s by the current solution at its column node; the warp sums
+// the three products; lane 0 then updates x, y, z in turn with the diagonal
+// block.  The row's blocks are 1944 contiguous bytes, so each row is read
+// with full sectors.  Warps stride over the colour's rows; each block adds
+// its share of sum(dx^2) and sum(x^2) to part[] once.
 __global__ void __launch_bounds__(256) k_sor_colour(BlockDev B, int p0, int p1,
                                                     const double *__restrict__ rhs, double *sol,
                                                     const SorCtl *ctl, double *part, int boff,
                                                     int nblk_tot)
 {
     if (((volatile const SorCtl *)ctl)->conv) return;
-    const int p = p0 + blockIdx.x * blockDim.x + threadIdx.x;
-    const int R = B.R;
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
     double v[2] = {0.0, 0.0};
-    if (p < p1) {
-        const int n = B.perm[p];
+    for (int p = p0 + blockIdx.x * wpb + (threadIdx.x >> 5); p < p1; p += gridDim.x * wpb) {
         const int ns = B.nslot[p];
-        double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-        for (int s = 1; s < ns; ++s) {
-            const int m = B.bcol[s * R + p];
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        if (lane >= 1 && lane < ns) {
+            const int m = B.bcol[sidx(p, lane)];
+            const double *b = B.blk + bidx(p, lane, 0);
             const double x0 = sol[3 * m], x1 = sol[3 * m + 1], x2 = sol[3 * m + 2];
-            const double *b = B.blk + (size_t)s * 9 * R + p;
-            acc0 += b[0] * x0 + b[(size_t)R] * x1 + b[2 * (size_t)R] * x2;
-            acc1 += b[3 * (size_t)R] * x0 + b[4 * (size_t)R] * x1 + b[5 * (size_t)R] * x2;
-            acc2 += b[6 * (size_t)R] * x0 + b[7 * (size_t)R] * x1 + b[8 * (size_t)R] * x2;
+            a0 = b[0] * x0 + b[1] * x1 + b[2] * x2;
+            a1 = b[3] * x0 + b[4] * x1 + b[5] * x2;
+            a2 = b[6] * x0 + b[7] * x1 + b[8] * x2;
         }
-        double D[9];
 #pragma unroll
-        for (int q = 0; q < 9; ++q) D[q] = B.blk[(size_t)q * R + p];
-        const double o0 = sol[3 * n], o1 = sol[3 * n + 1], o2 = sol[3 * n + 2];
-        double x0 = o0, x1 = o1, x2 = o2;
-        double t = (rhs[3 * n] - (acc0 + D[1] * x1 + D[2] * x2)) / D[0];
-        x0 = x0 + 1.2 * (t - x0);
-        t = (rhs[3 * n + 1] - (acc1 + D[3] * x0 + D[5] * x2)) / D[4];
-        x1 = x1 + 1.2 * (t - x1);
-        t = (rhs[3 * n + 2] - (acc2 + D[6] * x0 + D[7] * x1)) / D[8];
-        x2 = x2 + 1.2 * (t - x2);
-        sol[3 * n] = x0;
-        sol[3 * n + 1] = x1;
-        sol[3 * n + 2] = x2;
-        v[0] = (x0 - o0) * (x0 - o0) + (x1 - o1) * (x1 - o1) + (x2 - o2) * (x2 - o2);
-        v[1] = x0 * x0 + x1 * x1 + x2 * x2;
+        for (int o = 16; o > 0; o >>= 1) {
+            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        }
+        if (lane == 0) {
+            const int n = B.perm[p];
+            const double *D = B.blk + bidx(p, 0, 0);
+            const double o0 = sol[3 * n], o1 = sol[3 * n + 1], o2 = sol[3 * n + 2];
+            double x0 = o0, x1 = o1, x2 = o2;
+            double t = (rhs[3 * n] - (a0 + D[1] * x1 + D[2] * x2)) / D[0];
+            x0 = x0 + 1.2 * (t - x0);
+            t = (rhs[3 * n + 1] - (a1 + D[3] * x0 + D[5] * x2)) / D[4];
+            x1 = x1 + 1.2 * (t - x1);
+            t = (rhs[3 * n + 2] - (a2 + D[6] * x0 + D[7] * x1)) / D[8];
+            x2 = x2 + 1.2 * (t - x2);
+            sol[3 * n] = x0;
+            sol[3 * n + 1] = x1;
+            sol[3 * n + 2] = x2;
+            v[0] += (x0 - o0) * (x0 - o0) + (x1 - o1) * (x1 - o1) + (x2 - o2) * (x2 - o2);
+            v[1] += x0 * x0 + x1 * x1 + x2 * x2;
+        }
     }
     block_sum_store<2>(v, part + boff, nblk_tot);
+}
+
+// Whole FACSLS solve in one CTA for small meshes: the same warp-per-row
+// point update as k_sor_colour, colours separated by __syncthreads, and the
+// stopping test (Stif_sol.f90:206-210) evaluated in-block after every sweep.
+// Bounded by maxitl sweeps.  cstart[c] .. cstart[c+1] are the colour ranges.
+__global__ void __launch_bounds__(1024) k_sor_small(BlockDev B, const int *__restrict__ cstart,
+                                                    int ncol, const double *__restrict__ rhs,
+                                                    double *sol, SorCtl *ctl, double tolerl,
+                                                    int maxitl)
+{
+    __shared__ double red[2][32];
+    __shared__ int s_conv;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) s_conv = 0;
+    __syncthreads();
+    int sweeps = 0;
+    double err = 0.0;
+    while (!s_conv && sweeps < maxitl) {
+        double v0 = 0.0, v1 = 0.0;
+        for (int c = 0; c < ncol; ++c) {
+            const int p1 = cstart[c + 1];
+            for (int p = cstart[c] + wid; p < p1; p += nw) {
+                const int ns = B.nslot[p];
+                double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+                if (lane >= 1 && lane < ns) {
+                    const int m = B.bcol[sidx(p, lane)];
+                    const double *b = B.blk + bidx(p, lane, 0);
+                    const double x0 = sol[3 * m], x1 = sol[3 * m + 1], x2 = sol[3 * m + 2];
+                    a0 = b[0] * x0 + b[1] * x1 + b[2] * x2;
+                    a1 = b[3] * x0 + b[4] * x1 + b[5] * x2;
+                    a2 = b[6] * x0 + b[7] * x1 + b[8] * x2;
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+                    a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+                    a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+                }
+                if (lane == 0) {
+                    const int n = B.perm[p];
+                    const double *D = B.blk + bidx(p, 0, 0);
+                    const double o0 = sol[3 * n], o1 = sol[3 * n + 1], o2 = sol[3 * n + 2];
+                    double x0 = o0, x1 = o1, x2 = o2;
+                    double t = (rhs[3 * n] - (a0 + D[1] * x1 + D[2] * x2)) / D[0];
+                    x0 = x0 + 1.2 * (t - x0);
+                    t = (rhs[3 * n + 1] - (a1 + D[3] * x0 + D[5] * x2)) / D[4];
+                    x1 = x1 + 1.2 * (t - x1);
+                    t = (rhs[3 * n + 2] - (a2 + D[6] * x0 + D[7] * x1)) / D[8];
+                    x2 = x2 + 1.2 * (t - x2);
+                    sol[3 * n] = x0;
+                    sol[3 * n + 1] = x1;
+                    sol[3 * n + 2] = x2;
+                    v0 += (x0 - o0) * (x0 - o0) + (x1 - o1) * (x1 - o1) + (x2 - o2) * (x2 - o2);
+                    v1 += x0 * x0 + x1 * x1 + x2 * x2;
+                }
+            }
+            __syncthreads();   // the next colour reads this colour's values
+        }
+        if (lane == 0) {
+            red[0][wid] = v0;
+            red[1][wid] = v1;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double a = 0.0, b = 0.0;
+            for (int i = 0; i < nw; ++i) {
+                a += red[0][i];
+                b += red[1][i];
+            }
+            err = a / b;
+            if (err < tolerl) s_conv = 1;
+            ctl->err = err;
+        }
+        ++sweeps;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        ctl->sweeps = sweeps;
+        ctl->conv = s_conv;
+    }
 }
 
 // End of one sweep: error = sum(dx^2) / sum(x^2) (Stif_sol.f90:206-210).
@@ -515,7 +611,7 @@ __global__ void k_diag_check(BlockDev B, unsigned long long *firstbad)
     const int n = B.perm[p];
 #pragma unroll
     for (int c = 0; c < 3; ++c)
-        if (B.blk[(size_t)(4 * c) * B.R + p] == 0.0) atomicMin(firstbad, (unsigned long long)(3 * n + c));
+        if (B.blk[bidx(p, 0, 4 * c)] == 0.0) atomicMin(firstbad, (unsigned long long)(3 * n + c));
 }
 
 // ---------------------------------------------------------------- updates
@@ -680,17 +776,16 @@ __global__ void k_to_ell(BlockDev B, const int *rowof, int nnod, int ld, const i
     if (row >= 3 * nnod) return;
     const int n = row / 3, r = row % 3;
     const int p = rowof[n];
-    const int R = B.R;
     const int *ir = is + (size_t)row * ld;
     double *out = ss + (size_t)row * ld;
-    out[0] = B.blk[(size_t)(r * 3 + r) * R + p];
+    out[0] = B.blk[bidx(p, 0, r * 3 + r)];
     for (int k = 1; k <= ir[0]; ++k) {
         const int col = ir[k] - 1;
         const int m = col / 3, c = col % 3;
         int slot = -1;
         for (int s = 0; s < B.nslot[p]; ++s)
-            if (B.bcol[s * R + p] == m) { slot = s; break; }
-        out[k] = slot >= 0 ? B.blk[(size_t)(slot * 9 + r * 3 + c) * R + p] : 0.0;
+            if (B.bcol[sidx(p, s)] == m) { slot = s; break; }
+        out[k] = slot >= 0 ? B.blk[bidx(p, slot, r * 3 + c)] : 0.0;
     }
     for (int k = ir[0] + 1; k < ld; ++k) out[k] = 0.0;
 }

@@ -22,9 +22,9 @@ def rel(a, b):
     return float(np.abs(a - b).max() / s) if s > 0 else float(np.abs(a - b).max())
 
 
-def pair(p, threads=4):
+def pair(p, threads=4, mode=abi.FAS_MODE_PLAIN):
     pg, po = p.copy(), p.copy()
-    return GpuSolver(pg), OracleSolver(po, 8, threads=threads), pg, po
+    return GpuSolver(pg, mode=mode), OracleSolver(po, 8, threads=threads), pg, po
 
 
 def test_constitutive_points():
@@ -115,10 +115,16 @@ def test_elvals_suvals_facsls():
     assert rel(pg.ddx, po.ddx) < 1e-10
 
 
-@pytest.mark.parametrize("n,ninc", [((2, 2, 2), 3), ((3, 3, 3), 2), ((8, 8, 8), 1)])
-def test_increments_match(n, ninc):
+@pytest.mark.parametrize("n,ninc,mode", [((2, 2, 2), 3, abi.FAS_MODE_PLAIN),
+                                         ((3, 3, 3), 2, abi.FAS_MODE_PLAIN),
+                                         ((8, 8, 8), 1, abi.FAS_MODE_PLAIN),
+                                         ((3, 3, 3), 1, abi.FAS_MODE_SOR_GRID),
+                                         ((8, 8, 8), 1, abi.FAS_MODE_SOR_GRID)])
+def test_increments_match(n, ninc, mode):
+    """Both SOR launch shapes (one CTA, and grid-wide colour launches) give
+    the checker's iterates."""
     p = generator.structured_cube(n=n, ninc=ninc, seed=7)
-    g, o, pg, po = pair(p, threads=8)
+    g, o, pg, po = pair(p, threads=8, mode=mode)
     for inc in range(1, ninc + 1):
         rg, _ = g.increment(inc)
         ro, _ = o.increment(inc)
