@@ -216,6 +216,10 @@ def moved_bytes(prob, ns: int) -> int:
     return 4 * 3 * prob.nnod * 8 + prob.ngps * per_gp
 
 
+def _state_arrays(p):
+    return {n: getattr(p, n).copy() for n in ("x", "dx", "st", "sv", "ep", "ds", "cumslip")}
+
+
 def run_gpu(args):
     import torch
 
@@ -223,10 +227,10 @@ def run_gpu(args):
     torch.cuda.set_device(local)
     dist = init_dist(ws, "nccl")
     dev = torch.device("cuda", local)
-    from cpfem_code_b200 import GpuSolver, generator
+    from cpfem_code_b200 import GpuSolver, abi, generator
 
     prob = generator.workload(WORKLOAD)
-    ninc_needed = args.warmup + 2 * args.steps + 1
+    ninc_needed = args.warmup + args.steps + 2
     if prob.ninc1 < ninc_needed:
         prob = generator.workload(WORKLOAD, ninc=ninc_needed)
     g = GpuSolver(prob)
@@ -235,59 +239,93 @@ def run_gpu(args):
         inc += 1
         g.increment(inc)
     # the state at the start of the timed increments, kept on the host so the
-    # e2e leg can replay exactly the same increments
+    # e2e and tuned legs replay exactly the same increments
     g.download()
     start = prob.copy()
     inc0 = inc
+    incs = list(range(inc0 + 1, inc0 + args.steps + 1))
+
+    # ---- plain FP64, inputs resident in HBM: one event pair around the region
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
     clocks = ClockSampler(local)
     clocks.start()
-    g.profile(True)
-    nit = 0
-    sweeps = 0
+    g.profile(1)
+    nit = sweeps = 0
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        inc += 1
-        rep, _ = g.increment(inc)
+    for i in incs:
+        rep, _ = g.increment(i)
         nit += len(rep)
         sweeps += sum(r["sor_sweeps"] for r in rep)
-    prof = g.profile(False)
+    prof = g.profile(0)
     wall = time.perf_counter() - t0
     torch.cuda.synchronize()
     clk = clocks.stop()
     dev_s = prof["ms_total"] / 1e3
     t_max, work = reduce_max_sum(dist, dev_s, float(prob.ngps * nit), dev)
     value = work / t_max
+    g.download()
+    plain_end = _state_arrays(prob)
 
-    # e2e: the same increments again through the ABI, the whole state copied
-    # from pinned host memory before and back after every increment
-    nit_e, e2e_s = 0, 0.0
+    # ---- e2e: the same increments through the ABI, state from pinned host memory
+    nit_e, e2e_s, deterministic = 0, 0.0, None
     if not args.no_e2e:
-        host = start
+        host = start.copy()
         pinned_like(host)
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
         t0 = time.perf_counter()
-        for k in range(args.steps):
+        for i in incs:
             g.upload(host)
-            rep, _ = g.increment(inc0 + 1 + k)
+            rep, _ = g.increment(i)
             g.download(host)
             nit_e += len(rep)
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
-        prob = host
-    else:
-        g.download()
+        deterministic = all(np.array_equal(v, getattr(host, k)) for k, v in plain_end.items())
     te, work_e = reduce_max_sum(dist, e2e_s, float(prob.ngps * nit_e), dev)
-    mb = moved_bytes(prob, int(prob.nss.max()))
+
+    # ---- tuned form: FP32 SOR sweeps with FP64 residual refinement
+    tuned = None
+    if not args.no_tuned:
+        t = start.copy()
+        g.upload(t)
+        g.set_mode(abi.FAS_MODE_SOR_FP32)
+        torch.cuda.synchronize()
+        g.profile(1)
+        nit_t = 0
+        for i in incs:
+            rep, _ = g.increment(i)
+            nit_t += len(rep)
+        prof_t = g.profile(0)
+        g.set_mode(abi.FAS_MODE_PLAIN)
+        g.download(t)
+        st_ref, st_t = plain_end["st"], t.st
+        tt, work_t = reduce_max_sum(dist, prof_t["ms_total"] / 1e3, float(prob.ngps * nit_t), dev)
+        tuned = {"mode": "FP32-matrix SOR sweeps, FP64 residual refinement every 16 sweeps",
+                 "value": work_t / tt, "s_per_increment": tt / args.steps, "newton_iters": nit_t,
+                 "sor_sweeps": int(prof_t["sor_sweeps"]),
+                 "speedup_vs_plain_s_per_increment": (t_max / args.steps) / (tt / args.steps),
+                 "stress_err_per_point": float(np.abs(st_t - st_ref).max() / np.abs(st_ref).max()),
+                 "stress_err_macro": float(abs(st_t[:, 0].mean() - st_ref[:, 0].mean())
+                                           / abs(st_ref[:, 0].mean())),
+                 "err_reference": "plain FP64 GPU path (equal to the FP64 checker to ~1e-15)"}
+
+    # ---- per-kernel CUDA-event timing of one more increment (roofline)
+    k = start.copy()
+    g.upload(k)
+    torch.cuda.synchronize()
+    g.profile(2)
+    g.increment(incs[0])
+    prof_k = g.profile(0)
 
     if rank == 0:
         pk = peaks()
-        achieved = prof["sor_bytes"] / (prof["ms_sor_colour"] / 1e3) / 1e9 if prof["ms_sor_colour"] else 0.0
-        launch_ms = prof["ms_sor_colour"] / max(prof["n_sor_colour"], 1)
+        achieved = (prof_k["sor_bytes"] / (prof_k["ms_sor_colour"] / 1e3) / 1e9
+                    if prof_k["ms_sor_colour"] else 0.0)
+        launch_ms = prof_k["ms_sor_colour"] / max(prof_k["n_sor_colour"], 1)
         line = {
             "metric": METRIC,
             "value": value, "unit": "GP-updates/s", "n_gpus": ws, "steps": args.steps,
@@ -295,35 +333,40 @@ def run_gpu(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator, fs3pre semantics)",
             "config": {"workload": WORKLOAD, "desc": DESC, "parallelism": f"replicas{ws}",
-                       "increments": [args.warmup + 1, args.warmup + args.steps],
-                       "newton_iters": nit, "sor_sweeps": sweeps,
+                       "increments": [incs[0], incs[-1]], "newton_iters": nit, "sor_sweeps": sweeps,
                        "l2": "inputs larger than L2 (534 MB block matrix re-read every sweep)"},
             "s_per_increment": t_max / args.steps,
             "wall_s": wall,
-            "phases_ms": {"constitutive": prof["ms_constitutive"], "assembly": prof["ms_assembly"],
-                          "sor_colour": prof["ms_sor_colour"], "total": prof["ms_total"]},
-            "constitutive_gp_updates_per_s": prof["gp_updates"] / (prof["ms_constitutive"] / 1e3)
-            if prof["ms_constitutive"] else None,
             "gpu_launches": int(prof["n_launches"]),
+            "phases_ms_profiled_increment": {
+                "constitutive": prof_k["ms_constitutive"], "assembly": prof_k["ms_assembly"],
+                "sor_colour": prof_k["ms_sor_colour"], "total": prof_k["ms_total"]},
+            "constitutive_gp_updates_per_s": prof_k["gp_updates"] / (prof_k["ms_constitutive"] / 1e3)
+            if prof_k["ms_constitutive"] else None,
             "roofline": {"kernel": "k_sor_colour", "bound": "hbm", "achieved": achieved,
                          "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
                          "peak_source": pk["source"], "traffic": None,
                          "launch_ms": launch_ms,
-                         "bytes_per_launch": prof["sor_bytes"] / max(prof["n_sor_colour"], 1)},
+                         "bytes_per_launch": prof_k["sor_bytes"] / max(prof_k["n_sor_colour"], 1),
+                         "timed": f"CUDA events around every launch of increment {incs[0]}"},
             "clocks": clk,
             "e2e": {"value": work_e / te if te > 0 else None, "unit": "GP-updates/s",
-                    "h2d_bytes_per_step": mb, "d2h_bytes_per_step": mb,
+                    "h2d_bytes_per_step": moved_bytes(prob, int(prob.nss.max())),
+                    "d2h_bytes_per_step": moved_bytes(prob, int(prob.nss.max())),
                     "s_per_increment": te / args.steps if te > 0 else None,
-                    "newton_iters": nit_e, "increments": [inc0 + 1, inc0 + args.steps]},
+                    "newton_iters": nit_e, "increments": [incs[0], incs[-1]],
+                    "same_result_as_resident_run": deterministic},
+            "tuned": tuned,
         }
         if ws == 1 and not args.no_cpu:
-            # the state after the e2e increments is plastic: time the first
+            # plastic state at the end of the timed increments: time the first
             # Newton iteration of the next increment on the host cores
-            s = cpu_sample(prob, inc + 1, 0, 1, os.cpu_count() or 1)
+            # `prob` still holds the whole state downloaded after the timed run
+            s = cpu_sample(prob, incs[-1] + 1, 0, 1, os.cpu_count() or 1)
             line["cpu_baseline"] = {
                 "value": s["value"], "unit": "GP-updates/s", "cores": os.cpu_count() or 1,
                 "kind": "port",
-                "sample": f"Newton iteration 1 of increment {inc + 1} ({s['sweeps']} SOR sweeps) "
+                "sample": f"Newton iteration 1 of increment {incs[-1] + 1} ({s['sweeps']} SOR sweeps) "
                           f"by the C++ restatement from the same state, {s['seconds']:.1f} s"}
         print(json.dumps(line), flush=True)
     g.close()
@@ -341,6 +384,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer (e2e) leg")
+    ap.add_argument("--no-tuned", action="store_true", help="skip the tuned-form (FP32 SOR) leg")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

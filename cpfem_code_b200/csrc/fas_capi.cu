@@ -97,10 +97,14 @@ struct fas_handle {
     // block layout
     int ncol = 0;
     std::vector<int> col_start;
-    std::vector<double> col_bytes;
+    std::vector<double> col_bytes, col_bytes32;   // algorithmic bytes per colour launch
     DVec<int> perm, rowof, nslot, bcol;
     DVec<unsigned> bloc;
     DVec<double> blk;
+    DVec<float> blk32;           // FP32 copy for FAS_MODE_SOR_FP32
+    DVec<double> sor_d, sor_r;   // correction and residual of the refinement
+    int refine_every = 16;       // FP32 sweeps per FP64 residual
+    bool blk32_fresh = false;    // the last assembly wrote blk32
     // reductions and control
     std::vector<int> sor_boff, sor_nblk;
     DVec<int> d_cstart;          // colour ranges for the one-CTA SOR
@@ -114,8 +118,9 @@ struct fas_handle {
     // staging for state transfer
     DVec<unsigned char> stage;
     DVec<TwinEv> events;
-    // profiling
-    bool prof = false;
+    // profiling: 0 off, 1 counters + one event pair around the region,
+    // 2 also an event pair around every phase kernel launch
+    int prof = 0;
     fas_profile P{};
     std::vector<cudaEvent_t> ev_pool;
     std::vector<std::pair<std::pair<cudaEvent_t, cudaEvent_t>, double *>> pending;
@@ -154,6 +159,7 @@ struct fas_handle {
     {
         BlockDev b;
         b.R = nnod; b.perm = perm.p; b.nslot = nslot.p; b.bcol = bcol.p; b.bloc = bloc.p; b.blk = blk.p;
+        b.blk32 = (mode & FAS_MODE_SOR_FP32) ? blk32.p : nullptr;
         return b;
     }
 };
@@ -200,7 +206,7 @@ struct Span {                    // event pair around one launch while profiling
     double *acc;
     explicit Span(fas_handle *hh, double *accum) : h(hh), acc(accum)
     {
-        if (h->prof) {
+        if (h->prof >= 2) {
             a = take_event(h);
             b = take_event(h);
             cudaEventRecord(a, h->stream);
@@ -317,9 +323,12 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
     // algorithmic bytes of one colour launch: blocks and column ids of the
     // row, perm + nslot, and rhs read + solution read/write of its node
     h->col_bytes.assign(h->ncol, 0.0);
+    h->col_bytes32.assign(h->ncol, 0.0);
     for (int c = 0; c < h->ncol; ++c)
-        for (int p = h->col_start[c]; p < h->col_start[c + 1]; ++p)
+        for (int p = h->col_start[c]; p < h->col_start[c + 1]; ++p) {
             h->col_bytes[c] += nslot[p] * (72.0 + 4.0) + 8.0 + 72.0;
+            h->col_bytes32[c] += nslot[p] * (36.0 + 4.0) + 8.0 + 72.0 + 24.0;
+        }
     // algorithmic bytes of one assembly launch: each element record read
     // once (52 used doubles), each block written once, the slot tables and
     // node adjacency read once, fc and ddx written
@@ -345,9 +354,11 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
     int tot = 0;
     for (int c = 0; c < h->ncol; ++c) {
         h->sor_boff[c] = tot;
-        // warp per row, 8 rows per block, at most 8 blocks per SM resident
+        // warp per row, 8 rows per block; at most 4 blocks per SM, whose
+        // warps stride over the colour's rows, keeps the per-sweep partial
+        // sums few enough for a cheap deterministic check
         h->sor_nblk[c] = (int)std::min<long long>(nblocks(h->col_start[c + 1] - h->col_start[c], 8),
-                                                   (long long)h->nsm * 8);
+                                                   (long long)h->nsm * 4);
         tot += h->sor_nblk[c];
     }
     h->sor_nblk_tot = std::max(tot, 1);
@@ -708,9 +719,21 @@ template <int NS> int launch_elem(fas_handle *h, int inc, int nit)
 
 // ELVALS (+ SUVALS when bc): element pass then row-gather assembly.
 // Returns the first element's FAFERR code in element order, if any.
+int ensure_fp32(fas_handle *h)
+{
+    if (!(h->mode & FAS_MODE_SOR_FP32) || h->blk32.p || h->point_mode) return 0;
+    const size_t nd3 = 3 * (size_t)h->nnod;
+    CKA(h->blk32.alloc((size_t)SLOTS * 9 * h->nnod));
+    CKA(h->sor_d.alloc(nd3));
+    CKA(h->sor_r.alloc(nd3));
+    CK(h->blk32.zero(h->stream));
+    return 0;
+}
+
 int elvals_impl(fas_handle *h, int inc, int nit, bool bc)
 {
     cudaStream_t s = h->stream;
+    if (int rc = ensure_fp32(h)) return rc;
     CK(cudaMemsetAsync(h->ekey.p, 0xFF, sizeof(unsigned long long), s));
     CK(cudaMemsetAsync(h->flags.p, 0, sizeof(int), s));
     int rc;
@@ -732,6 +755,7 @@ int elvals_impl(fas_handle *h, int inc, int nit, bool bc)
         keep(h, sp);
         LAUNCHED(h);
         h->P.n_assembly++;
+        h->blk32_fresh = h->block().blk32 != nullptr;
         h->P.assembly_bytes += h->asm_bytes;
     }
     CK(cudaMemcpyAsync(h->hc->ekey, h->ekey.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
@@ -785,6 +809,45 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
         CK(cudaStreamSynchronize(s));
     }
     int done = small ? 1000 : 0, chunk = 4;
+    const bool fp32 = !small && (h->mode & FAS_MODE_SOR_FP32) && h->blk32.p && h->blk32_fresh;
+    if (fp32) {
+        // x (= ddx) starts at 0, so the first residual is rhs itself
+        CK(cudaMemcpyAsync(h->sor_r.p, h->rhs.p, nd3 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemsetAsync(h->sor_d.p, 0, nd3 * sizeof(double), s));
+        const int m = h->refine_every;
+        const unsigned rblk = (unsigned)std::min<long long>(nblocks(h->nnod, 8), (long long)h->nsm * 8);
+        int outer_per_chunk = 1;
+        while (done < 1000) {
+            for (int o = 0; o < outer_per_chunk && done < 1000; ++o) {
+                const int k = std::min(m, 1000 - done);
+                for (int it = 0; it < k; ++it) {
+                    for (int c = 0; c < h->ncol; ++c) {
+                        const int p0 = h->col_start[c], p1 = h->col_start[c + 1];
+                        if (p1 <= p0) continue;
+                        Span sp(h, &h->P.ms_sor_colour);
+                        k_sor_colour32<<<h->sor_nblk[c], 256, 0, s>>>(B, p0, p1, h->sor_r.p, h->ddx.p, h->sor_d.p,
+                                                                     h->sorctl.p, h->part_sor.p, h->sor_boff[c],
+                                                                     h->sor_nblk_tot);
+                        sp.end();
+                        keep(h, sp);
+                        LAUNCHED(h);
+                    }
+                    k_sor_check<<<1, 1024, 0, s>>>(h->part_sor.p, h->sor_nblk_tot, h->sorctl.p, tolerl);
+                    LAUNCHED(h);
+                }
+                done += k;
+                k_fold<<<nblocks((long long)nd3, 256), 256, 0, s>>>((int)nd3, h->ddx.p, h->sor_d.p);
+                LAUNCHED(h);
+                k_residual<<<rblk, 256, 0, s>>>(B, h->rhs.p, h->ddx.p, h->sor_r.p, h->sorctl.p);
+                LAUNCHED(h);
+            }
+            CK(cudaMemcpyAsync(&h->hc->sor, h->sorctl.p, sizeof(SorCtl), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            if (h->hc->sor.conv) break;
+            outer_per_chunk = std::min(outer_per_chunk * 2, 4);
+        }
+        done = 1000;
+    }
     while (done < 1000) {
         const int k = std::min(chunk, 1000 - done);
         for (int it = 0; it < k; ++it) {
@@ -813,6 +876,10 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
     h->P.n_sor_colour += small ? 1 : (int64_t)nsw * h->ncol;
     double bytes = 0.0;
     for (double b : h->col_bytes) bytes += b;
+    if (fp32) {   // FP32 blocks: 36 + 4 bytes per slot, plus the xs read
+        bytes = 0.0;
+        for (double b : h->col_bytes32) bytes += b;
+    }
     h->P.sor_bytes += bytes * nsw;
     if (sweeps) *sweeps = nsw;
     if (error) *error = h->hc->sor.err;
@@ -1167,10 +1234,10 @@ int32_t fas_gpu_profile(fas_handle *h, int32_t enable, fas_profile *out)
     if (enable) {
         h->P = fas_profile{};
         h->launches = 0;
-        h->prof = true;
+        h->prof = enable >= 2 ? 2 : 1;
         CK(cudaEventRecord(h->ev_t0, h->stream));
     } else {
-        h->prof = false;
+        h->prof = 0;
     }
     return 0;
 }

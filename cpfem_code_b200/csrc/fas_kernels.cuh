@@ -7,9 +7,11 @@
 //     upper triangle (21) -- written once per Newton iteration by the element
 //     kernel and read by the row-gather assembly;
 //   * stiffness: block-ELL of 3x3 node blocks, rows permuted so each SOR
-//     colour is a contiguous row range, row-major: the 27 blocks of a row
-//     are 1944 contiguous bytes, blk[((row*27 + slot)*9 + r*3 + c)];
-//     slot 0 = the diagonal block, bcol[row*27 + slot] = column node.
+//     colour is a contiguous row range.  The 27 blocks of a row are 1944
+//     contiguous bytes, component-major: blk[(row*9 + r*3 + c)*27 + slot],
+//     so one component of all slots of a row is 216 contiguous bytes (one
+//     coalesced warp load).  Slot 0 = the diagonal block,
+//     bcol[row*27 + slot] = column node.
 #pragma once
 
 #include "fas_device.cuh"
@@ -23,7 +25,7 @@ constexpr int MAXADJ = 8;        // elements per node
 
 // block matrix addressing (row-major rows of SLOTS 3x3 blocks)
 __host__ __device__ __forceinline__ size_t sidx(int p, int s) { return (size_t)p * 27 + s; }
-__host__ __device__ __forceinline__ size_t bidx(int p, int s, int q) { return ((size_t)p * 27 + s) * 9 + q; }
+__host__ __device__ __forceinline__ size_t bidx(int p, int s, int q) { return ((size_t)p * 9 + q) * 27 + s; }
 
 // upper-triangle index of chi(i,j), i <= j (0-based)
 __host__ __device__ __forceinline__ int utri(int i, int j) { return i * 6 - (i * (i - 1)) / 2 + (j - i); }
@@ -46,7 +48,8 @@ struct BlockDev {
     const int *bcol;     // [R][SLOTS] column node of each slot
     const unsigned *bloc;// [R][SLOTS] 4-bit local index of the column node in
                          // each adjacent element of the row node (0xF: absent)
-    double *blk;         // [R][SLOTS][9]
+    double *blk;         // [R][9][SLOTS]
+    float *blk32;        // FP32 copy of blk (tuned mode), or null
 };
 
 // ---------------------------------------------------------------- element pass
@@ -317,6 +320,10 @@ __global__ void __launch_bounds__(256) k_assemble(MeshDev Mh, BlockDev B,
     }
 #pragma unroll
     for (int q = 0; q < 9; ++q) B.blk[bidx(p, s, q)] = acc[q];
+    if (B.blk32) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) B.blk32[bidx(p, s, q)] = (float)acc[q];
+    }
 }
 
 // Stand-alone SUVALS (src/fasolt/Bconds.f90:19-113): ddx = fc, then the
@@ -337,6 +344,10 @@ __global__ void k_suvals(MeshDev Mh, BlockDev B, const int *rowof, const double 
         if (apply_bc(ibc, n, x, dx, xspec, fspec, nxs, nfs, efix, D, f)) *bad_bc = 1;
 #pragma unroll
         for (int q = 0; q < 9; ++q) B.blk[bidx(p, 0, q)] = D[q];
+        if (B.blk32) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) B.blk32[bidx(p, 0, q)] = (float)D[q];
+        }
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) ddx[3 * n + c] = f[c];
@@ -435,6 +446,60 @@ struct SorCtl {
     double pad;
 };
 
+// The point-SOR update of one row (FACSLS's inner loop, Stif_sol.f90:189-197,
+// for the three DOFs of one node) by one warp: lane s (1 <= s < nslot)
+// multiplies the off-diagonal block of slot s (stored as T) by the current
+// solution at its column node, the warp sums the products, and lane 0
+// updates x, y, z in turn with the diagonal block.  Returns in lane 0 the
+// squared change and the squared new values; `base` (may be null) is added
+// to the iterate for the latter (the refinement form).
+template <typename T>
+__device__ __forceinline__ void sor_row(const BlockDev &B, const T *__restrict__ blk, int p, int lane,
+                                        const double *__restrict__ rhs, double *sol,
+                                        const double *__restrict__ base, double &dv, double &vv)
+{
+    const int ns = B.nslot[p];
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    if (lane >= 1 && lane < ns) {
+        const int m = B.bcol[sidx(p, lane)];
+        const T *b = blk + bidx(p, lane, 0);
+        const double x0 = sol[3 * m], x1 = sol[3 * m + 1], x2 = sol[3 * m + 2];
+        a0 = (double)b[0 * 27] * x0 + (double)b[1 * 27] * x1 + (double)b[2 * 27] * x2;
+        a1 = (double)b[3 * 27] * x0 + (double)b[4 * 27] * x1 + (double)b[5 * 27] * x2;
+        a2 = (double)b[6 * 27] * x0 + (double)b[7 * 27] * x1 + (double)b[8 * 27] * x2;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+    }
+    if (lane == 0) {
+        const int n = B.perm[p];
+        double D[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) D[q] = (double)blk[bidx(p, 0, q)];
+        const double o0 = sol[3 * n], o1 = sol[3 * n + 1], o2 = sol[3 * n + 2];
+        double x0 = o0, x1 = o1, x2 = o2;
+        double t = (rhs[3 * n] - (a0 + D[1] * x1 + D[2] * x2)) / D[0];
+        x0 = x0 + 1.2 * (t - x0);
+        t = (rhs[3 * n + 1] - (a1 + D[3] * x0 + D[5] * x2)) / D[4];
+        x1 = x1 + 1.2 * (t - x1);
+        t = (rhs[3 * n + 2] - (a2 + D[6] * x0 + D[7] * x1)) / D[8];
+        x2 = x2 + 1.2 * (t - x2);
+        sol[3 * n] = x0;
+        sol[3 * n + 1] = x1;
+        sol[3 * n + 2] = x2;
+        dv += (x0 - o0) * (x0 - o0) + (x1 - o1) * (x1 - o1) + (x2 - o2) * (x2 - o2);
+        if (base) {
+            x0 += base[3 * n];
+            x1 += base[3 * n + 1];
+            x2 += base[3 * n + 2];
+        }
+        vv += x0 * x0 + x1 * x1 + x2 * x2;
+    }
+}
+
 // One warp per row: lane s (1 <= s < nslot) multiplies the off-diagonal
 // block of slot s by the current solution at its column node; the warp sums
 // the three products; lane 0 then updates x, y, z in turn with the diagonal
@@ -450,41 +515,8 @@ __global__ void __launch_bounds__(256) k_sor_colour(BlockDev B, int p0, int p1,
     const int lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
     double v[2] = {0.0, 0.0};
-    for (int p = p0 + blockIdx.x * wpb + (threadIdx.x >> 5); p < p1; p += gridDim.x * wpb) {
-        const int ns = B.nslot[p];
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        if (lane >= 1 && lane < ns) {
-            const int m = B.bcol[sidx(p, lane)];
-            const double *b = B.blk + bidx(p, lane, 0);
-            const double x0 = sol[3 * m], x1 = sol[3 * m + 1], x2 = sol[3 * m + 2];
-            a0 = b[0] * x0 + b[1] * x1 + b[2] * x2;
-            a1 = b[3] * x0 + b[4] * x1 + b[5] * x2;
-            a2 = b[6] * x0 + b[7] * x1 + b[8] * x2;
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
-        }
-        if (lane == 0) {
-            const int n = B.perm[p];
-            const double *D = B.blk + bidx(p, 0, 0);
-            const double o0 = sol[3 * n], o1 = sol[3 * n + 1], o2 = sol[3 * n + 2];
-            double x0 = o0, x1 = o1, x2 = o2;
-            double t = (rhs[3 * n] - (a0 + D[1] * x1 + D[2] * x2)) / D[0];
-            x0 = x0 + 1.2 * (t - x0);
-            t = (rhs[3 * n + 1] - (a1 + D[3] * x0 + D[5] * x2)) / D[4];
-            x1 = x1 + 1.2 * (t - x1);
-            t = (rhs[3 * n + 2] - (a2 + D[6] * x0 + D[7] * x1)) / D[8];
-            x2 = x2 + 1.2 * (t - x2);
-            sol[3 * n] = x0;
-            sol[3 * n + 1] = x1;
-            sol[3 * n + 2] = x2;
-            v[0] += (x0 - o0) * (x0 - o0) + (x1 - o1) * (x1 - o1) + (x2 - o2) * (x2 - o2);
-            v[1] += x0 * x0 + x1 * x1 + x2 * x2;
-        }
-    }
+    for (int p = p0 + blockIdx.x * wpb + (threadIdx.x >> 5); p < p1; p += gridDim.x * wpb)
+        sor_row<double>(B, B.blk, p, lane, rhs, sol, nullptr, v[0], v[1]);
     block_sum_store<2>(v, part + boff, nblk_tot);
 }
 
@@ -508,41 +540,8 @@ __global__ void __launch_bounds__(1024) k_sor_small(BlockDev B, const int *__res
         double v0 = 0.0, v1 = 0.0;
         for (int c = 0; c < ncol; ++c) {
             const int p1 = cstart[c + 1];
-            for (int p = cstart[c] + wid; p < p1; p += nw) {
-                const int ns = B.nslot[p];
-                double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-                if (lane >= 1 && lane < ns) {
-                    const int m = B.bcol[sidx(p, lane)];
-                    const double *b = B.blk + bidx(p, lane, 0);
-                    const double x0 = sol[3 * m], x1 = sol[3 * m + 1], x2 = sol[3 * m + 2];
-                    a0 = b[0] * x0 + b[1] * x1 + b[2] * x2;
-                    a1 = b[3] * x0 + b[4] * x1 + b[5] * x2;
-                    a2 = b[6] * x0 + b[7] * x1 + b[8] * x2;
-                }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-                    a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-                    a2 += __shfl_xor_sync(0xffffffffu, a2, o);
-                }
-                if (lane == 0) {
-                    const int n = B.perm[p];
-                    const double *D = B.blk + bidx(p, 0, 0);
-                    const double o0 = sol[3 * n], o1 = sol[3 * n + 1], o2 = sol[3 * n + 2];
-                    double x0 = o0, x1 = o1, x2 = o2;
-                    double t = (rhs[3 * n] - (a0 + D[1] * x1 + D[2] * x2)) / D[0];
-                    x0 = x0 + 1.2 * (t - x0);
-                    t = (rhs[3 * n + 1] - (a1 + D[3] * x0 + D[5] * x2)) / D[4];
-                    x1 = x1 + 1.2 * (t - x1);
-                    t = (rhs[3 * n + 2] - (a2 + D[6] * x0 + D[7] * x1)) / D[8];
-                    x2 = x2 + 1.2 * (t - x2);
-                    sol[3 * n] = x0;
-                    sol[3 * n + 1] = x1;
-                    sol[3 * n + 2] = x2;
-                    v0 += (x0 - o0) * (x0 - o0) + (x1 - o1) * (x1 - o1) + (x2 - o2) * (x2 - o2);
-                    v1 += x0 * x0 + x1 * x1 + x2 * x2;
-                }
-            }
+            for (int p = cstart[c] + wid; p < p1; p += nw)
+                sor_row<double>(B, B.blk, p, lane, rhs, sol, nullptr, v0, v1);
             __syncthreads();   // the next colour reads this colour's values
         }
         if (lane == 0) {
@@ -567,6 +566,70 @@ __global__ void __launch_bounds__(1024) k_sor_small(BlockDev B, const int *__res
         ctl->sweeps = sweeps;
         ctl->conv = s_conv;
     }
+}
+
+// ---------------------------------------------------------------- FP32 SOR
+// Tuned FACSLS: sweeps of point SOR on the correction equation K32 d = r with
+// the FP32 copy of the matrix (half the bytes of a sweep), FP64 vectors and
+// arithmetic.  xs is the iterate at the last residual; the stopping measure
+// is the reference's, on the iterate xs + d: sum(change^2) / sum((xs+d)^2).
+__global__ void __launch_bounds__(256) k_sor_colour32(BlockDev B, int p0, int p1,
+                                                      const double *__restrict__ res,
+                                                      const double *__restrict__ xs, double *d,
+                                                      const SorCtl *ctl, double *part, int boff,
+                                                      int nblk_tot)
+{
+    if (((volatile const SorCtl *)ctl)->conv) return;
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    double v[2] = {0.0, 0.0};
+    for (int p = p0 + blockIdx.x * wpb + (threadIdx.x >> 5); p < p1; p += gridDim.x * wpb)
+        sor_row<float>(B, B.blk32, p, lane, res, d, xs, v[0], v[1]);
+    block_sum_store<2>(v, part + boff, nblk_tot);
+}
+
+// FP64 residual of the assembled system, r = rhs - K x, one warp per row.
+// Skipped once the solve has converged.
+__global__ void __launch_bounds__(256) k_residual(BlockDev B, const double *__restrict__ rhs,
+                                                  const double *__restrict__ x, double *r,
+                                                  const SorCtl *ctl)
+{
+    if (((volatile const SorCtl *)ctl)->conv) return;
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    for (int p = blockIdx.x * wpb + (threadIdx.x >> 5); p < B.R; p += gridDim.x * wpb) {
+        const int ns = B.nslot[p];
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        if (lane < ns) {
+            const int m = B.bcol[sidx(p, lane)];
+            const double *b = B.blk + bidx(p, lane, 0);
+            const double x0 = x[3 * m], x1 = x[3 * m + 1], x2 = x[3 * m + 2];
+            a0 = b[0 * 27] * x0 + b[1 * 27] * x1 + b[2 * 27] * x2;
+            a1 = b[3 * 27] * x0 + b[4 * 27] * x1 + b[5 * 27] * x2;
+            a2 = b[6 * 27] * x0 + b[7 * 27] * x1 + b[8 * 27] * x2;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        }
+        if (lane == 0) {
+            const int n = B.perm[p];
+            r[3 * n] = rhs[3 * n] - a0;
+            r[3 * n + 1] = rhs[3 * n + 1] - a1;
+            r[3 * n + 2] = rhs[3 * n + 2] - a2;
+        }
+    }
+}
+
+// x += d, d = 0 (end of one refinement step).
+__global__ void k_fold(int ndof, double *x, double *d)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ndof) return;
+    x[i] += d[i];
+    d[i] = 0.0;
 }
 
 // End of one sweep: error = sum(dx^2) / sum(x^2) (Stif_sol.f90:206-210).

@@ -77,6 +77,90 @@ def fcc_aluminium(m: float = 0.05, h0: float = 150.0, tau_sat: float = 80.0,
                 smatrx=np.ones((ns, ns)))
 
 
+def _mb_direction(uvtw, ca):
+    """Miller-Bravais direction [uvtw] -> Cartesian, a1 along x."""
+    u, v, t, w = uvtw
+    return np.array([u - 0.5 * v - 0.5 * t, (v - t) * math.sqrt(3.0) / 2.0, w * ca])
+
+
+def _mb_normal(hkil, ca):
+    """Miller-Bravais plane (hkil) -> Cartesian normal, a1 along x."""
+    h, k, i, l = hkil
+    return np.array([h, (h + 2.0 * k) / math.sqrt(3.0), l / ca])
+
+
+def _family(planes, dirs, ca):
+    """All (plane, direction) pairs of the two index families that satisfy
+    the zone law h*u + k*v + i*t + l*w = 0, planes in the given order."""
+    out = []
+    for pl in planes:
+        for d in dirs:
+            if sum(a * b for a, b in zip(pl, d)) == 0:
+                n = _mb_normal(pl, ca)
+                b = _mb_direction(d, ca)
+                out.append((b / np.linalg.norm(b), n / np.linalg.norm(n)))
+    return out
+
+
+def _perms4(base):
+    """The six hexagonal variants of a Miller-Bravais index (cyclic
+    permutations of the first three indices, and their negatives in those
+    indices), duplicates removed, order kept."""
+    h, k, i, l = base
+    seen, out = set(), []
+    for a, b, c in ((h, k, i), (i, h, k), (k, i, h), (-h, -k, -i), (-i, -h, -k), (-k, -i, -h)):
+        t = (a, b, c, l)
+        if t not in seen:
+            seen.add(t)
+            out.append(t)
+    return out
+
+
+def hcp_systems(ca: float = 1.593):
+    """30 HCP systems: basal <a> (3), prismatic <a> (3), first-order
+    pyramidal <c+a> (12), second-order pyramidal <c+a> (6) and {10-12}
+    tension twins (6) -- the families of
+    additional_files/slip_systems/Zirconium that the mixed workload uses,
+    derived here from their Miller-Bravais indices for c/a = `ca`.
+    Returns ab, an (unit vectors) and a family label per system."""
+    a_dirs = [(2, -1, -1, 0), (-1, 2, -1, 0), (-1, -1, 2, 0)]
+    ca_dirs = _perms4((-1, -1, 2, 3))
+    fam = []
+    fam += [(s, "basal") for s in _family([(0, 0, 0, 1)], a_dirs, ca)]
+    fam += [(s, "prism") for s in _family(_perms4((1, 0, -1, 0))[:3], a_dirs, ca)]
+    fam += [(s, "pyr1ca") for s in _family(_perms4((1, 0, -1, 1)), ca_dirs, ca)]
+    fam += [(s, "pyr2ca") for s in _family(_perms4((1, 1, -2, 2)), ca_dirs, ca)]
+    twin_dirs = [d for d in _perms4((-1, 0, 1, 1))]
+    fam += [(s, "twin") for s in _family(_perms4((1, 0, -1, 2)), twin_dirs, ca)]
+    ab = np.array([f[0][0] for f in fam])
+    an = np.array([f[0][1] for f in fam])
+    labels = [f[1] for f in fam]
+    return ab, an, labels
+
+
+def hcp_zirconium(ca: float = 1.593, m: float = 0.05) -> dict:
+    """HCP zirconium: compliances of additional_files/compliances (Zr line),
+    the 30 systems of :func:`hcp_systems`, Voce hardening per family and
+    {10-12} twins that reorient by 180 - 2 atan(sqrt(3)/(c/a)) degrees
+    (85.2 for c/a = 1.593) -- the twin test of SLPINI needs |ssang| > 1.5."""
+    ab, an, labels = hcp_systems(ca)
+    ns = len(labels)
+    assert ns == 30
+    e = np.array([10.2e-6, 10.2e-6, 8.01e-6, -2.46e-6, -2.46e-6, -4.09e-6, 29.94e-6, 29.94e-6, 28.58e-6])
+    tw = 180.0 - 2.0 * math.degrees(math.atan(math.sqrt(3.0) / ca))
+    crss = {"basal": 45.0, "prism": 25.0, "pyr1ca": 90.0, "pyr2ca": 90.0, "twin": 30.0}
+    ampar = np.zeros((ns, 10))
+    ssang = np.zeros(ns)
+    tau0 = np.zeros(ns)
+    for k, lab in enumerate(labels):
+        ampar[k, :6] = (m, 200.0, 0.0, 1.0, 2.5 * crss[lab], 0.0)
+        tau0[k] = crss[lab]
+        if lab == "twin":
+            ssang[k] = tw
+    return dict(name="hcp-zr", ns=ns, e=e, ssang=ssang, ab=ab, an=an, ampar=ampar,
+                smatrx=np.ones((ns, ns)), tau0=tau0, labels=labels)
+
+
 def pack_materials(mats: list[dict]):
     """Material tables in the FAS_CPL layout (ld_ss = 60)."""
     nm = len(mats)
@@ -250,7 +334,10 @@ def structured_cube(n=(8, 8, 8), lengths=(1.0, 1.0, 1.0), xfree: int = 3,
     t0 = np.broadcast_to(np.asarray(tau0, float), (nm,))
     for k in range(nm):
         sel = le == k + 1
-        prob.sv[sel, 3:3 + nss[k]] = t0[k]
+        if "tau0" in materials[k]:
+            prob.sv[sel, 3:3 + nss[k]] = np.asarray(materials[k]["tau0"], float)[None, :]
+        else:
+            prob.sv[sel, 3:3 + nss[k]] = t0[k]
     prob.meta.update(dict(n=(nx, ny, nz), lengths=tuple(lengths), xfree=xfree, grain=grain,
                           seed=seed, grain_id=grain_id.astype(np.int32),
                           materials=[m["name"] for m in materials]))
@@ -347,6 +434,17 @@ def cube_config(n: int, ninc: int, grain: int, seed: int, eps: float = 1.0e-3,
                            grain=grain, seed=seed, ctrl=ctrl)
 
 
+def mixed_config(n: int = 32, ninc: int = 20, seed: int = 32, eps: float = 1.0e-3,
+                 ctrl: Control | None = None) -> Problem:
+    """n^3 cube of 50/50 random HCP-Zr / FCC-Al grains of 2^3 elements in
+    uniaxial tension; HCP is material 1 (DoReorient reads material 1's
+    tables, Fasolt3.f90:103,124-125), twins fire with probability 1, at most
+    once per GP."""
+    return structured_cube(n=(n, n, n), xfree=3, eps_inc=(eps, 0.0, 0.0), ninc=ninc, grain=2,
+                           materials=[hcp_zirconium(), fcc_aluminium()], fractions=[0.5, 0.5],
+                           seed=seed, twinlim=1, twinprob=1.0, ctrl=ctrl)
+
+
 WORKLOADS = {
     # 8^3 FCC, one grain per element, 10 increments to 1 %
     "cube8": dict(n=8, ninc=10, grain=1, seed=8),
@@ -358,6 +456,10 @@ WORKLOADS = {
 
 
 def workload(name: str, **over) -> Problem:
+    if name.startswith("mixed"):
+        kw = dict(n=int(name[5:] or 32))
+        kw.update(over)
+        return mixed_config(**kw)
     kw = dict(WORKLOADS[name])
     kw.update(over)
     return cube_config(**kw)

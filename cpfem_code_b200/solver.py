@@ -198,9 +198,10 @@ class GpuSolver(_SolverBase):
         if upload:
             self.upload()
 
-    def profile(self, enable: bool) -> dict:
-        """Start (True) or stop (False) device-side phase timing; returns the
-        counters gathered since the last start."""
+    def profile(self, level: int) -> dict:
+        """Start device-side profiling (1: counters and region time, 2: also
+        per-launch phase times) or stop it (0); returns the counters gathered
+        since the last start."""
         out = abi.FasProfile()
-        self._call("profile", 1 if enable else 0, C.byref(out))
+        self._call("profile", int(level), C.byref(out))
         return out.as_dict()

@@ -250,8 +250,11 @@ typedef struct fas_profile {
     double  assembly_bytes;    /* algorithmic bytes of the assembly kernel  */
 } fas_profile;
 
-/* enable != 0 starts (and zeroes) profiling, 0 stops it.  When `out` is
- * non-null the counters so far are written to it first. */
+/* enable = 1 starts (and zeroes) profiling with counters and one event
+ * pair around the whole region (ms_total); enable = 2 also brackets every
+ * phase kernel launch with an event pair (the per-phase ms_*, at some
+ * launch-rate cost); 0 stops.  When `out` is non-null the counters so far
+ * are written to it first. */
 FAS_API int32_t fas_gpu_profile(fas_handle *h, int32_t enable, fas_profile *out);
 
 #ifdef __cplusplus

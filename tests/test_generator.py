@@ -107,3 +107,37 @@ def test_grains_and_materials():
         assert np.unique(p.sv[sel, :3], axis=0).shape[0] == 1
     assert set(np.unique(p.le)) <= {1, 2}
     assert (p.sv[:, 3:15] == 25.0).all()
+
+
+def test_hcp_systems_geometry():
+    ab, an, lab = generator.hcp_systems(1.593)
+    counts = {k: lab.count(k) for k in set(lab)}
+    assert counts == {"basal": 3, "prism": 3, "pyr1ca": 12, "pyr2ca": 6, "twin": 6}
+    np.testing.assert_allclose(np.linalg.norm(ab, axis=1), 1.0, rtol=1e-14)
+    np.testing.assert_allclose(np.linalg.norm(an, axis=1), 1.0, rtol=1e-14)
+    np.testing.assert_allclose((ab * an).sum(axis=1), 0.0, atol=1e-14)
+    c = np.array([0.0, 0.0, 1.0])
+    lab = np.array(lab)
+    # basal normals are c; prism normals and <a> directions lie in the basal plane
+    np.testing.assert_allclose(an[lab == "basal"] @ c, 1.0)
+    np.testing.assert_allclose(an[lab == "prism"] @ c, 0.0, atol=1e-15)
+    # <c+a>: angle to c is atan(1/(c/a)) * ... |b.c| = c/a / sqrt(1 + (c/a)^2)
+    ca = 1.593
+    np.testing.assert_allclose(np.abs(ab[lab == "pyr1ca"] @ c), ca / np.sqrt(1 + ca ** 2), rtol=1e-12)
+    # {10-12} plane normal: tan(angle to c) = 2 / (sqrt(3) c/a) ... cos = l/ca / |n|
+    n = np.array([1.0, 1 / np.sqrt(3), 2 / ca])
+    np.testing.assert_allclose(an[lab == "twin"] @ c, n[2] / np.linalg.norm(n), rtol=1e-12)
+    # the six twin variants are related by 60 degree rotations about c
+    ang = np.sort(np.degrees(np.arctan2(an[lab == "twin"][:, 1], an[lab == "twin"][:, 0])) % 360)
+    np.testing.assert_allclose(np.diff(ang), 60.0, atol=1e-9)
+
+
+def test_hcp_material_and_mixed_workload():
+    z = generator.hcp_zirconium()
+    assert z["ssang"][np.array(z["labels"]) == "twin"] == pytest.approx(85.2, abs=0.05)
+    p = generator.mixed_config(n=4, ninc=2)
+    assert set(np.unique(p.le)) == {1, 2}
+    hcp = p.le == 1
+    assert (p.sv[hcp, 3:33] == z["tau0"][None, :]).all()
+    assert (p.sv[~hcp, 3:15] == 25.0).all() and (p.sv[~hcp, 15:33] == 0).all()
+    assert p.nsv == 33 and p.twinprob == 1.0 and p.twinlim == 1
