@@ -29,6 +29,7 @@ FAS_MODE_PLAIN = 0
 FAS_MODE_SOR_FP32 = 1
 FAS_MODE_SOR_NATURAL = 2
 FAS_MODE_SOR_GRID = 4
+FAS_MODE_CP_WARP = 8
 
 #: FAFERR codes the hot path raises, with the reference's meaning.
 FAFERR_TEXT = {

@@ -354,11 +354,12 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
     int tot = 0;
     for (int c = 0; c < h->ncol; ++c) {
         h->sor_boff[c] = tot;
-        // warp per row, 8 rows per block; at most 4 blocks per SM, whose
-        // warps stride over the colour's rows, keeps the per-sweep partial
-        // sums few enough for a cheap deterministic check
+        // warp per row, 8 rows per block; one wave of resident blocks (3 per
+        // SM at the kernel's register count) whose warps stride over the
+        // colour's rows -- also keeps the per-sweep partial sums few enough
+        // for a cheap deterministic check
         h->sor_nblk[c] = (int)std::min<long long>(nblocks(h->col_start[c + 1] - h->col_start[c], 8),
-                                                   (long long)h->nsm * 4);
+                                                   (long long)h->nsm * 3);
         tot += h->sor_nblk[c];
     }
     h->sor_nblk_tot = std::max(tot, 1);
@@ -707,8 +708,12 @@ int download_impl(fas_handle *h, const fas_state_desc *S)
 template <int NS> int launch_elem(fas_handle *h, int inc, int nit)
 {
     Span sp(h, &h->P.ms_constitutive);
-    k_elem<NS><<<nblocks(h->nlmnt, 128), 128, 0, h->stream>>>(
-        h->mesh(), h->M, h->C, h->gp(), h->x.p, h->dx.p, h->rec.p, h->h_tiem[inc - 1], inc, nit, h->ekey.p);
+    if (!(h->mode & FAS_MODE_CP_WARP))
+        k_elem<NS><<<nblocks(h->nlmnt, 128), 128, 0, h->stream>>>(
+            h->mesh(), h->M, h->C, h->gp(), h->x.p, h->dx.p, h->rec.p, h->h_tiem[inc - 1], inc, nit, h->ekey.p);
+    else
+        k_elem_wc<(NS > 12 ? 32 : 12)><<<nblocks(32LL * h->nlmnt, 128), 128, 0, h->stream>>>(
+            h->mesh(), h->M, h->C, h->gp(), h->x.p, h->dx.p, h->rec.p, h->h_tiem[inc - 1], inc, nit, h->ekey.p);
     sp.end();
     keep(h, sp);
     LAUNCHED(h);
@@ -740,7 +745,12 @@ int elvals_impl(fas_handle *h, int inc, int nit, bool bc)
     switch (h->ns_tmpl) {
     case 12: rc = launch_elem<12>(h, inc, nit); break;
     case 32: rc = launch_elem<32>(h, inc, nit); break;
-    default: rc = launch_elem<60>(h, inc, nit); break;
+    default: {   // more than 32 systems: one thread per GP only
+        const uint32_t m = h->mode;
+        h->mode &= ~FAS_MODE_CP_WARP;
+        rc = launch_elem<60>(h, inc, nit);
+        h->mode = m;
+    } break;
     }
     if (rc) return rc;
     {
@@ -1155,9 +1165,17 @@ int32_t fas_gpu_constitutive(fas_handle *h, int32_t inc, int32_t nit)
     Span sp(h, &h->P.ms_constitutive);
     const double dt = h->h_tiem[inc - 1];
     const unsigned nb = nblocks(h->ngps, 128);
+    const unsigned nbw = nblocks(32LL * h->ngps, 128);
+    const bool thr = !(h->mode & FAS_MODE_CP_WARP) || h->maxns > 32;
     switch (h->ns_tmpl) {
-    case 12: k_points<12><<<nb, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p); break;
-    case 32: k_points<32><<<nb, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p); break;
+    case 12:
+        if (thr) k_points<12><<<nb, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p);
+        else k_points_wc<12><<<nbw, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p);
+        break;
+    case 32:
+        if (thr) k_points<32><<<nb, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p);
+        else k_points_wc<32><<<nbw, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p);
+        break;
     default: k_points<60><<<nb, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p); break;
     }
     sp.end();

@@ -15,6 +15,7 @@
 #pragma once
 
 #include "fas_device.cuh"
+#include "fas_device_warp.cuh"
 
 namespace fasdev {
 
@@ -155,6 +156,135 @@ __global__ void __launch_bounds__(128) k_points(DevMat M, DevCtrl C, DevGp G, co
     for (int i = 0; i < 6; ++i)
 #pragma unroll
         for (int j = 0; j < 6; ++j) chi[(i + 6 * j) * (size_t)ng + g] = o.chi[i][j];
+}
+
+// ---------------------------------------------------------------- warp-cooperative pass
+// ELVALS per element with one warp per element: every lane forms the
+// element kinematics (identical values), the warp runs dstrss_wc with lane i
+// owning slip system i, and the lanes share out the stores.
+template <int NA>
+__global__ void __launch_bounds__(128) k_elem_wc(MeshDev Mh, DevMat M, DevCtrl C, DevGp G,
+                                                 const double *__restrict__ x,
+                                                 const double *__restrict__ dx, double *rec,
+                                                 double dt, int inc, int nit,
+                                                 unsigned long long *errkey)
+{
+    const int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (e >= Mh.nlmnt) return;           // whole warps only
+    const int ne = Mh.nlmnt;
+    double del[6], r[3], defl;
+    double *R = rec + (size_t)e * REC;
+    {
+        double xl[8][3], dxl[8][3];
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            const int n = Mh.ln[a * ne + e];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                xl[a][c] = x[3 * n + c];
+                dxl[a][c] = dx[3 * n + c];
+            }
+        }
+        double sfd[8][3];
+        const double w = shape12(xl, sfd);
+        if (w < 1.e-7) {
+            if (lane == 0) atomicMin(errkey, ((unsigned long long)e << 16) | 920ull);
+            return;
+        }
+        const int rc = dstrns(sfd, dxl, C.smalr, C.smale, del, r, defl);
+        if (rc) {
+            if (lane == 0) atomicMin(errkey, ((unsigned long long)e << 16) | (unsigned long long)rc);
+            return;
+        }
+        // record: lanes 0-23 shape derivatives, lane 30 the weight
+        double v = 0.0;
+#pragma unroll
+        for (int a = 0; a < 8; ++a)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                if (lane == 3 * a + c) v = sfd[a][c];
+        if (lane == REC_W) v = w;
+        if (lane < 24 || lane == REC_W) R[lane] = v;
+    }
+    const int g = Mh.gpe[e];
+    const int ng = G.ngps;
+    double st[6], ds[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        st[k] = G.st[k * ng + g];
+        ds[k] = G.ds[k * ng + g];
+    }
+    wc::GpOutW o;
+    const int rc = wc::dstrss_wc<NA>(M, C, G, g, Mh.le[e], del, r, st, ds, dt, inc, nit, o);
+    if (rc) {
+        if (lane == 0) atomicMin(errkey, ((unsigned long long)e << 16) | (unsigned long long)rc);
+        return;
+    }
+    if (lane == 0) G.dep[g] = o.deff;
+    if (lane < 6) {
+        double dk = 0.0, sk = 0.0, tk = 0.0;
+#pragma unroll
+        for (int k = 0; k < 6; ++k)
+            if (k == lane) {
+                dk = del[k];
+                sk = ds[k];
+                tk = o.t[k];
+            }
+        G.de[lane * ng + g] = dk;
+        G.ds[lane * ng + g] = sk;
+        R[REC_S + lane] = tk;
+        // tangent upper triangle, row `lane`
+#pragma unroll
+        for (int j = 0; j < 6; ++j)
+            if (j >= lane) R[REC_D + utri(lane, j)] = o.chirow[j];
+    }
+    if (lane < 3) {
+        double rk = 0.0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            if (k == lane) rk = r[k];
+        G.dr[lane * ng + g] = rk;
+    }
+}
+
+// Independent points with one warp per point (the micro-benchmark path).
+template <int NA>
+__global__ void __launch_bounds__(128) k_points_wc(DevMat M, DevCtrl C, DevGp G, const int *gp_iel,
+                                                   double *chi, double dt, int inc, int nit,
+                                                   unsigned long long *errkey)
+{
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (g >= G.ngps) return;
+    const int ng = G.ngps;
+    double de[6], r[3], st[6], ds[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        de[k] = G.de[k * ng + g];
+        st[k] = G.st[k * ng + g];
+        ds[k] = G.ds[k * ng + g];
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) r[k] = G.dr[k * ng + g];
+    wc::GpOutW o;
+    const int rc = wc::dstrss_wc<NA>(M, C, G, g, gp_iel[g], de, r, st, ds, dt, inc, nit, o);
+    if (rc) {
+        if (lane == 0) atomicMin(errkey, ((unsigned long long)g << 16) | (unsigned long long)rc);
+        return;
+    }
+    if (lane == 0) G.dep[g] = o.deff;
+    if (lane < 6) {
+        double sk = 0.0;
+#pragma unroll
+        for (int k = 0; k < 6; ++k)
+            if (k == lane) sk = ds[k];
+        G.ds[lane * ng + g] = sk;
+    }
+    if (lane < 6) {   // row `lane` of the tangent, column-major 6x6 per point
+#pragma unroll
+        for (int j = 0; j < 6; ++j) chi[(size_t)(lane + 6 * j) * ng + g] = o.chirow[j];
+    }
 }
 
 // gaussm (src/fasolt/Elvals.f90:132-220) for node pair (i, j) of one
@@ -446,51 +576,78 @@ struct SorCtl {
     double pad;
 };
 
-// The point-SOR update of one row (FACSLS's inner loop, Stif_sol.f90:189-197,
-// for the three DOFs of one node) by one warp: lane s (1 <= s < nslot)
-// multiplies the off-diagonal block of slot s (stored as T) by the current
-// solution at its column node, the warp sums the products, and lane 0
-// updates x, y, z in turn with the diagonal block.  Returns in lane 0 the
-// squared change and the squared new values; `base` (may be null) is added
-// to the iterate for the latter (the refinement form).
+// Operands of one row for one lane: the lane's 3x3 block (slot = lane), the
+// solution at the slot's column node, and (lane 0) the right-hand side.
+// Slot 0 is the row's own node, so lane 0 holds the diagonal block and the
+// node's current values.
+struct RowOps {
+    int ns, n;
+    double b[9];
+    double x0, x1, x2;
+    double r0, r1, r2;
+};
+
+// The matrix is streamed once per sweep and is larger than L2: its loads
+// are marked evict-first (ld.global.cs) so the solution vector, re-read by
+// every colour phase, stays resident in L2.
+__device__ __forceinline__ double ld_stream(const double *p) { return __ldcs(p); }
+__device__ __forceinline__ double ld_stream(const float *p) { return (double)__ldcs(p); }
+
 template <typename T>
-__device__ __forceinline__ void sor_row(const BlockDev &B, const T *__restrict__ blk, int p, int lane,
-                                        const double *__restrict__ rhs, double *sol,
-                                        const double *__restrict__ base, double &dv, double &vv)
+__device__ __forceinline__ void load_row(const BlockDev &B, const T *__restrict__ blk, int p, int lane,
+                                         const double *__restrict__ rhs, const double *sol, RowOps &o)
 {
-    const int ns = B.nslot[p];
+    o.ns = B.nslot[p];
+    const bool on = lane < o.ns;
+    const int m = on ? __ldcs(B.bcol + sidx(p, lane)) : 0;
+    o.n = __shfl_sync(0xffffffffu, m, 0);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) o.b[q] = on ? ld_stream(blk + bidx(p, lane, q)) : 0.0;
+    o.x0 = on ? sol[3 * m] : 0.0;
+    o.x1 = on ? sol[3 * m + 1] : 0.0;
+    o.x2 = on ? sol[3 * m + 2] : 0.0;
+    if (lane == 0) {
+        o.r0 = rhs[3 * m];
+        o.r1 = rhs[3 * m + 1];
+        o.r2 = rhs[3 * m + 2];
+    }
+}
+
+// The point-SOR update of one row (FACSLS's inner loop, Stif_sol.f90:189-197,
+// for the three DOFs of one node) by one warp: lanes 1..nslot-1 multiply
+// their off-diagonal block by the solution at the column node, the warp sums
+// the products, and lane 0 updates x, y, z in turn with the diagonal block.
+// Adds to dv / vv (lane 0) the squared change and the squared new values;
+// `base` (may be null) is added to the iterate for the latter.
+__device__ __forceinline__ void sor_update(const RowOps &o, int lane, double *sol,
+                                           const double *__restrict__ base, double &dv, double &vv)
+{
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    if (lane >= 1 && lane < ns) {
-        const int m = B.bcol[sidx(p, lane)];
-        const T *b = blk + bidx(p, lane, 0);
-        const double x0 = sol[3 * m], x1 = sol[3 * m + 1], x2 = sol[3 * m + 2];
-        a0 = (double)b[0 * 27] * x0 + (double)b[1 * 27] * x1 + (double)b[2 * 27] * x2;
-        a1 = (double)b[3 * 27] * x0 + (double)b[4 * 27] * x1 + (double)b[5 * 27] * x2;
-        a2 = (double)b[6 * 27] * x0 + (double)b[7 * 27] * x1 + (double)b[8 * 27] * x2;
+    if (lane >= 1) {
+        a0 = o.b[0] * o.x0 + o.b[1] * o.x1 + o.b[2] * o.x2;
+        a1 = o.b[3] * o.x0 + o.b[4] * o.x1 + o.b[5] * o.x2;
+        a2 = o.b[6] * o.x0 + o.b[7] * o.x1 + o.b[8] * o.x2;
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+    for (int k = 16; k > 0; k >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, k);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, k);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, k);
     }
     if (lane == 0) {
-        const int n = B.perm[p];
-        double D[9];
-#pragma unroll
-        for (int q = 0; q < 9; ++q) D[q] = (double)blk[bidx(p, 0, q)];
-        const double o0 = sol[3 * n], o1 = sol[3 * n + 1], o2 = sol[3 * n + 2];
-        double x0 = o0, x1 = o1, x2 = o2;
-        double t = (rhs[3 * n] - (a0 + D[1] * x1 + D[2] * x2)) / D[0];
+        const double *D = o.b;
+        const int n = o.n;
+        double x0 = o.x0, x1 = o.x1, x2 = o.x2;
+        double t = (o.r0 - (a0 + D[1] * x1 + D[2] * x2)) / D[0];
         x0 = x0 + 1.2 * (t - x0);
-        t = (rhs[3 * n + 1] - (a1 + D[3] * x0 + D[5] * x2)) / D[4];
+        t = (o.r1 - (a1 + D[3] * x0 + D[5] * x2)) / D[4];
         x1 = x1 + 1.2 * (t - x1);
-        t = (rhs[3 * n + 2] - (a2 + D[6] * x0 + D[7] * x1)) / D[8];
+        t = (o.r2 - (a2 + D[6] * x0 + D[7] * x1)) / D[8];
         x2 = x2 + 1.2 * (t - x2);
         sol[3 * n] = x0;
         sol[3 * n + 1] = x1;
         sol[3 * n + 2] = x2;
-        dv += (x0 - o0) * (x0 - o0) + (x1 - o1) * (x1 - o1) + (x2 - o2) * (x2 - o2);
+        dv += (x0 - o.x0) * (x0 - o.x0) + (x1 - o.x1) * (x1 - o.x1) + (x2 - o.x2) * (x2 - o.x2);
         if (base) {
             x0 += base[3 * n];
             x1 += base[3 * n + 1];
@@ -500,13 +657,37 @@ __device__ __forceinline__ void sor_row(const BlockDev &B, const T *__restrict__
     }
 }
 
+// Rows p, p + stride, ... < p1 of one colour by one warp, with the next
+// row's operands loaded while the current row is reduced and updated.
+// Within a colour no row reads a value another row of the colour writes
+// (same-colour nodes share no element), so the early loads see final values.
+template <typename T>
+__device__ __forceinline__ void sor_rows(const BlockDev &B, const T *__restrict__ blk, int p, int p1,
+                                         int stride, int lane, const double *__restrict__ rhs,
+                                         double *sol, const double *__restrict__ base, double &dv,
+                                         double &vv)
+{
+    if (p >= p1) return;
+    RowOps cur, nxt;
+    load_row<T>(B, blk, p, lane, rhs, sol, cur);
+    while (true) {
+        const int pn = p + stride;
+        const bool more = pn < p1;
+        if (more) load_row<T>(B, blk, pn, lane, rhs, sol, nxt);
+        sor_update(cur, lane, sol, base, dv, vv);
+        if (!more) break;
+        cur = nxt;
+        p = pn;
+    }
+}
+
 // One warp per row: lane s (1 <= s < nslot) multiplies the off-diagonal
 // block of slot s by the current solution at its column node; the warp sums
 // the three products; lane 0 then updates x, y, z in turn with the diagonal
 // block.  The row's blocks are 1944 contiguous bytes, so each row is read
 // with full sectors.  Warps stride over the colour's rows; each block adds
 // its share of sum(dx^2) and sum(x^2) to part[] once.
-__global__ void __launch_bounds__(256) k_sor_colour(BlockDev B, int p0, int p1,
+__global__ void __launch_bounds__(256, 3) k_sor_colour(BlockDev B, int p0, int p1,
                                                     const double *__restrict__ rhs, double *sol,
                                                     const SorCtl *ctl, double *part, int boff,
                                                     int nblk_tot)
@@ -515,8 +696,8 @@ __global__ void __launch_bounds__(256) k_sor_colour(BlockDev B, int p0, int p1,
     const int lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
     double v[2] = {0.0, 0.0};
-    for (int p = p0 + blockIdx.x * wpb + (threadIdx.x >> 5); p < p1; p += gridDim.x * wpb)
-        sor_row<double>(B, B.blk, p, lane, rhs, sol, nullptr, v[0], v[1]);
+    sor_rows<double>(B, B.blk, p0 + blockIdx.x * wpb + (threadIdx.x >> 5), p1, gridDim.x * wpb, lane,
+                     rhs, sol, nullptr, v[0], v[1]);
     block_sum_store<2>(v, part + boff, nblk_tot);
 }
 
@@ -540,8 +721,7 @@ __global__ void __launch_bounds__(1024) k_sor_small(BlockDev B, const int *__res
         double v0 = 0.0, v1 = 0.0;
         for (int c = 0; c < ncol; ++c) {
             const int p1 = cstart[c + 1];
-            for (int p = cstart[c] + wid; p < p1; p += nw)
-                sor_row<double>(B, B.blk, p, lane, rhs, sol, nullptr, v0, v1);
+            sor_rows<double>(B, B.blk, cstart[c] + wid, p1, nw, lane, rhs, sol, nullptr, v0, v1);
             __syncthreads();   // the next colour reads this colour's values
         }
         if (lane == 0) {
@@ -573,7 +753,7 @@ __global__ void __launch_bounds__(1024) k_sor_small(BlockDev B, const int *__res
 // the FP32 copy of the matrix (half the bytes of a sweep), FP64 vectors and
 // arithmetic.  xs is the iterate at the last residual; the stopping measure
 // is the reference's, on the iterate xs + d: sum(change^2) / sum((xs+d)^2).
-__global__ void __launch_bounds__(256) k_sor_colour32(BlockDev B, int p0, int p1,
+__global__ void __launch_bounds__(256, 3) k_sor_colour32(BlockDev B, int p0, int p1,
                                                       const double *__restrict__ res,
                                                       const double *__restrict__ xs, double *d,
                                                       const SorCtl *ctl, double *part, int boff,
@@ -583,8 +763,8 @@ __global__ void __launch_bounds__(256) k_sor_colour32(BlockDev B, int p0, int p1
     const int lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
     double v[2] = {0.0, 0.0};
-    for (int p = p0 + blockIdx.x * wpb + (threadIdx.x >> 5); p < p1; p += gridDim.x * wpb)
-        sor_row<float>(B, B.blk32, p, lane, res, d, xs, v[0], v[1]);
+    sor_rows<float>(B, B.blk32, p0 + blockIdx.x * wpb + (threadIdx.x >> 5), p1, gridDim.x * wpb, lane,
+                    res, d, xs, v[0], v[1]);
     block_sum_store<2>(v, part + boff, nblk_tot);
 }
 

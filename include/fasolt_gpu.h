@@ -57,6 +57,9 @@ extern "C" {
 #define FAS_MODE_SOR_FP32     1u  /* SOR sweeps on an FP32 copy of the
                                      matrix with FP64 residual refinement   */
 #define FAS_MODE_SOR_NATURAL  2u  /* (oracle only) natural-order SOR        */
+#define FAS_MODE_CP_WARP      8u  /* Gauss-point update with one warp per GP
+                                     (lanes = slip systems) instead of one
+                                     thread per GP; at most 32 systems      */
 #define FAS_MODE_SOR_GRID     4u  /* always use the grid-wide SOR launches,
                                      also for meshes small enough for the
                                      one-CTA solve                          */

@@ -27,9 +27,11 @@ def pair(p, threads=4, mode=abi.FAS_MODE_PLAIN):
     return GpuSolver(pg, mode=mode), OracleSolver(po, 8, threads=threads), pg, po
 
 
-def test_constitutive_points():
+@pytest.mark.parametrize("mode", [abi.FAS_MODE_PLAIN, abi.FAS_MODE_CP_WARP])
+def test_constitutive_points(mode):
+    """One thread per point (default) and one warp per point."""
     p = generator.point_batch(2048, seed=11)
-    g, o, pg, po = pair(p)
+    g, o, pg, po = pair(p, mode=mode)
     g.constitutive(1, 1)
     o.constitutive(1, 1)
     g.download()
@@ -119,7 +121,8 @@ def test_elvals_suvals_facsls():
                                          ((3, 3, 3), 2, abi.FAS_MODE_PLAIN),
                                          ((8, 8, 8), 1, abi.FAS_MODE_PLAIN),
                                          ((3, 3, 3), 1, abi.FAS_MODE_SOR_GRID),
-                                         ((8, 8, 8), 1, abi.FAS_MODE_SOR_GRID)])
+                                         ((8, 8, 8), 1, abi.FAS_MODE_SOR_GRID),
+                                         ((4, 4, 4), 2, abi.FAS_MODE_CP_WARP)])
 def test_increments_match(n, ninc, mode):
     """Both SOR launch shapes (one CTA, and grid-wide colour launches) give
     the checker's iterates."""
@@ -221,12 +224,13 @@ def test_fp32_sor_refinement_error():
     assert per_point < 1e-4 and macro < 1e-5
 
 
-def test_mixed_fcc_hcp_increment():
+@pytest.mark.parametrize("mode", [abi.FAS_MODE_PLAIN, abi.FAS_MODE_CP_WARP])
+def test_mixed_fcc_hcp_increment(mode):
     """Mixed FCC (12 systems) / HCP (30 systems, with twins) grains: the
-    32-system kernel instantiation against the checker, including twin
+    32-system kernel instantiations against the checker, including twin
     triggers and reorientation."""
     p = generator.mixed_config(n=6, ninc=2)
-    g, o, pg, po = pair(p, threads=8)
+    g, o, pg, po = pair(p, threads=8, mode=mode)
     for inc in (1, 2):
         rg, evg = g.increment(inc)
         ro, evo = o.increment(inc)
