@@ -21,6 +21,7 @@ FAS_E_ELTYPE = -4
 FAS_E_NOMEM = -5
 FAS_E_RANGE = -6
 FAS_E_STATE = -7
+FAS_E_TIMEOUT = -8
 FAS_MAXSS = 60
 SVLD = 63          # maxsvs, src/fasolt/fas-com-mod.f90:14
 XSLD = 99          # second dimension of x_spec / f_spec (fas-com-mod.f90:30-31)
@@ -50,6 +51,7 @@ ABI_TEXT = {
     FAS_E_NOMEM: "device allocation failed",
     FAS_E_RANGE: "size beyond a documented maximum",
     FAS_E_STATE: "call out of order (state not uploaded)",
+    FAS_E_TIMEOUT: "a bounded device-side wait gave up (copy engine stalled)",
 }
 
 _p = C.c_void_p
@@ -174,6 +176,7 @@ def declare(lib: C.CDLL, prefix: str) -> None:
         "get_tangent": (i32, [H, _p, i32]),
         "get_cp_stats": (i32, [H, _i32p, C.POINTER(C.c_double)]),
         "get_cp_ops": (i32, [H, C.POINTER(C.c_double)]),
+        "lattice_strain": (i32, [H, _p, i32]) if prefix == "fas_gpu" else (i32, [H, _p]),
     }
     if prefix == "fas_gpu":
         sig["profile"] = (i32, [H, i32, C.POINTER(FasProfile)])

@@ -104,6 +104,7 @@ struct fas_handle {
     DVec<float> blk32;           // FP32 copy for FAS_MODE_SOR_FP32
     DVec<double> sor_d, sor_r;   // correction and residual of the refinement
     int refine_every = 16;       // FP32 sweeps per FP64 residual
+    cudaGraphExec_t sor_graph = nullptr;   // GRAPH_SWEEPS plain sweeps
     bool blk32_fresh = false;    // the last assembly wrote blk32
     // reductions and control
     std::vector<int> sor_boff, sor_nblk;
@@ -130,6 +131,7 @@ struct fas_handle {
 
     ~fas_handle()
     {
+        if (sor_graph) cudaGraphExecDestroy(sor_graph);
         for (auto e : ev_pool) cudaEventDestroy(e);
         if (ev_t0) cudaEventDestroy(ev_t0);
         if (ev_t1) cudaEventDestroy(ev_t1);
@@ -287,8 +289,8 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
     for (int p = 0; p < nn; ++p) h->col_start[h->h_colour[perm[p]] + 1] = p + 1;
     for (int c = 1; c <= h->ncol; ++c) h->col_start[c] = std::max(h->col_start[c], h->col_start[c - 1]);
 
-    std::vector<int> nslot(nn), bcol((size_t)SLOTS * nn, 0);
-    std::vector<unsigned> bloc((size_t)SLOTS * nn, 0xFFFFFFFFu);
+    std::vector<int> nslot(nn), bcol((size_t)CROW * nn, 0);
+    std::vector<unsigned> bloc((size_t)CROW * nn, 0xFFFFFFFFu);
     for (int p = 0; p < nn; ++p) {
         const int n = perm[p];
         int nb[SLOTS];
@@ -306,6 +308,7 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
         if ((int)others.size() + 1 > SLOTS) return FAS_E_RANGE;
         for (int m : others) nb[cnt++] = m;
         nslot[p] = cnt;
+        bcol[sidx(p, CROW - 1)] = cnt;   // the pad slot carries the slot count
         for (int s = 0; s < cnt; ++s) {
             bcol[sidx(p, s)] = nb[s];
             unsigned word = 0xFFFFFFFFu;
@@ -339,9 +342,9 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
     CKA(h->perm.alloc(nn));
     CKA(h->rowof.alloc(nn));
     CKA(h->nslot.alloc(nn));
-    CKA(h->bcol.alloc((size_t)SLOTS * nn));
-    CKA(h->bloc.alloc((size_t)SLOTS * nn));
-    CKA(h->blk.alloc((size_t)SLOTS * 9 * nn));
+    CKA(h->bcol.alloc((size_t)CROW * nn));
+    CKA(h->bloc.alloc((size_t)CROW * nn));
+    CKA(h->blk.alloc((size_t)BROW * nn));
     CK(h->perm.put(perm.data(), nn, s));
     CK(h->rowof.put(rowof.data(), nn, s));
     CK(h->nslot.put(nslot.data(), nn, s));
@@ -354,12 +357,11 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
     int tot = 0;
     for (int c = 0; c < h->ncol; ++c) {
         h->sor_boff[c] = tot;
-        // warp per row, 8 rows per block; one wave of resident blocks (3 per
-        // SM at the kernel's register count) whose warps stride over the
-        // colour's rows -- also keeps the per-sweep partial sums few enough
-        // for a cheap deterministic check
-        h->sor_nblk[c] = (int)std::min<long long>(nblocks(h->col_start[c + 1] - h->col_start[c], 8),
-                                                   (long long)h->nsm * 3);
+        // chunks of TMA_ROWS rows; at most 4 CTAs per SM (their shared-memory
+        // rings fit together), which also keeps the per-sweep partial sums
+        // few enough for a cheap deterministic check
+        h->sor_nblk[c] = (int)std::min<long long>(nblocks(h->col_start[c + 1] - h->col_start[c], TMA_ROWS),
+                                                   (long long)h->nsm * 4);
         tot += h->sor_nblk[c];
     }
     h->sor_nblk_tot = std::max(tot, 1);
@@ -381,6 +383,10 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
     if (prop.major != 10) return FAS_E_NODEVICE;
     h->nsm = prop.multiProcessorCount;
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CK(cudaFuncSetAttribute(k_sor_colour_tma<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            tma_smem_bytes<double>()));
+    CK(cudaFuncSetAttribute(k_sor_colour_tma<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            tma_smem_bytes<float>()));
     CK(cudaMallocHost((void **)&h->hc, sizeof(HostCtl)));
     CK(cudaEventCreate(&h->ev_t0));
     CK(cudaEventCreate(&h->ev_t1));
@@ -728,7 +734,7 @@ int ensure_fp32(fas_handle *h)
 {
     if (!(h->mode & FAS_MODE_SOR_FP32) || h->blk32.p || h->point_mode) return 0;
     const size_t nd3 = 3 * (size_t)h->nnod;
-    CKA(h->blk32.alloc((size_t)SLOTS * 9 * h->nnod));
+    CKA(h->blk32.alloc((size_t)BROW * h->nnod));
     CKA(h->sor_d.alloc(nd3));
     CKA(h->sor_r.alloc(nd3));
     CK(h->blk32.zero(h->stream));
@@ -791,6 +797,50 @@ int suvals_impl(fas_handle *h, int inc)
     return h->hc->flags[0] ? FAS_E_ARG : 0;
 }
 
+// GRAPH_SWEEPS plain sweeps (ncol colour launches + the check, each)
+// captured once into a CUDA graph: one graph launch replaces
+// GRAPH_SWEEPS * (ncol + 1) kernel launches.
+constexpr int GRAPH_SWEEPS = 4;
+
+// One colour phase: FP64 blocks on (rhs, sol), or the FP32 copy on the
+// refinement's (residual, correction) with the iterate as base.
+void launch_colour(fas_handle *h, int c, bool fp32)
+{
+    const int p0 = h->col_start[c], p1 = h->col_start[c + 1];
+    if (p1 <= p0) return;
+    if (fp32)
+        k_sor_colour_tma<float><<<h->sor_nblk[c], 32 * TMA_ROWS, tma_smem_bytes<float>(), h->stream>>>(
+            h->blk32.p, h->bcol.p, p0, p1, h->sor_r.p, h->sor_d.p, h->ddx.p, h->sorctl.p, h->part_sor.p,
+            h->sor_boff[c], h->sor_nblk_tot);
+    else
+        k_sor_colour_tma<double><<<h->sor_nblk[c], 32 * TMA_ROWS, tma_smem_bytes<double>(), h->stream>>>(
+            h->blk.p, h->bcol.p, p0, p1, h->rhs.p, h->ddx.p, nullptr, h->sorctl.p, h->part_sor.p,
+            h->sor_boff[c], h->sor_nblk_tot);
+}
+
+void launch_plain_sweep(fas_handle *h, const BlockDev &B, double tolerl)
+{
+    (void)B;
+    for (int c = 0; c < h->ncol; ++c) launch_colour(h, c, false);
+    k_sor_check<<<1, 1024, 0, h->stream>>>(h->part_sor.p, h->sor_nblk_tot, h->sorctl.p, tolerl);
+}
+
+int ensure_sor_graph(fas_handle *h, const BlockDev &B, double tolerl)
+{
+    if (h->sor_graph) return 0;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    for (int it = 0; it < GRAPH_SWEEPS; ++it) launch_plain_sweep(h, B, tolerl);
+    CK(cudaStreamEndCapture(h->stream, &g));
+    const cudaError_t e = cudaGraphInstantiate(&h->sor_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        h->sor_graph = nullptr;
+        return FAS_E_CUDA;
+    }
+    return 0;
+}
+
 // FACSLS: rhs <- ddx, ddx <- 0, multicolour SOR sweeps until the relative
 // change drops below toler^2 or 1000 sweeps (Stif_sol.f90:173-213).
 int facsls_impl(fas_handle *h, int *sweeps, double *error)
@@ -832,12 +882,9 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
                 const int k = std::min(m, 1000 - done);
                 for (int it = 0; it < k; ++it) {
                     for (int c = 0; c < h->ncol; ++c) {
-                        const int p0 = h->col_start[c], p1 = h->col_start[c + 1];
-                        if (p1 <= p0) continue;
+                        if (h->col_start[c + 1] <= h->col_start[c]) continue;
                         Span sp(h, &h->P.ms_sor_colour);
-                        k_sor_colour32<<<h->sor_nblk[c], 256, 0, s>>>(B, p0, p1, h->sor_r.p, h->ddx.p, h->sor_d.p,
-                                                                     h->sorctl.p, h->part_sor.p, h->sor_boff[c],
-                                                                     h->sor_nblk_tot);
+                        launch_colour(h, c, true);
                         sp.end();
                         keep(h, sp);
                         LAUNCHED(h);
@@ -858,15 +905,17 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
         }
         done = 1000;
     }
+    const bool graph = h->prof < 2 && done < 1000 && ensure_sor_graph(h, B, tolerl) == 0;
     while (done < 1000) {
         const int k = std::min(chunk, 1000 - done);
-        for (int it = 0; it < k; ++it) {
+        if (graph && k % GRAPH_SWEEPS == 0) {
+            for (int it = 0; it < k; it += GRAPH_SWEEPS) CK(cudaGraphLaunch(h->sor_graph, s));
+            h->launches += (int64_t)k * (h->ncol + 1);
+        } else for (int it = 0; it < k; ++it) {
             for (int c = 0; c < h->ncol; ++c) {
-                const int p0 = h->col_start[c], p1 = h->col_start[c + 1];
-                if (p1 <= p0) continue;
+                if (h->col_start[c + 1] <= h->col_start[c]) continue;
                 Span sp(h, &h->P.ms_sor_colour);
-                k_sor_colour<<<h->sor_nblk[c], 256, 0, s>>>(B, p0, p1, h->rhs.p, h->ddx.p, h->sorctl.p,
-                                                           h->part_sor.p, h->sor_boff[c], h->sor_nblk_tot);
+                launch_colour(h, c, false);
                 sp.end();
                 keep(h, sp);
                 LAUNCHED(h);
@@ -893,6 +942,7 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
     h->P.sor_bytes += bytes * nsw;
     if (sweeps) *sweeps = nsw;
     if (error) *error = h->hc->sor.err;
+    if (h->hc->sor.fault) return FAS_E_TIMEOUT;
     if (h->hc->sor.err > 10.0 * tolerl) return 904;
     return 0;
 }
@@ -1227,6 +1277,17 @@ int32_t fas_gpu_get_cp_stats(fas_handle *h, int32_t *iters, double *erepmd)
     if (iters) CK(cudaMemcpy(iters, h->cp_iters.p, h->ngps * sizeof(int), cudaMemcpyDeviceToHost));
     if (erepmd) CK(cudaMemcpy(erepmd, h->erepmd.p, h->ngps * sizeof(double), cudaMemcpyDeviceToHost));
     return 0;
+}
+
+int32_t fas_gpu_lattice_strain(fas_handle *h, void *strain, int32_t real_bytes)
+{
+    if (!h || !strain || (real_bytes != 4 && real_bytes != 8)) return FAS_E_ARG;
+    if (!h->have_state) return FAS_E_STATE;
+    DVec<double> d;
+    CKA(d.alloc(6 * (size_t)h->ngps));
+    k_elaseps<<<nblocks(h->ngps, 128), 128, 0, h->stream>>>(h->M, h->gp(), h->gp_iel.p, d.p);
+    LAUNCHED(h);
+    return down_field(h, strain, real_bytes, 6, 6, h->ngps, d.p);
 }
 
 int32_t fas_gpu_get_cp_ops(fas_handle *h, double *ops)

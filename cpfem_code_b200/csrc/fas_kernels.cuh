@@ -7,11 +7,11 @@
 //     upper triangle (21) -- written once per Newton iteration by the element
 //     kernel and read by the row-gather assembly;
 //   * stiffness: block-ELL of 3x3 node blocks, rows permuted so each SOR
-//     colour is a contiguous row range.  The 27 blocks of a row are 1944
-//     contiguous bytes, component-major: blk[(row*9 + r*3 + c)*27 + slot],
-//     so one component of all slots of a row is 216 contiguous bytes (one
-//     coalesced warp load).  Slot 0 = the diagonal block,
-//     bcol[row*27 + slot] = column node.
+//     colour is a contiguous row range.  A row is BROW = 244 values (the 27
+//     blocks, component-major, plus one pad value): blk[row*244 + (r*3+c)*27
+//     + slot], so one component of all slots is 216 contiguous bytes and a
+//     row is 1952 bytes, a multiple of 16 as bulk copies need.  Slot 0 = the
+//     diagonal block; bcol[row*28 + slot] = column node (28 ints per row).
 #pragma once
 
 #include "fas_device.cuh"
@@ -24,9 +24,11 @@ constexpr int REC_S = 24, REC_W = 30, REC_D = 32;
 constexpr int SLOTS = 27;        // node blocks per row of an 8-node brick mesh
 constexpr int MAXADJ = 8;        // elements per node
 
-// block matrix addressing (row-major rows of SLOTS 3x3 blocks)
-__host__ __device__ __forceinline__ size_t sidx(int p, int s) { return (size_t)p * 27 + s; }
-__host__ __device__ __forceinline__ size_t bidx(int p, int s, int q) { return ((size_t)p * 9 + q) * 27 + s; }
+// block matrix addressing
+constexpr int BROW = 244;        // values per block row (27 x 9 + 1 pad)
+constexpr int CROW = 28;         // column ids per block row (27 + 1 pad)
+__host__ __device__ __forceinline__ size_t sidx(int p, int s) { return (size_t)p * CROW + s; }
+__host__ __device__ __forceinline__ size_t bidx(int p, int s, int q) { return (size_t)p * BROW + q * 27 + s; }
 
 // upper-triangle index of chi(i,j), i <= j (0-based)
 __host__ __device__ __forceinline__ int utri(int i, int j) { return i * 6 - (i * (i - 1)) / 2 + (j - i); }
@@ -573,7 +575,8 @@ struct SorCtl {
     int conv;       // set once error < toler^2
     int sweeps;     // sweeps actually performed
     double err;     // error of the last sweep
-    double pad;
+    int fault;      // a bounded wait gave up
+    int pad;
 };
 
 // Operands of one row for one lane: the lane's 3x3 block (slot = lane), the
@@ -681,28 +684,156 @@ __device__ __forceinline__ void sor_rows(const BlockDev &B, const T *__restrict_
     }
 }
 
-// One warp per row: lane s (1 <= s < nslot) multiplies the off-diagonal
-// block of slot s by the current solution at its column node; the warp sums
-// the three products; lane 0 then updates x, y, z in turn with the diagonal
-// block.  The row's blocks are 1944 contiguous bytes, so each row is read
-// with full sectors.  Warps stride over the colour's rows; each block adds
-// its share of sum(dx^2) and sum(x^2) to part[] once.
-__global__ void __launch_bounds__(256, 3) k_sor_colour(BlockDev B, int p0, int p1,
-                                                    const double *__restrict__ rhs, double *sol,
-                                                    const SorCtl *ctl, double *part, int boff,
-                                                    int nblk_tot)
+// ---------------------------------------------------------------- bulk-copy SOR
+// Shared-memory staging of block rows with the bulk-copy (TMA) engine:
+// cp.async.bulk global -> shared, completion counted on an mbarrier.
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up (returns false) after 2^22 polls instead of
+// spinning for ever.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity)
+{
+    for (int i = 0; i < (1 << 22); ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+constexpr int TMA_ROWS = 8;      // rows per chunk (= warps per CTA)
+constexpr int TMA_STAGES = 3;    // chunks in flight per CTA
+
+template <typename T> __host__ __device__ constexpr int tma_stage_bytes()
+{
+    return TMA_ROWS * BROW * (int)sizeof(T) + TMA_ROWS * CROW * 4;
+}
+template <typename T> __host__ __device__ constexpr int tma_smem_bytes()
+{
+    return TMA_STAGES * tma_stage_bytes<T>() + TMA_STAGES * 8;
+}
+
+// One colour phase of SOR with the colour's block rows streamed through a
+// TMA_STAGES-deep shared-memory ring.  CTA b takes chunks b, b + grid, ...
+// of TMA_ROWS consecutive rows; thread 0 issues the bulk copies (values and
+// column ids of the chunk) and re-arms a stage once all warps have read it;
+// warp w updates row w of the chunk from shared memory.  The solution
+// gathers stay ordinary (L2-resident) loads.  Every mbarrier wait is
+// bounded; on a timeout the CTA waits (bounded) for its own copies still in
+// flight, raises ctl->fault and leaves.
+template <typename T>
+__global__ void __launch_bounds__(256) k_sor_colour_tma(const T *__restrict__ blk, const int *__restrict__ bcol,
+                                                        int p0, int p1, const double *__restrict__ rhs,
+                                                        double *sol, const double *__restrict__ base,
+                                                        SorCtl *ctl, double *part, int boff, int nblk_tot)
 {
     if (((volatile const SorCtl *)ctl)->conv) return;
-    const int lane = threadIdx.x & 31;
-    const int wpb = blockDim.x >> 5;
-    double v[2] = {0.0, 0.0};
-    sor_rows<double>(B, B.blk, p0 + blockIdx.x * wpb + (threadIdx.x >> 5), p1, gridDim.x * wpb, lane,
-                     rhs, sol, nullptr, v[0], v[1]);
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr int VB = TMA_ROWS * BROW * (int)sizeof(T);
+    constexpr int SB = tma_stage_bytes<T>();
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TMA_STAGES * SB);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nchunks = (p1 - p0 + TMA_ROWS - 1) / TMA_ROWS;
+    const int myn = (int)blockIdx.x < nchunks ? (nchunks - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TMA_STAGES; ++s) mbar_init(&bars[s], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    auto issue = [&](int k) {
+        const int c = blockIdx.x + k * gridDim.x;
+        const int r0 = p0 + c * TMA_ROWS;
+        const int nr = min(TMA_ROWS, p1 - r0);
+        unsigned char *st = smem + (k % TMA_STAGES) * SB;
+        const unsigned bv = (unsigned)(nr * BROW * sizeof(T)), bc = (unsigned)(nr * CROW * 4);
+        mbar_expect_tx(&bars[k % TMA_STAGES], bv + bc);
+        bulk_g2s(st, blk + (size_t)r0 * BROW, bv, &bars[k % TMA_STAGES]);
+        bulk_g2s(st + VB, bcol + (size_t)r0 * CROW, bc, &bars[k % TMA_STAGES]);
+    };
+    if (threadIdx.x == 0)
+        for (int k = 0; k < min(TMA_STAGES, myn); ++k) issue(k);
+    double v0 = 0.0, v1 = 0.0;
+    int k = 0;
+    bool fault = false;
+    for (; k < myn; ++k) {
+        const int st = k % TMA_STAGES;
+        const unsigned par = (unsigned)((k / TMA_STAGES) & 1);
+        const int ok = __syncthreads_and(mbar_wait_bounded(&bars[st], par) ? 1 : 0);
+        if (!ok) {
+            fault = true;
+            break;
+        }
+        const int c = blockIdx.x + k * gridDim.x;
+        const int nr = min(TMA_ROWS, p1 - (p0 + c * TMA_ROWS));
+        if (warp < nr) {
+            const T *vals = reinterpret_cast<const T *>(smem + st * SB) + warp * BROW;
+            const int *cols = reinterpret_cast<const int *>(smem + st * SB + VB) + warp * CROW;
+            RowOps o;
+            o.ns = cols[27];
+            const bool on = lane < o.ns;
+            const int m = on ? cols[lane] : 0;
+            o.n = cols[0];
+#pragma unroll
+            for (int q = 0; q < 9; ++q) o.b[q] = on ? (double)vals[q * 27 + lane] : 0.0;
+            o.x0 = on ? sol[3 * m] : 0.0;
+            o.x1 = on ? sol[3 * m + 1] : 0.0;
+            o.x2 = on ? sol[3 * m + 2] : 0.0;
+            if (lane == 0) {
+                o.r0 = rhs[3 * m];
+                o.r1 = rhs[3 * m + 1];
+                o.r2 = rhs[3 * m + 2];
+            }
+            sor_update(o, lane, sol, base, v0, v1);
+        }
+        __syncthreads();   // every warp is done with this stage
+        if (threadIdx.x == 0 && k + TMA_STAGES < myn) {
+            fence_proxy_async();
+            issue(k + TMA_STAGES);
+        }
+    }
+    if (fault) {
+        if (threadIdx.x == 0) {
+            // copies issued for chunks k .. min(k + STAGES, myn) - 1 may still land
+            for (int j = k; j < min(k + TMA_STAGES, myn); ++j)
+                mbar_wait_bounded(&bars[j % TMA_STAGES], (unsigned)((j / TMA_STAGES) & 1));
+            atomicExch(&ctl->fault, 1);
+        }
+        return;
+    }
+    double v[2] = {v0, v1};
     block_sum_store<2>(v, part + boff, nblk_tot);
 }
 
 // Whole FACSLS solve in one CTA for small meshes: the same warp-per-row
-// point update as k_sor_colour, colours separated by __syncthreads, and the
+// point update as k_sor_colour_tma, colours separated by __syncthreads, and the
 // stopping test (Stif_sol.f90:206-210) evaluated in-block after every sweep.
 // Bounded by maxitl sweeps.  cstart[c] .. cstart[c+1] are the colour ranges.
 __global__ void __launch_bounds__(1024) k_sor_small(BlockDev B, const int *__restrict__ cstart,
@@ -748,26 +879,7 @@ __global__ void __launch_bounds__(1024) k_sor_small(BlockDev B, const int *__res
     }
 }
 
-// ---------------------------------------------------------------- FP32 SOR
-// Tuned FACSLS: sweeps of point SOR on the correction equation K32 d = r with
-// the FP32 copy of the matrix (half the bytes of a sweep), FP64 vectors and
-// arithmetic.  xs is the iterate at the last residual; the stopping measure
-// is the reference's, on the iterate xs + d: sum(change^2) / sum((xs+d)^2).
-__global__ void __launch_bounds__(256, 3) k_sor_colour32(BlockDev B, int p0, int p1,
-                                                      const double *__restrict__ res,
-                                                      const double *__restrict__ xs, double *d,
-                                                      const SorCtl *ctl, double *part, int boff,
-                                                      int nblk_tot)
-{
-    if (((volatile const SorCtl *)ctl)->conv) return;
-    const int lane = threadIdx.x & 31;
-    const int wpb = blockDim.x >> 5;
-    double v[2] = {0.0, 0.0};
-    sor_rows<float>(B, B.blk32, p0 + blockIdx.x * wpb + (threadIdx.x >> 5), p1, gridDim.x * wpb, lane,
-                    res, d, xs, v[0], v[1]);
-    block_sum_store<2>(v, part + boff, nblk_tot);
-}
-
+// ---------------------------------------------------------------- FP32 SOR refinement
 // FP64 residual of the assembled system, r = rhs - K x, one warp per row.
 // Skipped once the solve has converged.
 __global__ void __launch_bounds__(256) k_residual(BlockDev B, const double *__restrict__ rhs,
@@ -978,6 +1090,30 @@ __global__ void k_reorient(DevGp G, DevMat M, TwinEv *ev, int cap, int *nev)
     }
     G.twinsys[j] = 0;
     G.timestwinned[j] = G.timestwinned[j] + 1;
+}
+
+// ELASEPS (src/csvmkr/data_out.f90:263-361): elastic (lattice) strain of
+// every GP, e = S(phi) sigma with the compliance of ELASTC at the committed
+// Euler angles sv(1:3) and the GP's material; out[k * ngps + g].
+__global__ void k_elaseps(DevMat M, DevGp G, const int *gp_iel, double *out)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G.ngps) return;
+    const int ng = G.ngps;
+    const int iel = gp_iel[g];
+    const int mc = (iel < 0 ? -iel : iel) - 1;
+    double S[6][6];
+    elastc(M.e + 9 * mc, G.sv[g], G.sv[ng + g], G.sv[2 * ng + g], S);
+    double st[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) st[k] = G.st[k * ng + g];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        double acc = 0.0;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) acc = acc + S[i][c] * st[c];
+        out[i * ng + g] = acc;
+    }
 }
 
 // ---------------------------------------------------------------- exports

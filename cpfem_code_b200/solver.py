@@ -160,6 +160,15 @@ class _SolverBase:
         self._call("get_tangent", abi.ptr(out), 8)
         return out
 
+    def lattice_strain(self) -> np.ndarray:
+        """ELASEPS for every GP: [ngps, 6] elastic strains (engineering shears)."""
+        out = np.zeros((self.prob.ngps, 6), np.float64)
+        if self.prefix == "fas_gpu":
+            self._call("lattice_strain", abi.ptr(out), 8)
+        else:
+            self._call("lattice_strain", abi.ptr(out))
+        return out
+
     def cp_ops(self) -> np.ndarray:
         out = np.zeros(self.prob.ngps, np.float64)
         self._call("get_cp_ops", out.ctypes.data_as(C.POINTER(C.c_double)))

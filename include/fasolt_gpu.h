@@ -49,6 +49,7 @@ extern "C" {
 #define FAS_E_NOMEM        (-5)  /* device allocation failed                 */
 #define FAS_E_RANGE        (-6)  /* size beyond a documented maximum         */
 #define FAS_E_STATE        (-7)  /* call out of order (e.g. no state yet)    */
+#define FAS_E_TIMEOUT      (-8)  /* a device-side bounded wait gave up       */
 
 #define FAS_MAXSS  60            /* maxss, src/fasolt/fas-com-mod.f90:57     */
 
@@ -233,6 +234,12 @@ FAS_API int32_t fas_gpu_get_tangent(fas_handle *h, void *chi, int32_t real_bytes
 /* Per-GP diagnostics of the last constitutive pass: outer (CPSTRS) iteration
  * count and final erepmd.  Either pointer may be null. */
 FAS_API int32_t fas_gpu_get_cp_stats(fas_handle *h, int32_t *iters, double *erepmd);
+
+/* ELASEPS (src/csvmkr/data_out.f90:263-361): the elastic lattice strain
+ * e = S(sv(1:3)) st of every GP, engineering shears, into strain(6, ngps)
+ * (column-major, element size real_bytes).  The forward map of csvmkr's
+ * el_eps columns. */
+FAS_API int32_t fas_gpu_lattice_strain(fas_handle *h, void *strain, int32_t real_bytes);
 
 /* Per-GP algorithmic operation count of the last constitutive pass (the
  * formulas of fas_flops.h summed over the iterations each GP took). */

@@ -1664,6 +1664,26 @@ int32_t ora_get_cp_ops(ora_problem *p, double *ops)
     return 0;
 }
 
+// ELASEPS, src/csvmkr/data_out.f90:263-361
+int32_t ora_lattice_strain(ora_problem *p, double *out)
+{
+    DISPATCH(p, {
+        if (!out) return FAS_E_ARG;
+        for (int g = 0; g < P.ngps; ++g) {
+            const auto &m = P.mat[std::abs(P.gp_iel[g]) - 1];
+            const auto *sv = &P.sv[(size_t)g * SVLD];
+            decltype(P.toler) S[6][6];
+            elastc(m.e, sv[0], sv[1], sv[2], S);
+            for (int i = 0; i < 6; ++i) {
+                decltype(P.toler) acc = 0;
+                for (int c = 0; c < 6; ++c) acc = acc + S[i][c] * P.st[(size_t)g * 6 + c];
+                out[(size_t)g * 6 + i] = (double)acc;
+            }
+        }
+    });
+    return 0;
+}
+
 double ora_spower(double a, double b) { return spower<double>(a, b); }
 double ora_fj2vom(int32_t stress, const double *x6) { return fj2vom<double>(stress != 0, x6); }
 int32_t ora_factor_solve(int32_t n, const double *a, double *x)

@@ -60,6 +60,9 @@ int32_t ora_get_cp_stats(ora_problem *p, int32_t *iters, double *erepmd);
 /* Per-GP algorithmic operation counts of the last constitutive pass. */
 int32_t ora_get_cp_ops(ora_problem *p, double *ops);
 
+/* ELASEPS (src/csvmkr/data_out.f90:263-361): out[g*6 + k]. */
+int32_t ora_lattice_strain(ora_problem *p, double *out);
+
 /* Low-level single-routine checks for the known-answer tests (double). */
 double  ora_spower(double a, double b);
 double  ora_fj2vom(int32_t stress, const double *x6);

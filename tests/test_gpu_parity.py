@@ -241,3 +241,11 @@ def test_mixed_fcc_hcp_increment(mode):
         assert rel(pg.st, po.st) < 1e-10
         assert rel(pg.sv[:, :33], po.sv[:, :33]) < 1e-10
         np.testing.assert_array_equal(pg.timestwinned, po.timestwinned)
+
+
+def test_lattice_strain():
+    p = generator.structured_cube(n=(3, 3, 3), ninc=1, seed=3)
+    g, o, pg, po = pair(p)
+    g.increment(1)
+    o.increment(1)
+    assert rel(g.lattice_strain(), o.lattice_strain()) < 1e-10

@@ -246,3 +246,16 @@ def test_converged_point_satisfies_crystal_plasticity(oracle_lib):
     theta = mat["ampar"][0, 1] * np.clip(1 - s0 / mat["ampar"][0, 4], 0, None)
     np.testing.assert_allclose(
         s1, s0 + np.einsum("ij,nj,nj->ni", mat["smatrx"], theta, np.abs(gam)), rtol=1e-12)
+
+
+def test_lattice_strain_is_compliance_times_stress(oracle_lib):
+    """ELASEPS (data_out.f90:263-361) = the ELASTC compliance at sv(1:3)
+    times the stress."""
+    from oracle import OracleSolver
+    p, mat = _point_problem(16)
+    rng = np.random.default_rng(9)
+    p.st[:] = rng.standard_normal(p.st.shape) * 50.0
+    o = OracleSolver(p, 8)
+    e = o.lattice_strain()
+    S = generator.rotated_compliance(mat["e"], p.sv[:, :3])
+    np.testing.assert_allclose(e, np.einsum("nij,nj->ni", S, p.st), rtol=1e-13, atol=1e-20)
