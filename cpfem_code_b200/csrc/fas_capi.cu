@@ -357,11 +357,11 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
     int tot = 0;
     for (int c = 0; c < h->ncol; ++c) {
         h->sor_boff[c] = tot;
-        // chunks of TMA_ROWS rows; at most 4 CTAs per SM (their shared-memory
+        // chunks of TMA_ROWS rows; at most 2 CTAs per SM (their shared-memory
         // rings fit together), which also keeps the per-sweep partial sums
         // few enough for a cheap deterministic check
         h->sor_nblk[c] = (int)std::min<long long>(nblocks(h->col_start[c + 1] - h->col_start[c], TMA_ROWS),
-                                                   (long long)h->nsm * 4);
+                                                   (long long)h->nsm * 2);
         tot += h->sor_nblk[c];
     }
     h->sor_nblk_tot = std::max(tot, 1);
@@ -809,11 +809,11 @@ void launch_colour(fas_handle *h, int c, bool fp32)
     const int p0 = h->col_start[c], p1 = h->col_start[c + 1];
     if (p1 <= p0) return;
     if (fp32)
-        k_sor_colour_tma<float><<<h->sor_nblk[c], 32 * TMA_ROWS, tma_smem_bytes<float>(), h->stream>>>(
+        k_sor_colour_tma<float><<<h->sor_nblk[c], TMA_THREADS, tma_smem_bytes<float>(), h->stream>>>(
             h->blk32.p, h->bcol.p, p0, p1, h->sor_r.p, h->sor_d.p, h->ddx.p, h->sorctl.p, h->part_sor.p,
             h->sor_boff[c], h->sor_nblk_tot);
     else
-        k_sor_colour_tma<double><<<h->sor_nblk[c], 32 * TMA_ROWS, tma_smem_bytes<double>(), h->stream>>>(
+        k_sor_colour_tma<double><<<h->sor_nblk[c], TMA_THREADS, tma_smem_bytes<double>(), h->stream>>>(
             h->blk.p, h->bcol.p, p0, p1, h->rhs.p, h->ddx.p, nullptr, h->sorctl.p, h->part_sor.p,
             h->sor_boff[c], h->sor_nblk_tot);
 }

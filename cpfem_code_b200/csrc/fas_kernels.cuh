@@ -701,12 +701,33 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes)
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
 }
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar)
+// L2 cache policies: the streamed matrix is evict-first, the solution
+// vector gathered by every colour phase evict-last.
+__device__ __forceinline__ uint64_t l2_evict_first()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t l2_evict_last()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ double ld_keep(const double *ptr, uint64_t pol)
+{
+    double v;
+    asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(ptr), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar,
+                                         uint64_t pol)
 {
     asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, "
+        "[%3], %4;" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
         : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
@@ -729,7 +750,8 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-constexpr int TMA_ROWS = 8;      // rows per chunk (= warps per CTA)
+constexpr int TMA_ROWS = 16;     // rows per chunk
+constexpr int TMA_THREADS = 64;  // 2 warps; 4 lanes per row
 constexpr int TMA_STAGES = 3;    // chunks in flight per CTA
 
 template <typename T> __host__ __device__ constexpr int tma_stage_bytes()
@@ -742,32 +764,41 @@ template <typename T> __host__ __device__ constexpr int tma_smem_bytes()
 }
 
 // One colour phase of SOR with the colour's block rows streamed through a
-// TMA_STAGES-deep shared-memory ring.  CTA b takes chunks b, b + grid, ...
-// of TMA_ROWS consecutive rows; thread 0 issues the bulk copies (values and
-// column ids of the chunk) and re-arms a stage once all warps have read it;
-// warp w updates row w of the chunk from shared memory.  The solution
-// gathers stay ordinary (L2-resident) loads.  Every mbarrier wait is
-// bounded; on a timeout the CTA waits (bounded) for its own copies still in
-// flight, raises ctl->fault and leaves.
+// TMA_STAGES-deep shared-memory ring by the bulk-copy engine (evict-first in
+// L2).  CTA b takes chunks b, b + grid, ... of TMA_ROWS consecutive rows;
+// thread 0 issues the copies (values and column ids) and re-arms a stage
+// once every row of it is done.  Four lanes serve one row: lane q of the
+// row's quad multiplies the blocks of slots q, q+4, q+8, ... by the solution
+// at their column nodes (gathered with evict-last so the vector stays in
+// L2), the quad sums its three partial products, and its first lane does the
+// x, y, z point update with the diagonal block (slot 0).  Within a colour
+// no row reads a value another row of the colour writes.  Every mbarrier
+// wait is bounded; on a timeout the CTA waits (bounded) for its own copies
+// still in flight, raises ctl->fault and leaves.
 template <typename T>
-__global__ void __launch_bounds__(256) k_sor_colour_tma(const T *__restrict__ blk, const int *__restrict__ bcol,
-                                                        int p0, int p1, const double *__restrict__ rhs,
-                                                        double *sol, const double *__restrict__ base,
-                                                        SorCtl *ctl, double *part, int boff, int nblk_tot)
+__global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restrict__ blk,
+                                                                const int *__restrict__ bcol, int p0, int p1,
+                                                                const double *__restrict__ rhs, double *sol,
+                                                                const double *__restrict__ base, SorCtl *ctl,
+                                                                double *part, int boff, int nblk_tot)
 {
     if (((volatile const SorCtl *)ctl)->conv) return;
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int VB = TMA_ROWS * BROW * (int)sizeof(T);
     constexpr int SB = tma_stage_bytes<T>();
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TMA_STAGES * SB);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int row = threadIdx.x >> 2;     // row of the chunk served by this quad
+    const int q = threadIdx.x & 3;        // lane within the quad
     const int nchunks = (p1 - p0 + TMA_ROWS - 1) / TMA_ROWS;
     const int myn = (int)blockIdx.x < nchunks ? (nchunks - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     if (threadIdx.x == 0) {
-        for (int s = 0; s < TMA_STAGES; ++s) mbar_init(&bars[s], 1);
+        for (int st = 0; st < TMA_STAGES; ++st) mbar_init(&bars[st], 1);
         mbar_fence_init();
     }
     __syncthreads();
+    const uint64_t stream_pol = l2_evict_first();
+    const uint64_t keep_pol = l2_evict_last();
     auto issue = [&](int k) {
         const int c = blockIdx.x + k * gridDim.x;
         const int r0 = p0 + c * TMA_ROWS;
@@ -775,8 +806,8 @@ __global__ void __launch_bounds__(256) k_sor_colour_tma(const T *__restrict__ bl
         unsigned char *st = smem + (k % TMA_STAGES) * SB;
         const unsigned bv = (unsigned)(nr * BROW * sizeof(T)), bc = (unsigned)(nr * CROW * 4);
         mbar_expect_tx(&bars[k % TMA_STAGES], bv + bc);
-        bulk_g2s(st, blk + (size_t)r0 * BROW, bv, &bars[k % TMA_STAGES]);
-        bulk_g2s(st + VB, bcol + (size_t)r0 * CROW, bc, &bars[k % TMA_STAGES]);
+        bulk_g2s(st, blk + (size_t)r0 * BROW, bv, &bars[k % TMA_STAGES], stream_pol);
+        bulk_g2s(st + VB, bcol + (size_t)r0 * CROW, bc, &bars[k % TMA_STAGES], stream_pol);
     };
     if (threadIdx.x == 0)
         for (int k = 0; k < min(TMA_STAGES, myn); ++k) issue(k);
@@ -793,32 +824,71 @@ __global__ void __launch_bounds__(256) k_sor_colour_tma(const T *__restrict__ bl
         }
         const int c = blockIdx.x + k * gridDim.x;
         const int nr = min(TMA_ROWS, p1 - (p0 + c * TMA_ROWS));
-        if (warp < nr) {
-            const T *vals = reinterpret_cast<const T *>(smem + st * SB) + warp * BROW;
-            const int *cols = reinterpret_cast<const int *>(smem + st * SB + VB) + warp * CROW;
-            RowOps o;
-            o.ns = cols[27];
-            const bool on = lane < o.ns;
-            const int m = on ? cols[lane] : 0;
-            o.n = cols[0];
+        const bool live = row < nr;
+        const T *vals = reinterpret_cast<const T *>(smem + st * SB) + (live ? row : 0) * BROW;
+        const int *cols = reinterpret_cast<const int *>(smem + st * SB + VB) + (live ? row : 0) * CROW;
+        const int ns = live ? cols[27] : 0;
+        // this lane's slots: q, q + 4, ..., below ns (slot 0 is the diagonal)
+        double xs0[7], xs1[7], xs2[7];
 #pragma unroll
-            for (int q = 0; q < 9; ++q) o.b[q] = on ? (double)vals[q * 27 + lane] : 0.0;
-            o.x0 = on ? sol[3 * m] : 0.0;
-            o.x1 = on ? sol[3 * m + 1] : 0.0;
-            o.x2 = on ? sol[3 * m + 2] : 0.0;
-            if (lane == 0) {
-                o.r0 = rhs[3 * m];
-                o.r1 = rhs[3 * m + 1];
-                o.r2 = rhs[3 * m + 2];
-            }
-            sor_update(o, lane, sol, base, v0, v1);
+        for (int j = 0; j < 7; ++j) {
+            const int sl = q + 4 * j;
+            const bool on = sl < ns;
+            const int m = on ? cols[sl] : 0;
+            xs0[j] = on ? ld_keep(sol + 3 * m, keep_pol) : 0.0;
+            xs1[j] = on ? ld_keep(sol + 3 * m + 1, keep_pol) : 0.0;
+            xs2[j] = on ? ld_keep(sol + 3 * m + 2, keep_pol) : 0.0;
         }
-        __syncthreads();   // every warp is done with this stage
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+#pragma unroll
+        for (int j = 0; j < 7; ++j) {
+            const int sl = q + 4 * j;
+            if (sl >= 1 && sl < ns) {
+                const T *b = vals + sl;
+                a0 += (double)b[0 * 27] * xs0[j] + (double)b[1 * 27] * xs1[j] + (double)b[2 * 27] * xs2[j];
+                a1 += (double)b[3 * 27] * xs0[j] + (double)b[4 * 27] * xs1[j] + (double)b[5 * 27] * xs2[j];
+                a2 += (double)b[6 * 27] * xs0[j] + (double)b[7 * 27] * xs1[j] + (double)b[8 * 27] * xs2[j];
+            }
+        }
+        a0 += __shfl_xor_sync(0xffffffffu, a0, 1);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, 1);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, 1);
+        a0 += __shfl_xor_sync(0xffffffffu, a0, 2);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, 2);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, 2);
+        if (live && q == 0) {
+            const int n = cols[0];
+            double D[9];
+#pragma unroll
+            for (int qq = 0; qq < 9; ++qq) D[qq] = (double)vals[qq * 27];
+            const double o0 = xs0[0], o1 = xs1[0], o2 = xs2[0];
+            const double r0v = ld_keep(rhs + 3 * n, keep_pol), r1v = ld_keep(rhs + 3 * n + 1, keep_pol),
+                         r2v = ld_keep(rhs + 3 * n + 2, keep_pol);
+            double x0 = o0, x1 = o1, x2 = o2;
+            double t = (r0v - (a0 + D[1] * x1 + D[2] * x2)) / D[0];
+            x0 = x0 + 1.2 * (t - x0);
+            t = (r1v - (a1 + D[3] * x0 + D[5] * x2)) / D[4];
+            x1 = x1 + 1.2 * (t - x1);
+            t = (r2v - (a2 + D[6] * x0 + D[7] * x1)) / D[8];
+            x2 = x2 + 1.2 * (t - x2);
+            sol[3 * n] = x0;
+            sol[3 * n + 1] = x1;
+            sol[3 * n + 2] = x2;
+            v0 += (x0 - o0) * (x0 - o0) + (x1 - o1) * (x1 - o1) + (x2 - o2) * (x2 - o2);
+            if (base) {
+                x0 += base[3 * n];
+                x1 += base[3 * n + 1];
+                x2 += base[3 * n + 2];
+            }
+            v1 += x0 * x0 + x1 * x1 + x2 * x2;
+        }
+        __syncthreads();   // every row of this stage is done
         if (threadIdx.x == 0 && k + TMA_STAGES < myn) {
             fence_proxy_async();
             issue(k + TMA_STAGES);
         }
     }
+    (void)lane;
     if (fault) {
         if (threadIdx.x == 0) {
             // copies issued for chunks k .. min(k + STAGES, myn) - 1 may still land
