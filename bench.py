@@ -334,7 +334,7 @@ def run_gpu(args):
             "data": "synthetic (seeded generator, fs3pre semantics)",
             "config": {"workload": WORKLOAD, "desc": DESC, "parallelism": f"replicas{ws}",
                        "increments": [incs[0], incs[-1]], "newton_iters": nit, "sor_sweeps": sweeps,
-                       "l2": "inputs larger than L2 (534 MB block matrix re-read every sweep)"},
+                       "l2": "inputs larger than L2 (536 MB block matrix re-read every sweep)"},
             "s_per_increment": t_max / args.steps,
             "wall_s": wall,
             "gpu_launches": int(prof["n_launches"]),

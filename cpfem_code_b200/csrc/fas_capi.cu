@@ -357,11 +357,11 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
     int tot = 0;
     for (int c = 0; c < h->ncol; ++c) {
         h->sor_boff[c] = tot;
-        // chunks of TMA_ROWS rows; at most 2 CTAs per SM (their shared-memory
-        // rings fit together), which also keeps the per-sweep partial sums
-        // few enough for a cheap deterministic check
+        // chunks of TMA_ROWS rows; one wave of as many CTAs as the
+        // shared-memory rings let reside per SM, which also keeps the
+        // per-sweep partial sums few enough for a cheap deterministic check
         h->sor_nblk[c] = (int)std::min<long long>(nblocks(h->col_start[c + 1] - h->col_start[c], TMA_ROWS),
-                                                   (long long)h->nsm * 2);
+                                                   (long long)h->nsm * TMA_CTAS_PER_SM);
         tot += h->sor_nblk[c];
     }
     h->sor_nblk_tot = std::max(tot, 1);

@@ -750,9 +750,28 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-constexpr int TMA_ROWS = 16;     // rows per chunk
-constexpr int TMA_THREADS = 64;  // 2 warps; 4 lanes per row
-constexpr int TMA_STAGES = 3;    // chunks in flight per CTA
+// Launch shape of the colour kernel (compile-time; -D overrides for tuning).
+#ifndef FAS_TMA_ROWS
+#define FAS_TMA_ROWS 8
+#endif
+#ifndef FAS_TMA_LPR
+#define FAS_TMA_LPR 8
+#endif
+#ifndef FAS_TMA_STAGES
+#define FAS_TMA_STAGES 3
+#endif
+#ifndef FAS_TMA_PD
+#define FAS_TMA_PD 1
+#endif
+constexpr int TMA_ROWS = FAS_TMA_ROWS;       // rows per chunk
+constexpr int TMA_LPR = FAS_TMA_LPR;         // lanes per row (a power of two, at most 32)
+constexpr int TMA_SPL = (SLOTS + TMA_LPR - 1) / TMA_LPR;   // slots per lane
+constexpr int TMA_THREADS = TMA_ROWS * TMA_LPR;
+constexpr int TMA_STAGES = FAS_TMA_STAGES;   // chunks in flight per CTA
+constexpr int TMA_PD = FAS_TMA_PD;           // chunks whose gathers run ahead of the computed one
+static_assert(TMA_PD >= 1 && TMA_PD < TMA_STAGES, "gathers run ahead within the ring");
+static_assert(TMA_LPR >= 1 && TMA_LPR <= 32 && (TMA_LPR & (TMA_LPR - 1)) == 0, "lanes per row");
+static_assert(TMA_THREADS % 32 == 0 && TMA_THREADS <= 1024, "whole warps per CTA");
 
 template <typename T> __host__ __device__ constexpr int tma_stage_bytes()
 {
@@ -762,17 +781,25 @@ template <typename T> __host__ __device__ constexpr int tma_smem_bytes()
 {
     return TMA_STAGES * tma_stage_bytes<T>() + TMA_STAGES * 8;
 }
+// CTAs of the FP64 kernel that fit on one SM (228 KB of shared memory,
+// 1 KB of it reserved per CTA); the colour grid is sized to fill them.
+constexpr int TMA_CTAS_PER_SM = (228 * 1024) / (tma_smem_bytes<double>() + 1024) < 32 / (TMA_THREADS / 32)
+                                    ? (228 * 1024) / (tma_smem_bytes<double>() + 1024)
+                                    : 32 / (TMA_THREADS / 32);
+static_assert(TMA_CTAS_PER_SM >= 1, "the ring must fit in shared memory");
 
 // One colour phase of SOR with the colour's block rows streamed through a
 // TMA_STAGES-deep shared-memory ring by the bulk-copy engine (evict-first in
 // L2).  CTA b takes chunks b, b + grid, ... of TMA_ROWS consecutive rows;
 // thread 0 issues the copies (values and column ids) and re-arms a stage
-// once every row of it is done.  Four lanes serve one row: lane q of the
-// row's quad multiplies the blocks of slots q, q+4, q+8, ... by the solution
+// once every row of it is done.  TMA_LPR lanes serve one row: lane q of the
+// row's group multiplies the blocks of slots q, q+LPR, ... by the solution
 // at their column nodes (gathered with evict-last so the vector stays in
-// L2), the quad sums its three partial products, and its first lane does the
+// L2), the group sums its three partial products, and its first lane does the
 // x, y, z point update with the diagonal block (slot 0).  Within a colour
-// no row reads a value another row of the colour writes.  Every mbarrier
+// no row reads a value another row of the colour writes, so the gathers of
+// chunk k+1 (and its right-hand side) are issued before chunk k is
+// computed: one L2 round trip per chunk is hidden.  Every mbarrier
 // wait is bounded; on a timeout the CTA waits (bounded) for its own copies
 // still in flight, raises ctl->fault and leaves.
 template <typename T>
@@ -788,8 +815,8 @@ __global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restr
     constexpr int SB = tma_stage_bytes<T>();
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TMA_STAGES * SB);
     const int lane = threadIdx.x & 31;
-    const int row = threadIdx.x >> 2;     // row of the chunk served by this quad
-    const int q = threadIdx.x & 3;        // lane within the quad
+    const int row = threadIdx.x / TMA_LPR;   // row of the chunk served by this group
+    const int q = threadIdx.x % TMA_LPR;     // lane within the group
     const int nchunks = (p1 - p0 + TMA_ROWS - 1) / TMA_ROWS;
     const int myn = (int)blockIdx.x < nchunks ? (nchunks - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     if (threadIdx.x == 0) {
@@ -812,64 +839,96 @@ __global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restr
     if (threadIdx.x == 0)
         for (int k = 0; k < min(TMA_STAGES, myn); ++k) issue(k);
     double v0 = 0.0, v1 = 0.0;
-    int k = 0;
-    bool fault = false;
-    for (; k < myn; ++k) {
-        const int st = k % TMA_STAGES;
-        const unsigned par = (unsigned)((k / TMA_STAGES) & 1);
-        const int ok = __syncthreads_and(mbar_wait_bounded(&bars[st], par) ? 1 : 0);
-        if (!ok) {
-            fault = true;
-            break;
+    // Gathered operands: set 0 belongs to the chunk being computed, set j
+    // to chunk k + j.  No row of a colour reads a value written by another
+    // row of the same colour, so the gathers of the next TMA_PD chunks are
+    // in flight while chunk k is computed.
+    double gx0[TMA_PD + 1][TMA_SPL] = {}, gx1[TMA_PD + 1][TMA_SPL] = {}, gx2[TMA_PD + 1][TMA_SPL] = {};
+    double gr[TMA_PD + 1][3] = {};
+    auto gather = [&](int kk, double (&g0)[TMA_SPL], double (&g1)[TMA_SPL], double (&g2)[TMA_SPL],
+                      double (&grr)[3]) {
+        const int c = blockIdx.x + kk * gridDim.x;
+        const int nrow = min(TMA_ROWS, p1 - (p0 + c * TMA_ROWS));
+        const bool live = row < nrow;
+        const int *cols = reinterpret_cast<const int *>(smem + (kk % TMA_STAGES) * SB + VB) + (live ? row : 0) * CROW;
+        const int ns = live ? cols[27] : 0;
+#pragma unroll
+        for (int j = 0; j < TMA_SPL; ++j) {
+            const int sl = q + TMA_LPR * j;
+            const bool on = sl < ns;
+            const int m = on ? cols[sl] : 0;
+            g0[j] = on ? ld_keep(sol + 3 * m, keep_pol) : 0.0;
+            g1[j] = on ? ld_keep(sol + 3 * m + 1, keep_pol) : 0.0;
+            g2[j] = on ? ld_keep(sol + 3 * m + 2, keep_pol) : 0.0;
         }
+        const bool own = live && q == 0;
+        const int n = cols[0];
+        grr[0] = own ? ld_keep(rhs + 3 * n, keep_pol) : 0.0;
+        grr[1] = own ? ld_keep(rhs + 3 * n + 1, keep_pol) : 0.0;
+        grr[2] = own ? ld_keep(rhs + 3 * n + 2, keep_pol) : 0.0;
+    };
+    // chunks [0, waited) have landed; chunks [0, min(myn, k + TMA_STAGES))
+    // have been issued when iteration k starts
+    int waited = 0, k = 0;
+    bool fault = false;
+#pragma unroll
+    for (int i = 0; i < TMA_PD; ++i) {
+        if (!fault && i < myn) {
+            if (__syncthreads_and(mbar_wait_bounded(&bars[i], 0u) ? 1 : 0)) {
+                waited = i + 1;
+                gather(i, gx0[i], gx1[i], gx2[i], gr[i]);
+            } else {
+                fault = true;
+            }
+        }
+    }
+    for (; !fault && k < myn; ++k) {
+        if (k + TMA_PD < myn) {
+            const int kk = k + TMA_PD;
+            const unsigned par = (unsigned)((kk / TMA_STAGES) & 1);
+            if (!__syncthreads_and(mbar_wait_bounded(&bars[kk % TMA_STAGES], par) ? 1 : 0)) {
+                fault = true;
+                break;
+            }
+            waited = kk + 1;
+            gather(kk, gx0[TMA_PD], gx1[TMA_PD], gx2[TMA_PD], gr[TMA_PD]);
+        }
+        const int st = k % TMA_STAGES;
         const int c = blockIdx.x + k * gridDim.x;
-        const int nr = min(TMA_ROWS, p1 - (p0 + c * TMA_ROWS));
-        const bool live = row < nr;
+        const int nrow = min(TMA_ROWS, p1 - (p0 + c * TMA_ROWS));
+        const bool live = row < nrow;
         const T *vals = reinterpret_cast<const T *>(smem + st * SB) + (live ? row : 0) * BROW;
         const int *cols = reinterpret_cast<const int *>(smem + st * SB + VB) + (live ? row : 0) * CROW;
         const int ns = live ? cols[27] : 0;
-        // this lane's slots: q, q + 4, ..., below ns (slot 0 is the diagonal)
-        double xs0[7], xs1[7], xs2[7];
-#pragma unroll
-        for (int j = 0; j < 7; ++j) {
-            const int sl = q + 4 * j;
-            const bool on = sl < ns;
-            const int m = on ? cols[sl] : 0;
-            xs0[j] = on ? ld_keep(sol + 3 * m, keep_pol) : 0.0;
-            xs1[j] = on ? ld_keep(sol + 3 * m + 1, keep_pol) : 0.0;
-            xs2[j] = on ? ld_keep(sol + 3 * m + 2, keep_pol) : 0.0;
-        }
         double a0 = 0.0, a1 = 0.0, a2 = 0.0;
 #pragma unroll
-        for (int j = 0; j < 7; ++j) {
-            const int sl = q + 4 * j;
+        for (int j = 0; j < TMA_SPL; ++j) {
+            const int sl = q + TMA_LPR * j;
             if (sl >= 1 && sl < ns) {
                 const T *b = vals + sl;
-                a0 += (double)b[0 * 27] * xs0[j] + (double)b[1 * 27] * xs1[j] + (double)b[2 * 27] * xs2[j];
-                a1 += (double)b[3 * 27] * xs0[j] + (double)b[4 * 27] * xs1[j] + (double)b[5 * 27] * xs2[j];
-                a2 += (double)b[6 * 27] * xs0[j] + (double)b[7 * 27] * xs1[j] + (double)b[8 * 27] * xs2[j];
+                a0 += (double)b[0 * 27] * gx0[0][j] + (double)b[1 * 27] * gx1[0][j] + (double)b[2 * 27] * gx2[0][j];
+                a1 += (double)b[3 * 27] * gx0[0][j] + (double)b[4 * 27] * gx1[0][j] + (double)b[5 * 27] * gx2[0][j];
+                a2 += (double)b[6 * 27] * gx0[0][j] + (double)b[7 * 27] * gx1[0][j] + (double)b[8 * 27] * gx2[0][j];
             }
         }
-        a0 += __shfl_xor_sync(0xffffffffu, a0, 1);
-        a1 += __shfl_xor_sync(0xffffffffu, a1, 1);
-        a2 += __shfl_xor_sync(0xffffffffu, a2, 1);
-        a0 += __shfl_xor_sync(0xffffffffu, a0, 2);
-        a1 += __shfl_xor_sync(0xffffffffu, a1, 2);
-        a2 += __shfl_xor_sync(0xffffffffu, a2, 2);
+#pragma unroll
+        for (int o = 1; o < TMA_LPR; o <<= 1) {
+            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        }
         if (live && q == 0) {
             const int n = cols[0];
             double D[9];
 #pragma unroll
             for (int qq = 0; qq < 9; ++qq) D[qq] = (double)vals[qq * 27];
-            const double o0 = xs0[0], o1 = xs1[0], o2 = xs2[0];
-            const double r0v = ld_keep(rhs + 3 * n, keep_pol), r1v = ld_keep(rhs + 3 * n + 1, keep_pol),
-                         r2v = ld_keep(rhs + 3 * n + 2, keep_pol);
+            const double o0 = gx0[0][0], o1 = gx1[0][0], o2 = gx2[0][0];
             double x0 = o0, x1 = o1, x2 = o2;
-            double t = (r0v - (a0 + D[1] * x1 + D[2] * x2)) / D[0];
+            double t = (gr[0][0] - (a0 + D[1] * x1 + D[2] * x2)) / D[0];
             x0 = x0 + 1.2 * (t - x0);
-            t = (r1v - (a1 + D[3] * x0 + D[5] * x2)) / D[4];
+            t = (gr[0][1] - (a1 + D[3] * x0 + D[5] * x2)) / D[4];
             x1 = x1 + 1.2 * (t - x1);
-            t = (r2v - (a2 + D[6] * x0 + D[7] * x1)) / D[8];
+            t = (gr[0][2] - (a2 + D[6] * x0 + D[7] * x1)) / D[8];
             x2 = x2 + 1.2 * (t - x2);
             sol[3 * n] = x0;
             sol[3 * n + 1] = x1;
@@ -887,12 +946,24 @@ __global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restr
             fence_proxy_async();
             issue(k + TMA_STAGES);
         }
+#pragma unroll
+        for (int i = 0; i < TMA_PD; ++i) {
+#pragma unroll
+            for (int j = 0; j < TMA_SPL; ++j) {
+                gx0[i][j] = gx0[i + 1][j];
+                gx1[i][j] = gx1[i + 1][j];
+                gx2[i][j] = gx2[i + 1][j];
+            }
+            gr[i][0] = gr[i + 1][0];
+            gr[i][1] = gr[i + 1][1];
+            gr[i][2] = gr[i + 1][2];
+        }
     }
     (void)lane;
     if (fault) {
         if (threadIdx.x == 0) {
-            // copies issued for chunks k .. min(k + STAGES, myn) - 1 may still land
-            for (int j = k; j < min(k + TMA_STAGES, myn); ++j)
+            // copies issued and not yet seen to land may still write the ring
+            for (int j = waited; j < min(myn, k + TMA_STAGES); ++j)
                 mbar_wait_bounded(&bars[j % TMA_STAGES], (unsigned)((j / TMA_STAGES) & 1));
             atomicExch(&ctl->fault, 1);
         }
