@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -1322,3 +1323,112 @@ int32_t fas_gpu_profile(fas_handle *h, int32_t enable, fas_profile *out)
 }
 
 }  // extern "C"
+
+// ================================================================ FACSLS
+// without device allocation.  No counterpart in the reference: it exists
+// for callers that must not allocate device memory once set-up is over
+// (fas_gpu_facsls_noalloc in fasolt_gpu.h says who and why).
+//
+// The SOR kernels' scratch -- the control words of the stopping test
+// (SorCtl) and the per-CTA reduction partials -- lives in this file-scope
+// array instead of in buffers of the handle: a 256-byte block for the
+// control words, then FAS_NOALLOC_PARTIALS pairs of doubles (the sums of
+// |dx|^2 and |x|^2 of every colour CTA).  131,328 bytes per device.
+static __device__ __align__(256) unsigned char fas_noalloc_scratch[256 + 2 * sizeof(double) * FAS_NOALLOC_PARTIALS];
+
+namespace {
+
+constexpr size_t NOALLOC_CTL_BYTES = 256;
+constexpr int NOALLOC_MAXDEV = 64;
+static_assert(sizeof(SorCtl) <= NOALLOC_CTL_BYTES, "control words exceed their block");
+
+std::mutex g_noalloc_mu;
+unsigned char *g_noalloc_addr[NOALLOC_MAXDEV] = {};
+
+// The device address of fas_noalloc_scratch on device `dev`, looked up
+// once per device (with that device current) and cached.
+int noalloc_scratch(int dev, unsigned char **out)
+{
+    if (dev < 0 || dev >= NOALLOC_MAXDEV) return FAS_E_RANGE;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        int cur = -1;
+        CK(cudaGetDevice(&cur));
+        if (cur != dev) CK(cudaSetDevice(dev));
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, fas_noalloc_scratch);
+        if (cur != dev) CK(cudaSetDevice(cur));
+        if (e != cudaSuccess || !p) return FAS_E_CUDA;
+        g_noalloc_addr[dev] = static_cast<unsigned char *>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return 0;
+}
+
+// The FP64 FACSLS of facsls_impl (same kernels, colour order, sweep
+// chunks and stopping test) on the static scratch; no CUDA graph, no
+// FP32-matrix sweeps, no profiling spans.
+int facsls_noalloc_impl(fas_handle *h, int *sweeps, double *error)
+{
+    if (h->sor_nblk_tot > FAS_NOALLOC_PARTIALS) return FAS_E_RANGE;
+    unsigned char *scr = nullptr;
+    const int rc = noalloc_scratch(h->dev, &scr);
+    if (rc) return rc;
+    SorCtl *ctl = reinterpret_cast<SorCtl *>(scr);
+    double *part = reinterpret_cast<double *>(scr + NOALLOC_CTL_BYTES);
+    cudaStream_t s = h->stream;
+    const size_t nd3 = 3 * (size_t)h->nnod;
+    CK(cudaMemcpyAsync(h->rhs.p, h->ddx.p, nd3 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemsetAsync(h->ddx.p, 0, nd3 * sizeof(double), s));
+    CK(cudaMemsetAsync(h->ekey.p + 1, 0xFF, sizeof(unsigned long long), s));
+    CK(cudaMemsetAsync(ctl, 0, sizeof(SorCtl), s));   // the control words start every solve at zero
+    BlockDev B = h->block();
+    k_diag_check<<<nblocks(h->nnod, 256), 256, 0, s>>>(B, h->ekey.p + 1);
+    LAUNCHED(h);
+    CK(cudaMemcpyAsync(&h->hc->ekey[1], h->ekey.p + 1, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (h->hc->ekey[1] != ~0ull) return 903;
+    const double tolerl = h->C.toler * h->C.toler;
+    if (h->sor_small && !(h->mode & FAS_MODE_SOR_GRID)) {
+        k_sor_small<<<1, 1024, 0, s>>>(B, h->d_cstart.p, h->ncol, h->rhs.p, h->ddx.p, ctl, tolerl, 1000);
+        LAUNCHED(h);
+    } else {
+        int done = 0, chunk = 4;
+        while (done < 1000) {
+            const int k = std::min(chunk, 1000 - done);
+            for (int it = 0; it < k; ++it) {
+                for (int c = 0; c < h->ncol; ++c) {
+                    const int p0 = h->col_start[c], p1 = h->col_start[c + 1];
+                    if (p1 <= p0) continue;
+                    k_sor_colour_tma<double><<<h->sor_nblk[c], TMA_THREADS, tma_smem_bytes<double>(), s>>>(
+                        h->blk.p, h->bcol.p, p0, p1, h->rhs.p, h->ddx.p, nullptr, ctl, part, h->sor_boff[c],
+                        h->sor_nblk_tot);
+                    LAUNCHED(h);
+                }
+                k_sor_check<<<1, 1024, 0, s>>>(part, h->sor_nblk_tot, ctl, tolerl);
+                LAUNCHED(h);
+            }
+            done += k;
+            CK(cudaMemcpyAsync(&h->hc->sor, ctl, sizeof(SorCtl), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            if (h->hc->sor.conv || h->hc->sor.fault) break;
+            chunk = std::min(chunk * 2, 64);
+        }
+    }
+    CK(cudaMemcpyAsync(&h->hc->sor, ctl, sizeof(SorCtl), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (sweeps) *sweeps = h->hc->sor.sweeps;
+    if (error) *error = h->hc->sor.err;
+    if (h->hc->sor.fault) return FAS_E_TIMEOUT;
+    if (h->hc->sor.err > 10.0 * tolerl) return 904;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" int32_t fas_gpu_facsls_noalloc(fas_handle *h, int32_t *sweeps, double *error)
+{
+    if (!h) return FAS_E_ARG;
+    if (!h->have_state || h->point_mode) return FAS_E_STATE;
+    return facsls_noalloc_impl(h, sweeps, error);
+}

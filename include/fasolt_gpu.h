@@ -267,6 +267,43 @@ typedef struct fas_profile {
  * are written to it first. */
 FAS_API int32_t fas_gpu_profile(fas_handle *h, int32_t enable, fas_profile *out);
 
+/* FACSLS that allocates no device memory in the call.  No counterpart in
+ * the reference.
+ *
+ * Who needs it: a driver that must not allocate device memory once set-up
+ * is over -- one that hands all memory left after fas_gpu_create to
+ * another allocator (a coupled solver's pool, a caching allocator) or runs
+ * under a fixed device-memory cap.  fas_gpu_facsls allocates on first use
+ * (it instantiates a CUDA graph of its sweeps), which can then fail in
+ * the middle of a run; this entry point never does.
+ *
+ * What it does: the same solve as fas_gpu_facsls -- same kernels, colour
+ * order, sweep count and stopping test, same return codes (903, 904,
+ * FAS_E_TIMEOUT) -- on the FP64 blocks, with the kernels' scratch (the
+ * stopping-test control words and one pair of partial sums per colour
+ * CTA) in a static device array of this library instead of buffers of the
+ * handle.  It ignores FAS_MODE_SOR_FP32 and is not timed by
+ * fas_gpu_profile.
+ *
+ * Limits and rules:
+ *  - the array holds FAS_NOALLOC_PARTIALS partial pairs (131,328 bytes per
+ *    device, held by every GPU that loads the library until the process
+ *    exits); a handle whose layout needs more (colours x CTAs per colour;
+ *    a structured brick mesh on a 148-SM B200 needs 8 x 592) gets
+ *    FAS_E_RANGE;
+ *  - the first call on each device looks up the array's device address
+ *    (cudaGetSymbolAddress, with the handle's device made current for the
+ *    look-up); make that first call before any stream capture begins;
+ *  - the control words must be zero when a solve starts: every call zeroes
+ *    them itself on the handle's stream before its first sweep; the
+ *    partial sums need no initial value (each is written before it is
+ *    read);
+ *  - there is one array per device and process, so calls that overlap in
+ *    time on the same device (two host threads, two handles) race on it:
+ *    the caller must serialise them. */
+#define FAS_NOALLOC_PARTIALS 8192
+FAS_API int32_t fas_gpu_facsls_noalloc(fas_handle *h, int32_t *sweeps, double *error);
+
 #ifdef __cplusplus
 }
 #endif
