@@ -803,6 +803,26 @@ int suvals_impl(fas_handle *h, int inc)
 // GRAPH_SWEEPS * (ncol + 1) kernel launches.
 constexpr int GRAPH_SWEEPS = 4;
 
+// Launch with programmatic stream serialisation: the kernel may start while
+// the previous kernel of the stream drains and waits for it with
+// pdl_wait() (the SOR colour and check kernels do).
+template <typename... KArgs, typename... Args>
+void launch_pdl(void (*kern)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+                Args... args)
+{
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 // One colour phase: FP64 blocks on (rhs, sol), or the FP32 copy on the
 // refinement's (residual, correction) with the iterate as base.
 void launch_colour(fas_handle *h, int c, bool fp32)
@@ -810,20 +830,25 @@ void launch_colour(fas_handle *h, int c, bool fp32)
     const int p0 = h->col_start[c], p1 = h->col_start[c + 1];
     if (p1 <= p0) return;
     if (fp32)
-        k_sor_colour_tma<float><<<h->sor_nblk[c], TMA_THREADS, tma_smem_bytes<float>(), h->stream>>>(
-            h->blk32.p, h->bcol.p, p0, p1, h->sor_r.p, h->sor_d.p, h->ddx.p, h->sorctl.p, h->part_sor.p,
-            h->sor_boff[c], h->sor_nblk_tot);
+        launch_pdl(k_sor_colour_tma<float>, h->sor_nblk[c], TMA_THREADS, tma_smem_bytes<float>(), h->stream,
+                   h->blk32.p, h->bcol.p, p0, p1, h->sor_r.p, h->sor_d.p, h->ddx.p, h->sorctl.p, h->part_sor.p,
+                   h->sor_boff[c], h->sor_nblk_tot);
     else
-        k_sor_colour_tma<double><<<h->sor_nblk[c], TMA_THREADS, tma_smem_bytes<double>(), h->stream>>>(
-            h->blk.p, h->bcol.p, p0, p1, h->rhs.p, h->ddx.p, nullptr, h->sorctl.p, h->part_sor.p,
-            h->sor_boff[c], h->sor_nblk_tot);
+        launch_pdl(k_sor_colour_tma<double>, h->sor_nblk[c], TMA_THREADS, tma_smem_bytes<double>(), h->stream,
+                   h->blk.p, h->bcol.p, p0, p1, h->rhs.p, h->ddx.p, (const double *)nullptr, h->sorctl.p,
+                   h->part_sor.p, h->sor_boff[c], h->sor_nblk_tot);
+}
+
+void launch_check(fas_handle *h, double tolerl)
+{
+    launch_pdl(k_sor_check, 1, 1024, 0, h->stream, h->part_sor.p, h->sor_nblk_tot, h->sorctl.p, tolerl);
 }
 
 void launch_plain_sweep(fas_handle *h, const BlockDev &B, double tolerl)
 {
     (void)B;
     for (int c = 0; c < h->ncol; ++c) launch_colour(h, c, false);
-    k_sor_check<<<1, 1024, 0, h->stream>>>(h->part_sor.p, h->sor_nblk_tot, h->sorctl.p, tolerl);
+    launch_check(h, tolerl);
 }
 
 int ensure_sor_graph(fas_handle *h, const BlockDev &B, double tolerl)
@@ -890,7 +915,7 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
                         keep(h, sp);
                         LAUNCHED(h);
                     }
-                    k_sor_check<<<1, 1024, 0, s>>>(h->part_sor.p, h->sor_nblk_tot, h->sorctl.p, tolerl);
+                    launch_check(h, tolerl);
                     LAUNCHED(h);
                 }
                 done += k;
@@ -921,7 +946,7 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
                 keep(h, sp);
                 LAUNCHED(h);
             }
-            k_sor_check<<<1, 1024, 0, s>>>(h->part_sor.p, h->sor_nblk_tot, h->sorctl.p, tolerl);
+            launch_check(h, tolerl);
             LAUNCHED(h);
         }
         done += k;

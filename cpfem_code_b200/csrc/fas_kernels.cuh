@@ -749,6 +749,13 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity
     return false;
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialisation may start while the previous kernel of the stream drains.
+// pdl_wait() returns once that kernel has completed and its writes are
+// visible; before it, only data the previous kernel does not write may be
+// touched.  Under an ordinary launch both are no-ops.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // Launch shape of the colour kernel (compile-time; -D overrides for tuning).
 #ifndef FAS_TMA_ROWS
@@ -809,8 +816,8 @@ __global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restr
                                                                 const double *__restrict__ base, SorCtl *ctl,
                                                                 double *part, int boff, int nblk_tot)
 {
-    if (((volatile const SorCtl *)ctl)->conv) return;
     extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int s_pre, s_post;
     constexpr int VB = TMA_ROWS * BROW * (int)sizeof(T);
     constexpr int SB = tma_stage_bytes<T>();
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TMA_STAGES * SB);
@@ -819,11 +826,6 @@ __global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restr
     const int q = threadIdx.x % TMA_LPR;     // lane within the group
     const int nchunks = (p1 - p0 + TMA_ROWS - 1) / TMA_ROWS;
     const int myn = (int)blockIdx.x < nchunks ? (nchunks - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
-    if (threadIdx.x == 0) {
-        for (int st = 0; st < TMA_STAGES; ++st) mbar_init(&bars[st], 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
     const uint64_t stream_pol = l2_evict_first();
     const uint64_t keep_pol = l2_evict_last();
     auto issue = [&](int k) {
@@ -836,8 +838,29 @@ __global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restr
         bulk_g2s(st, blk + (size_t)r0 * BROW, bv, &bars[k % TMA_STAGES], stream_pol);
         bulk_g2s(st + VB, bcol + (size_t)r0 * CROW, bc, &bars[k % TMA_STAGES], stream_pol);
     };
-    if (threadIdx.x == 0)
-        for (int k = 0; k < min(TMA_STAGES, myn); ++k) issue(k);
+    // Prologue, overlapped with the previous kernel under a programmatic
+    // launch.  The stopping flag only goes from 0 to 1 within a solve, so a
+    // flag already set here is final and nothing is copied; the blocks and
+    // column ids do not change during a solve, so their first copies may
+    // start before the previous kernel has finished.
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < TMA_STAGES; ++st) mbar_init(&bars[st], 1);
+        mbar_fence_init();
+        s_pre = ((volatile const SorCtl *)ctl)->conv;
+        if (!s_pre)
+            for (int k = 0; k < min(TMA_STAGES, myn); ++k) issue(k);
+    }
+    __syncthreads();
+    pdl_launch_dependents();
+    if (s_pre) return;
+    pdl_wait();   // the previous colour's solution values and the flag are visible from here
+    if (threadIdx.x == 0) s_post = ((volatile const SorCtl *)ctl)->conv;
+    __syncthreads();
+    if (s_post) {
+        if (threadIdx.x == 0)   // the copies must land before the CTA's shared memory is released
+            for (int k = 0; k < min(TMA_STAGES, myn); ++k) mbar_wait_bounded(&bars[k], 0u);
+        return;
+    }
     double v0 = 0.0, v1 = 0.0;
     // Gathered operands: set 0 belongs to the chunk being computed, set j
     // to chunk k + j.  No row of a colour reads a value written by another
@@ -1069,6 +1092,8 @@ __global__ void k_fold(int ndof, double *x, double *d)
 __global__ void __launch_bounds__(1024) k_sor_check(const double *part, int nblk, SorCtl *ctl,
                                                     double tolerl)
 {
+    pdl_launch_dependents();
+    pdl_wait();   // every colour's partial sums are visible from here
     if (ctl->conv) return;
     double v[2] = {0.0, 0.0};
     for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
