@@ -21,6 +21,12 @@
 
 using namespace fasdev;
 
+// Quotients of the SOR point update from precomputed reciprocals (1) or by
+// division (0); both give the correctly rounded quotient.
+#ifndef FAS_SOR_RCP
+#define FAS_SOR_RCP 1
+#endif
+
 namespace {
 
 template <class T> struct DVec {
@@ -104,8 +110,10 @@ struct fas_handle {
     DVec<double> blk;
     DVec<float> blk32;           // FP32 copy for FAS_MODE_SOR_FP32
     DVec<double> sor_d, sor_r;   // correction and residual of the refinement
+    DVec<double> rdiag;          // reciprocals of the diagonal entries, row order
     int refine_every = 16;       // FP32 sweeps per FP64 residual
     cudaGraphExec_t sor_graph = nullptr;   // GRAPH_SWEEPS plain sweeps
+    cudaGraphExec_t sor32_graph = nullptr; // one refinement cycle of the FP32 form
     bool blk32_fresh = false;    // the last assembly wrote blk32
     // reductions and control
     std::vector<int> sor_boff, sor_nblk;
@@ -133,6 +141,7 @@ struct fas_handle {
     ~fas_handle()
     {
         if (sor_graph) cudaGraphExecDestroy(sor_graph);
+        if (sor32_graph) cudaGraphExecDestroy(sor32_graph);
         for (auto e : ev_pool) cudaEventDestroy(e);
         if (ev_t0) cudaEventDestroy(ev_t0);
         if (ev_t1) cudaEventDestroy(ev_t1);
@@ -367,6 +376,7 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
     }
     h->sor_nblk_tot = std::max(tot, 1);
     CKA(h->part_sor.alloc((size_t)2 * h->sor_nblk_tot));
+    if (FAS_SOR_RCP) CKA(h->rdiag.alloc((size_t)3 * nn));
     CKA(h->d_cstart.alloc(h->ncol + 1));
     CK(h->d_cstart.put(h->col_start.data(), h->ncol + 1, s));
     h->sor_small = nn <= SOR_SMALL_ROWS;
@@ -831,12 +841,13 @@ void launch_colour(fas_handle *h, int c, bool fp32)
     if (p1 <= p0) return;
     if (fp32)
         launch_pdl(k_sor_colour_tma<float>, h->sor_nblk[c], TMA_THREADS, tma_smem_bytes<float>(), h->stream,
-                   h->blk32.p, h->bcol.p, p0, p1, h->sor_r.p, h->sor_d.p, h->ddx.p, h->sorctl.p, h->part_sor.p,
-                   h->sor_boff[c], h->sor_nblk_tot);
+                   h->blk32.p, h->bcol.p, p0, p1, h->sor_r.p, h->sor_d.p, h->ddx.p, (const double *)nullptr,
+                   h->sorctl.p, h->part_sor.p, h->sor_boff[c], h->sor_nblk_tot);
     else
         launch_pdl(k_sor_colour_tma<double>, h->sor_nblk[c], TMA_THREADS, tma_smem_bytes<double>(), h->stream,
-                   h->blk.p, h->bcol.p, p0, p1, h->rhs.p, h->ddx.p, (const double *)nullptr, h->sorctl.p,
-                   h->part_sor.p, h->sor_boff[c], h->sor_nblk_tot);
+                   h->blk.p, h->bcol.p, p0, p1, h->rhs.p, h->ddx.p, (const double *)nullptr,
+                   (const double *)(FAS_SOR_RCP ? h->rdiag.p : nullptr), h->sorctl.p, h->part_sor.p,
+                   h->sor_boff[c], h->sor_nblk_tot);
 }
 
 void launch_check(fas_handle *h, double tolerl)
@@ -867,6 +878,36 @@ int ensure_sor_graph(fas_handle *h, const BlockDev &B, double tolerl)
     return 0;
 }
 
+// One refinement cycle of the FP32 form: refine_every FP32 sweeps on the
+// correction, the fold into the iterate and the FP64 residual.
+void launch_fp32_cycle(fas_handle *h, const BlockDev &B, double tolerl, int sweeps)
+{
+    const size_t nd3 = 3 * (size_t)h->nnod;
+    const unsigned rblk = (unsigned)std::min<long long>(nblocks(h->nnod, 8), (long long)h->nsm * 8);
+    for (int it = 0; it < sweeps; ++it) {
+        for (int c = 0; c < h->ncol; ++c) launch_colour(h, c, true);
+        launch_check(h, tolerl);
+    }
+    k_fold<<<nblocks((long long)nd3, 256), 256, 0, h->stream>>>((int)nd3, h->ddx.p, h->sor_d.p);
+    k_residual<<<rblk, 256, 0, h->stream>>>(B, h->rhs.p, h->ddx.p, h->sor_r.p, h->sorctl.p);
+}
+
+int ensure_fp32_graph(fas_handle *h, const BlockDev &B, double tolerl)
+{
+    if (h->sor32_graph) return 0;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    launch_fp32_cycle(h, B, tolerl, h->refine_every);
+    CK(cudaStreamEndCapture(h->stream, &g));
+    const cudaError_t e = cudaGraphInstantiate(&h->sor32_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        h->sor32_graph = nullptr;
+        return FAS_E_CUDA;
+    }
+    return 0;
+}
+
 // FACSLS: rhs <- ddx, ddx <- 0, multicolour SOR sweeps until the relative
 // change drops below toler^2 or 1000 sweeps (Stif_sol.f90:173-213).
 int facsls_impl(fas_handle *h, int *sweeps, double *error)
@@ -885,6 +926,10 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
     if (h->hc->ekey[1] != ~0ull) return 903;
     const double tolerl = h->C.toler * h->C.toler;
     const bool small = h->sor_small && !(h->mode & FAS_MODE_SOR_GRID);
+    if (!small && FAS_SOR_RCP) {
+        k_rdiag<<<nblocks(h->nnod, 256), 256, 0, s>>>(B, h->rdiag.p);
+        LAUNCHED(h);
+    }
     if (small) {
         Span sp(h, &h->P.ms_sor_colour);
         k_sor_small<<<1, 1024, 0, s>>>(B, h->d_cstart.p, h->ncol, h->rhs.p, h->ddx.p, h->sorctl.p, tolerl, 1000);
@@ -902,10 +947,17 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
         CK(cudaMemsetAsync(h->sor_d.p, 0, nd3 * sizeof(double), s));
         const int m = h->refine_every;
         const unsigned rblk = (unsigned)std::min<long long>(nblocks(h->nnod, 8), (long long)h->nsm * 8);
+        const bool graph32 = h->prof < 2 && ensure_fp32_graph(h, B, tolerl) == 0;
         int outer_per_chunk = 1;
         while (done < 1000) {
             for (int o = 0; o < outer_per_chunk && done < 1000; ++o) {
                 const int k = std::min(m, 1000 - done);
+                if (graph32 && k == m) {
+                    CK(cudaGraphLaunch(h->sor32_graph, s));
+                    h->launches += (int64_t)k * (h->ncol + 1) + 2;
+                    done += k;
+                    continue;
+                }
                 for (int it = 0; it < k; ++it) {
                     for (int c = 0; c < h->ncol; ++c) {
                         if (h->col_start[c + 1] <= h->col_start[c]) continue;
@@ -1426,8 +1478,8 @@ int facsls_noalloc_impl(fas_handle *h, int *sweeps, double *error)
                     const int p0 = h->col_start[c], p1 = h->col_start[c + 1];
                     if (p1 <= p0) continue;
                     k_sor_colour_tma<double><<<h->sor_nblk[c], TMA_THREADS, tma_smem_bytes<double>(), s>>>(
-                        h->blk.p, h->bcol.p, p0, p1, h->rhs.p, h->ddx.p, nullptr, ctl, part, h->sor_boff[c],
-                        h->sor_nblk_tot);
+                        h->blk.p, h->bcol.p, p0, p1, h->rhs.p, h->ddx.p, nullptr, nullptr, ctl, part,
+                        h->sor_boff[c], h->sor_nblk_tot);
                     LAUNCHED(h);
                 }
                 k_sor_check<<<1, 1024, 0, s>>>(part, h->sor_nblk_tot, ctl, tolerl);

@@ -757,15 +757,48 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
+// End of one sweep, by one whole block: error = sum(dx^2) / sum(x^2) over
+// the per-CTA partials of every colour (Stif_sol.f90:206-210).
+__device__ __forceinline__ void sweep_test(const double *part, int nblk, SorCtl *ctl, double tolerl)
+{
+    double v[2] = {0.0, 0.0};
+    for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
+        v[0] += part[i];
+        v[1] += part[nblk + i];
+    }
+    __shared__ double red[2][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        double t = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        if (lane == 0) red[k][wid] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        double a = 0.0, b = 0.0;
+        for (int i = 0; i < nw; ++i) {
+            a += red[0][i];
+            b += red[1][i];
+        }
+        const double err = a / b;
+        ctl->err = err;
+        ctl->sweeps += 1;
+        if (err < tolerl) ctl->conv = 1;
+    }
+}
+
 // Launch shape of the colour kernel (compile-time; -D overrides for tuning).
 #ifndef FAS_TMA_ROWS
 #define FAS_TMA_ROWS 8
 #endif
 #ifndef FAS_TMA_LPR
-#define FAS_TMA_LPR 8
+#define FAS_TMA_LPR 4
 #endif
 #ifndef FAS_TMA_STAGES
-#define FAS_TMA_STAGES 3
+#define FAS_TMA_STAGES 2
 #endif
 #ifndef FAS_TMA_PD
 #define FAS_TMA_PD 1
@@ -813,7 +846,8 @@ template <typename T>
 __global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restrict__ blk,
                                                                 const int *__restrict__ bcol, int p0, int p1,
                                                                 const double *__restrict__ rhs, double *sol,
-                                                                const double *__restrict__ base, SorCtl *ctl,
+                                                                const double *__restrict__ base,
+                                                                const double *__restrict__ rdiag, SorCtl *ctl,
                                                                 double *part, int boff, int nblk_tot)
 {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -867,9 +901,9 @@ __global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restr
     // row of the same colour, so the gathers of the next TMA_PD chunks are
     // in flight while chunk k is computed.
     double gx0[TMA_PD + 1][TMA_SPL] = {}, gx1[TMA_PD + 1][TMA_SPL] = {}, gx2[TMA_PD + 1][TMA_SPL] = {};
-    double gr[TMA_PD + 1][3] = {};
+    double gr[TMA_PD + 1][6] = {};   // right-hand side and reciprocal diagonal of the row's node
     auto gather = [&](int kk, double (&g0)[TMA_SPL], double (&g1)[TMA_SPL], double (&g2)[TMA_SPL],
-                      double (&grr)[3]) {
+                      double (&grr)[6]) {
         const int c = blockIdx.x + kk * gridDim.x;
         const int nrow = min(TMA_ROWS, p1 - (p0 + c * TMA_ROWS));
         const bool live = row < nrow;
@@ -889,6 +923,12 @@ __global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restr
         grr[0] = own ? ld_keep(rhs + 3 * n, keep_pol) : 0.0;
         grr[1] = own ? ld_keep(rhs + 3 * n + 1, keep_pol) : 0.0;
         grr[2] = own ? ld_keep(rhs + 3 * n + 2, keep_pol) : 0.0;
+        if (rdiag) {
+            const double *rd = rdiag + 3 * (size_t)(p0 + c * TMA_ROWS + row);
+            grr[3] = own ? rd[0] : 0.0;
+            grr[4] = own ? rd[1] : 0.0;
+            grr[5] = own ? rd[2] : 0.0;
+        }
     };
     // chunks [0, waited) have landed; chunks [0, min(myn, k + TMA_STAGES))
     // have been issued when iteration k starts
@@ -947,12 +987,33 @@ __global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restr
             for (int qq = 0; qq < 9; ++qq) D[qq] = (double)vals[qq * 27];
             const double o0 = gx0[0][0], o1 = gx1[0][0], o2 = gx2[0][0];
             double x0 = o0, x1 = o1, x2 = o2;
-            double t = (gr[0][0] - (a0 + D[1] * x1 + D[2] * x2)) / D[0];
-            x0 = x0 + 1.2 * (t - x0);
-            t = (gr[0][1] - (a1 + D[3] * x0 + D[5] * x2)) / D[4];
-            x1 = x1 + 1.2 * (t - x1);
-            t = (gr[0][2] - (a2 + D[6] * x0 + D[7] * x1)) / D[8];
-            x2 = x2 + 1.2 * (t - x2);
+            double t;
+            if (rdiag) {
+                // num / D from the correctly rounded reciprocal of D: with
+                // q0 = num * (1/D) and the exact remainder e = num - q0 * D
+                // (one FMA), q0 + e * (1/D) rounds to the correctly rounded
+                // quotient (Markstein, IBM J. Res. Dev. 34 (1990) 111-119).
+                const double i0 = gr[0][3], i1 = gr[0][4], i2 = gr[0][5];
+                double nm = gr[0][0] - (a0 + D[1] * x1 + D[2] * x2);
+                double q0 = nm * i0;
+                t = fma(fma(-q0, D[0], nm), i0, q0);
+                x0 = x0 + 1.2 * (t - x0);
+                nm = gr[0][1] - (a1 + D[3] * x0 + D[5] * x2);
+                q0 = nm * i1;
+                t = fma(fma(-q0, D[4], nm), i1, q0);
+                x1 = x1 + 1.2 * (t - x1);
+                nm = gr[0][2] - (a2 + D[6] * x0 + D[7] * x1);
+                q0 = nm * i2;
+                t = fma(fma(-q0, D[8], nm), i2, q0);
+                x2 = x2 + 1.2 * (t - x2);
+            } else {
+                t = (gr[0][0] - (a0 + D[1] * x1 + D[2] * x2)) / D[0];
+                x0 = x0 + 1.2 * (t - x0);
+                t = (gr[0][1] - (a1 + D[3] * x0 + D[5] * x2)) / D[4];
+                x1 = x1 + 1.2 * (t - x1);
+                t = (gr[0][2] - (a2 + D[6] * x0 + D[7] * x1)) / D[8];
+                x2 = x2 + 1.2 * (t - x2);
+            }
             sol[3 * n] = x0;
             sol[3 * n + 1] = x1;
             sol[3 * n + 2] = x2;
@@ -977,9 +1038,8 @@ __global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restr
                 gx1[i][j] = gx1[i + 1][j];
                 gx2[i][j] = gx2[i + 1][j];
             }
-            gr[i][0] = gr[i + 1][0];
-            gr[i][1] = gr[i + 1][1];
-            gr[i][2] = gr[i + 1][2];
+#pragma unroll
+            for (int j = 0; j < 6; ++j) gr[i][j] = gr[i + 1][j];
         }
     }
     (void)lane;
@@ -1095,33 +1155,17 @@ __global__ void __launch_bounds__(1024) k_sor_check(const double *part, int nblk
     pdl_launch_dependents();
     pdl_wait();   // every colour's partial sums are visible from here
     if (ctl->conv) return;
-    double v[2] = {0.0, 0.0};
-    for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
-        v[0] += part[i];
-        v[1] += part[nblk + i];
-    }
-    __shared__ double red[2][32];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    sweep_test(part, nblk, ctl, tolerl);
+}
+
+// Correctly rounded reciprocals of the three diagonal entries of every row
+// (row order), for the colour kernel's quotient.
+__global__ void k_rdiag(BlockDev B, double *rdiag)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= B.R) return;
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        double t = v[k];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-        if (lane == 0) red[k][wid] = t;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const int nw = (blockDim.x + 31) >> 5;
-        double a = 0.0, b = 0.0;
-        for (int i = 0; i < nw; ++i) {
-            a += red[0][i];
-            b += red[1][i];
-        }
-        const double err = a / b;
-        ctl->err = err;
-        ctl->sweeps += 1;
-        if (err < tolerl) ctl->conv = 1;
-    }
+    for (int c = 0; c < 3; ++c) rdiag[3 * (size_t)p + c] = 1.0 / B.blk[bidx(p, 0, 4 * c)];
 }
 
 // 903 test (Stif_sol.f90:183-185): first DOF whose diagonal entry is zero.
