@@ -119,16 +119,18 @@ def read(path: str, real_bytes: int = 4) -> tuple[Problem, int]:
     first = int(r.ints()[0])
     nlmnt, nnod, ngps, nsv = (int(v) for v in r.ints())
     le, lt, nd, npe = (np.zeros(nlmnt, np.int32) for _ in range(4))
-    ln = np.zeros((nlmnt, 8), np.int32)
-    lg = np.zeros((nlmnt, 1), np.int32)
+    lns, lgs = [], []
     for e in range(nlmnt):
         le[e], lt[e], nd[e], npe[e] = r.ints()
-        v = r.ints()
-        if nd[e] > 8:
-            raise ValueError("elements with more than 8 nodes are not supported")
-        ln[e, :nd[e]] = v
-        v = r.ints()
-        lg[e, :npe[e]] = v[:1] if npe[e] else 0
+        lns.append(r.ints()[:nd[e]])
+        lgs.append(r.ints()[:npe[e]])
+    if nlmnt and (nd.max() > 20 or npe.max() > 8):
+        raise ValueError("elements with more than 20 nodes or 8 Gauss points")
+    ln = np.zeros((nlmnt, max(int(nd.max()) if nlmnt else 1, 1)), np.int32)
+    lg = np.zeros((nlmnt, max(int(npe.max()) if nlmnt else 1, 1)), np.int32)
+    for e in range(nlmnt):
+        ln[e, :nd[e]] = lns[e]
+        lg[e, :npe[e]] = lgs[e]
     ib = np.zeros(nnod, np.int32)
     x = np.zeros(3 * nnod)
     dx = np.zeros(3 * nnod)

@@ -2,10 +2,11 @@
 
 The reference builds its input with the interactive pre-processor ``fs3pre``
 (src/prepro/fs3pre.f90) and writes a ``.fsd`` file.  This module produces the
-same tables directly, for 8-node one-Gauss-point bricks (``lt = 12``):
+same tables directly, for 8-node one-Gauss-point bricks (``lt = 12``) and
+20-node eight-Gauss-point bricks (``lt = 22``):
 
-* elements in (z, y, x) loop order with ADDEL_8NQ's local node order
-  (src/prepro/fs3pre.f90:183-233);
+* elements in (z, y, x) loop order with ADDEL_8NQ's or ADDEL_20NQ's local
+  node order (src/prepro/fs3pre.f90:183-291);
 * node numbers in first-occurrence order, which is what SWEEP's duplicate
   removal leaves (src/prepro/fs3p-swp.f90:53-109), computed with one sort
   instead of the O(nnod^2) sweep;
@@ -27,6 +28,12 @@ from .problem import Control, Problem
 # ADDEL_8NQ local node offsets (fs3pre.f90:193-196)
 BRICK8 = np.array([(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0),
                    (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)], dtype=np.int64)
+# ADDEL_20NQ local node offsets in half edges (fs3pre.f90:250-255): bottom
+# face corners and mid-sides anticlockwise from the origin, the four
+# vertical mid-edges, then the top face like the bottom one
+BRICK20_HALF = np.array([(0, 0, 0), (1, 0, 0), (2, 0, 0), (2, 1, 0), (2, 2, 0), (1, 2, 0), (0, 2, 0),
+                         (0, 1, 0), (0, 0, 1), (2, 0, 1), (2, 2, 1), (0, 2, 1), (0, 0, 2), (1, 0, 2),
+                         (2, 0, 2), (2, 1, 2), (2, 2, 2), (1, 2, 2), (0, 2, 2), (0, 1, 2)], dtype=np.int64)
 
 
 # ----------------------------------------------------------------- materials
@@ -269,36 +276,46 @@ def structured_cube(n=(8, 8, 8), lengths=(1.0, 1.0, 1.0), xfree: int = 3,
                     materials: list[dict] | None = None, fractions=None,
                     tau0: float | list[float] = 25.0, seed: int = 0,
                     twinlim: int = 0, twinprob: float = 0.0,
-                    ctrl: Control | None = None) -> Problem:
-    """An nx x ny x nz brick of 8-node bricks with fs3pre's numbering, boundary
+                    ctrl: Control | None = None, nodes: int = 8) -> Problem:
+    """An nx x ny x nz brick of bricks with fs3pre's numbering, boundary
     codes, loading and per-grain random orientations (see module docstring).
 
+    `nodes` = 8 gives ADDEL_8NQ's one-point bricks (``lt = 12``), 20 gives
+    ADDEL_20NQ's 20-node, 8-point bricks (``lt = 22``, fs3pre.f90:241-291).
     `grain` = edge of the cubic grains in elements.  With several materials,
     each grain draws its material from `fractions` (fs3p-matl.f90:33-57
     draws per element; here per grain so grains stay single-phase)."""
     nx, ny, nz = (int(v) for v in n)
+    if nodes not in (8, 20):
+        raise ValueError("nodes must be 8 or 20")
     materials = materials or [fcc_aluminium()]
     nel = nx * ny * nz
     dxl = np.array([lengths[0] / nx, lengths[1] / ny, lengths[2] / nz])
     iz, iy, ix = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
     ix, iy, iz = ix.ravel(), iy.ravel(), iz.ravel()          # element order: x fastest
-    gx = ix[:, None] + BRICK8[None, :, 0]
-    gy = iy[:, None] + BRICK8[None, :, 1]
-    gz = iz[:, None] + BRICK8[None, :, 2]
-    key = (gx + (nx + 1) * (gy + (ny + 1) * gz)).ravel()
+    # node positions on the lattice of half (20 nodes) or whole edges (8 nodes)
+    if nodes == 8:
+        off, h = BRICK8, 1
+    else:
+        off, h = BRICK20_HALF, 2
+    npg = 1 if nodes == 8 else 8
+    gx = h * ix[:, None] + off[None, :, 0]
+    gy = h * iy[:, None] + off[None, :, 1]
+    gz = h * iz[:, None] + off[None, :, 2]
+    key = (gx + (h * nx + 1) * (gy + (h * ny + 1) * gz)).ravel()
     uniq, first, inv = np.unique(key, return_index=True, return_inverse=True)
     order = np.argsort(first, kind="stable")
     rank = np.empty_like(order)
     rank[order] = np.arange(order.size)
-    ln = (rank[inv].reshape(nel, 8) + 1).astype(np.int32)
+    ln = (rank[inv].reshape(nel, nodes) + 1).astype(np.int32)
     nnod = uniq.size
     # coordinates from the first-occurrence element: x0 + delx * xyz
     fo = first[order]
-    fe, fa = fo // 8, fo % 8
+    fe, fa = fo // nodes, fo % nodes
     x0 = np.stack([dxl[0] * ix[fe], dxl[1] * iy[fe], dxl[2] * iz[fe]], axis=1)
-    xyz = x0 + dxl[None, :] * BRICK8[fa]
+    xyz = x0 + dxl[None, :] * (off[fa] / float(h))
     x = np.ascontiguousarray(xyz.reshape(-1))
-    tolerance = 0.5 * float(dxl.min())       # SETSWTOL: 0.5 * shortest distance
+    tolerance = 0.5 * float(dxl.min()) / h   # SETSWTOL: 0.5 * shortest intra-element distance
     ib = setbounds(x, tolerance, xfree)
 
     rng = np.random.default_rng(seed)
@@ -320,25 +337,28 @@ def structured_cube(n=(8, 8, 8), lengths=(1.0, 1.0, 1.0), xfree: int = 3,
     nss, e, ssang, ab, an, ampar, smatrx = pack_materials(materials)
     tiem, x_spec = setkinc(lengths, xfree, eps_inc, ninc)
     nsv = 3 + int(nss.max())
+    ngps = npg * nel
     prob = Problem(
-        nlmnt=nel, nnod=nnod, ngps=nel, le=le, lt=np.full(nel, 12, np.int32),
-        nd=np.full(nel, 8, np.int32), np_=np.ones(nel, np.int32), ln=ln,
-        lg=np.arange(1, nel + 1, dtype=np.int32).reshape(nel, 1), ib=ib,
+        nlmnt=nel, nnod=nnod, ngps=ngps, le=le, lt=np.full(nel, 12 if nodes == 8 else 22, np.int32),
+        nd=np.full(nel, nodes, np.int32), np_=np.full(nel, npg, np.int32), ln=ln,
+        lg=np.arange(1, ngps + 1, dtype=np.int32).reshape(nel, npg), ib=ib,
         nss=nss, e=e, ssang=ssang, ab=ab, an=an, ampar=ampar, smatrx=smatrx,
         nmpar=6, twinlim=twinlim, twinprob=twinprob, tiem=tiem, x_spec=x_spec,
         f_spec=np.zeros((ninc, abi.XSLD, 3)), nxs=50, nfs=0,
         ctrl=ctrl or Control(), nsv=nsv)
     prob.zero_state()
     prob.x[:] = x
-    prob.sv[:, 0:3] = euler[grain_id]
+    gp_grain = np.repeat(grain_id, npg)      # the element's GPs share its grain
+    prob.sv[:, 0:3] = euler[gp_grain]
     t0 = np.broadcast_to(np.asarray(tau0, float), (nm,))
+    gp_le = np.repeat(le, npg)
     for k in range(nm):
-        sel = le == k + 1
+        sel = gp_le == k + 1
         if "tau0" in materials[k]:
             prob.sv[sel, 3:3 + nss[k]] = np.asarray(materials[k]["tau0"], float)[None, :]
         else:
             prob.sv[sel, 3:3 + nss[k]] = t0[k]
-    prob.meta.update(dict(n=(nx, ny, nz), lengths=tuple(lengths), xfree=xfree, grain=grain,
+    prob.meta.update(dict(n=(nx, ny, nz), lengths=tuple(lengths), xfree=xfree, grain=grain, nodes=nodes,
                           seed=seed, grain_id=grain_id.astype(np.int32),
                           materials=[m["name"] for m in materials]))
     return prob

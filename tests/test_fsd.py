@@ -26,6 +26,18 @@ def test_roundtrip_real8(tmp_path):
     assert q.twinlim == p.twinlim and q.twinprob == p.twinprob
 
 
+def test_roundtrip_20_node_bricks(tmp_path):
+    """20-node, 8-Gauss-point bricks (the element type of the reference's
+    sample input) keep their 20 node and 8 GP ids per element."""
+    p = generator.structured_cube(n=(2, 1, 2), ninc=2, nodes=20)
+    path = str(tmp_path / "b.fsd")
+    fsd.write(path, p, real_bytes=8)
+    q, _ = fsd.read(path, real_bytes=8)
+    for k in _fields(p):
+        np.testing.assert_array_equal(getattr(q, k), getattr(p, k), err_msg=k)
+    assert q.ln.shape == (p.nlmnt, 20) and q.lg.shape == (p.nlmnt, 8)
+
+
 def test_roundtrip_real4_rounds_to_float32(tmp_path):
     p = generator.structured_cube(n=(2, 1, 1), ninc=2)
     path = str(tmp_path / "a.fsd")

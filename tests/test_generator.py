@@ -6,23 +6,28 @@ import pytest
 from cpfem_code_b200 import generator
 
 
-def _addel_sweep(nx, ny, nz, dxl):
-    """ADDEL_8NQ (fs3pre.f90:183-233) then SWEEP (fs3p-swp.f90:53-109),
-    literally: append 8 nodes per element, then remove every node that lies
-    within the tolerance of an earlier one, renumbering the topology."""
+def _addel_sweep(nx, ny, nz, dxl, nodes=8):
+    """ADDEL_8NQ / ADDEL_20NQ (fs3pre.f90:183-291) then SWEEP
+    (fs3p-swp.f90:53-109), literally: append the element's nodes, then remove
+    every node that lies within the tolerance of an earlier one, renumbering
+    the topology.  The tolerance is SETSWTOL's half of the shortest
+    intra-element distance (fs3p-swp.f90:7-45)."""
+    local = generator.BRICK8 if nodes == 8 else generator.BRICK20_HALF / 2.0
     xs, ln = [], []
     for iz in range(nz):
         for iy in range(ny):
             for ix in range(nx):
                 x0 = np.array([dxl[0] * ix, dxl[1] * iy, dxl[2] * iz])
                 el = []
-                for off in generator.BRICK8:
+                for off in local:
                     xs.append(x0 + dxl * off)
                     el.append(len(xs))
                 ln.append(el)
     x = np.array(xs)
     ln = np.array(ln)
-    tol = 0.5 * dxl.min()
+    e0 = x[ln[0] - 1]
+    d2 = ((e0[:, None, :] - e0[None, :, :]) ** 2).sum(-1)
+    tol = 0.5 * np.sqrt(d2[np.triu_indices(len(local), 1)].min())
     i_test = 1
     while i_test < len(x):
         i_test += 1
@@ -37,6 +42,20 @@ def _addel_sweep(nx, ny, nz, dxl):
             ln = np.where(ln > i_test, ln - 1, ln)
             i_test -= 1
     return x.reshape(-1), ln
+
+
+@pytest.mark.parametrize("n", [(1, 1, 1), (2, 2, 2), (2, 1, 3)])
+def test_numbering_matches_sweep_20_node(n):
+    p = generator.structured_cube(n=n, lengths=(1.0, 2.0, 0.5), ninc=1, nodes=20)
+    dxl = np.array([1.0 / n[0], 2.0 / n[1], 0.5 / n[2]])
+    x, ln = _addel_sweep(*n, dxl, nodes=20)
+    assert p.nnod == len(x) // 3
+    np.testing.assert_array_equal(p.ln, ln)
+    np.testing.assert_allclose(p.x, x, rtol=0, atol=1e-15)
+    assert (p.lt == 22).all() and (p.nd == 20).all() and (p.np_ == 8).all()
+    # ADDEL_20NQ's GP numbering: 8 * element - 8 + i
+    np.testing.assert_array_equal(p.lg.ravel(), np.arange(1, 8 * p.nlmnt + 1))
+    assert p.ngps == 8 * p.nlmnt
 
 
 @pytest.mark.parametrize("n", [(1, 1, 1), (2, 2, 2), (3, 2, 1), (2, 3, 4)])
