@@ -270,6 +270,82 @@ template <class R> R shape12(const R xn[8][3], R dndx[8][3])
     return R(8.0) * w;
 }
 
+// SHAPE_22, src/fasolt/Shapef.f90:210-342: 20-node brick, 8 Gauss points at
+// (+-1/sqrt3)^3, GPs 1-4 anticlockwise from node 1 at zeta = -1/sqrt3, 5-8
+// above them.  The reference tabulates the local derivatives of the
+// serendipity functions at its GPs to 6 decimals; shape22_table() evaluates
+// the same functions at the GP coordinate 0.57735 and rounds them to 6
+// decimals, which reproduces all 480 entries of that table (with the exact
+// 1/sqrt3, 24 entries would differ in the last digit).  Local node
+// positions follow ADDEL_20NQ's order (corners 1,3,5,7
+// and mid-sides 2,4,6,8 at zeta = -1, vertical mid-edges 9-12, the top
+// face 13-20 like the bottom one).
+struct Shape22Table {
+    double dn[8][3][20];   // dn[g][j][i] = dndn(j+1, i+1, g+1)
+};
+inline const Shape22Table &shape22_table()
+{
+    static const Shape22Table t = [] {
+        static const int loc[20][3] = {{-1, -1, -1}, {0, -1, -1}, {1, -1, -1}, {1, 0, -1}, {1, 1, -1},
+                                       {0, 1, -1},   {-1, 1, -1}, {-1, 0, -1}, {-1, -1, 0}, {1, -1, 0},
+                                       {1, 1, 0},    {-1, 1, 0},  {-1, -1, 1}, {0, -1, 1},  {1, -1, 1},
+                                       {1, 0, 1},    {1, 1, 1},   {0, 1, 1},   {-1, 1, 1},  {-1, 0, 1}};
+        static const int gsign[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                                        {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+        const double a = 0.57735;
+        Shape22Table t{};
+        for (int g = 0; g < 8; ++g) {
+            const double q[3] = {gsign[g][0] * a, gsign[g][1] * a, gsign[g][2] * a};
+            for (int i = 0; i < 20; ++i) {
+                const int *c = loc[i];
+                double d[3];
+                if (c[0] && c[1] && c[2]) {   // corner
+                    const double f[3] = {1 + q[0] * c[0], 1 + q[1] * c[1], 1 + q[2] * c[2]};
+                    const double sum = q[0] * c[0] + q[1] * c[1] + q[2] * c[2] - 2;
+                    for (int j = 0; j < 3; ++j) {
+                        const int j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+                        d[j] = 0.125 * c[j] * f[j1] * f[j2] * (sum + f[j]);
+                    }
+                } else {                       // mid-edge: the zero coordinate is the edge's
+                    const int z = !c[0] ? 0 : (!c[1] ? 1 : 2);
+                    const int z1 = (z + 1) % 3, z2 = (z + 2) % 3;
+                    const double f1 = 1 + q[z1] * c[z1], f2 = 1 + q[z2] * c[z2], e = 1 - q[z] * q[z];
+                    d[z] = 0.25 * (-2 * q[z]) * f1 * f2;
+                    d[z1] = 0.25 * e * c[z1] * f2;
+                    d[z2] = 0.25 * e * f1 * c[z2];
+                }
+                for (int j = 0; j < 3; ++j) t.dn[g][j][i] = std::round(d[j] * 1e6) / 1e6;
+            }
+        }
+        return t;
+    }();
+    return t;
+}
+
+// xn[i][k] = xnode(k+1,i+1); dndx[i][k] = dndx(k+1,i+1); g is 0-based.
+template <class R> R shape22(int g, const R xn[20][3], R dndx[20][3])
+{
+    const Shape22Table &t = shape22_table();
+    R dn[3][20];
+    for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 20; ++i) dn[j][i] = (R)t.dn[g][j][i];
+    R jac[3][3];
+    for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 3; ++j) {
+            R s = 0;
+            for (int i = 0; i < 20; ++i) s = s + dn[j][i] * xn[i][k];
+            jac[j][k] = s;
+        }
+    R w = invert3(jac);
+    for (int i = 0; i < 20; ++i)
+        for (int k = 0; k < 3; ++k) {
+            R s = 0;
+            for (int j = 0; j < 3; ++j) s = s + jac[k][j] * dn[j][i];
+            dndx[i][k] = s;
+        }
+    return R(1.0) * w;
+}
+
 // ================================================================ constitutive
 // Per-GP working set: the FAS_CPL module scratch (fas-com-mod.f90:62-66),
 // made private to one Gauss-point update.
@@ -848,14 +924,14 @@ template <class R> int elvals(Problem<R> &P, int inc, int nit)
     P.sumcpiter = 0;
     const int NE = P.nlmnt;
     const int CH = 2048;
-    std::vector<R> esm_buf((size_t)CH * 576), fl_buf((size_t)CH * 24);
+    std::vector<R> esm_buf((size_t)CH * 3600), fl_buf((size_t)CH * 60);
     std::vector<int> rc_buf(CH);
     for (int e0 = 0; e0 < NE; e0 += CH) {
         const int e1 = std::min(NE, e0 + CH);
 #pragma omp parallel for schedule(dynamic, 16) num_threads(P.nthreads) if (P.nthreads > 1)
         for (int e = e0; e < e1; ++e) {
-            R *esm = &esm_buf[(size_t)(e - e0) * 576];
-            R *fl = &fl_buf[(size_t)(e - e0) * 24];
+            R *esm = &esm_buf[(size_t)(e - e0) * 3600];
+            R *fl = &fl_buf[(size_t)(e - e0) * 60];
             rc_buf[e - e0] = 0;
             const int iel = P.le[e], itp = P.lt[e], nn = P.nd[e];
             const int n3 = 3 * nn;
@@ -884,51 +960,56 @@ template <class R> int elvals(Problem<R> &P, int inc, int nit)
                 }
                 continue;
             }
-            // lt == 12 only (one Gauss point); checked at create
-            R sfd[8][3];
-            R weight = shape12(xl, sfd);
-            if (weight < R(1.e-7)) { rc_buf[e - e0] = 920; continue; }
-            const int j = P.lg[e * 1];
-            R del[6], r[3], defl;
-            int rc = dstrns(P, 8, sfd, dxl, del, r, defl);
-            if (rc) { rc_buf[e - e0] = rc; continue; }
-            R stl[6], dsl[6], s[6], d[6][6];
-            for (int k = 0; k < 6; ++k) {
-                stl[k] = P.st[(size_t)j * 6 + k];
-                dsl[k] = P.ds[(size_t)j * 6 + k];
-            }
-            rc = dstrss(P, iel, j, defl, del, stl, dsl, s, r, d, inc, nit);
-            if (rc) { rc_buf[e - e0] = rc; continue; }
-            P.dep[j] = defl;
-            for (int k = 0; k < 6; ++k) {
-                P.de[(size_t)j * 6 + k] = del[k];
-                P.ds[(size_t)j * 6 + k] = dsl[k];
-            }
-            for (int k = 0; k < 3; ++k) P.dr[(size_t)j * 3 + k] = r[k];
-            R *chi = &P.chi_gp[(size_t)j * 36];
-            for (int a = 0; a < 6; ++a)
-                for (int b = 0; b < 6; ++b) chi[a + 6 * b] = d[a][b];
-            for (int i = 0; i < 8; ++i) {
-                fl[3 * i + 0] = fl[3 * i + 0] + weight * (s[0] * sfd[i][0] + s[5] * sfd[i][1] + s[4] * sfd[i][2]);
-                fl[3 * i + 1] = fl[3 * i + 1] + weight * (s[1] * sfd[i][1] + s[3] * sfd[i][2] + s[5] * sfd[i][0]);
-                fl[3 * i + 2] = fl[3 * i + 2] + weight * (s[2] * sfd[i][2] + s[4] * sfd[i][0] + s[3] * sfd[i][1]);
-            }
-            for (int i = 0; i < 8; ++i)
-                for (int jn = 0; jn < 8; ++jn) {
-                    R gm[3][3];
-                    gaussm_block(sfd[i], sfd[jn], d, s, gm);
-                    for (int a = 0; a < 3; ++a)
-                        for (int b = 0; b < 3; ++b)
-                            esm[(3 * i + a) * n3 + 3 * jn + b] =
-                                esm[(3 * i + a) * n3 + 3 * jn + b] + weight * gm[a][b];
+            // lt == 12 (one GP) or 22 (eight GPs); checked at create.  The GP
+            // loop of Elvals.f90:82-236: forces and stiffness accumulate GP by GP.
+            const int ng = P.np[e];
+            for (int ig = 0; ig < ng; ++ig) {
+                R sfd[20][3];
+                R weight = itp == 12 ? shape12(reinterpret_cast<const R(*)[3]>(xl), reinterpret_cast<R(*)[3]>(sfd))
+                                     : shape22(ig, xl, sfd);
+                if (weight < R(1.e-7)) { rc_buf[e - e0] = 920; break; }
+                const int j = P.lg[(size_t)e * 8 + ig];
+                R del[6], r[3], defl;
+                int rc = dstrns(P, nn, sfd, dxl, del, r, defl);
+                if (rc) { rc_buf[e - e0] = rc; break; }
+                R stl[6], dsl[6], s[6], d[6][6];
+                for (int k = 0; k < 6; ++k) {
+                    stl[k] = P.st[(size_t)j * 6 + k];
+                    dsl[k] = P.ds[(size_t)j * 6 + k];
                 }
+                rc = dstrss(P, iel, j, defl, del, stl, dsl, s, r, d, inc, nit);
+                if (rc) { rc_buf[e - e0] = rc; break; }
+                P.dep[j] = defl;
+                for (int k = 0; k < 6; ++k) {
+                    P.de[(size_t)j * 6 + k] = del[k];
+                    P.ds[(size_t)j * 6 + k] = dsl[k];
+                }
+                for (int k = 0; k < 3; ++k) P.dr[(size_t)j * 3 + k] = r[k];
+                R *chi = &P.chi_gp[(size_t)j * 36];
+                for (int a2 = 0; a2 < 6; ++a2)
+                    for (int b2 = 0; b2 < 6; ++b2) chi[a2 + 6 * b2] = d[a2][b2];
+                for (int i = 0; i < nn; ++i) {
+                    fl[3 * i + 0] = fl[3 * i + 0] + weight * (s[0] * sfd[i][0] + s[5] * sfd[i][1] + s[4] * sfd[i][2]);
+                    fl[3 * i + 1] = fl[3 * i + 1] + weight * (s[1] * sfd[i][1] + s[3] * sfd[i][2] + s[5] * sfd[i][0]);
+                    fl[3 * i + 2] = fl[3 * i + 2] + weight * (s[2] * sfd[i][2] + s[4] * sfd[i][0] + s[3] * sfd[i][1]);
+                }
+                for (int i = 0; i < nn; ++i)
+                    for (int jn = 0; jn < nn; ++jn) {
+                        R gm[3][3];
+                        gaussm_block(sfd[i], sfd[jn], d, s, gm);
+                        for (int a2 = 0; a2 < 3; ++a2)
+                            for (int b2 = 0; b2 < 3; ++b2)
+                                esm[(3 * i + a2) * n3 + 3 * jn + b2] =
+                                    esm[(3 * i + a2) * n3 + 3 * jn + b2] + weight * gm[a2][b2];
+                    }
+            }
         }
         // serial scatter in element order; the first error (in element order)
         // stops the pass like FAFERR's STOP
         for (int e = e0; e < e1; ++e) {
             if (rc_buf[e - e0]) return rc_buf[e - e0];
-            const R *esm = &esm_buf[(size_t)(e - e0) * 576];
-            const R *fl = &fl_buf[(size_t)(e - e0) * 24];
+            const R *esm = &esm_buf[(size_t)(e - e0) * 3600];
+            const R *fl = &fl_buf[(size_t)(e - e0) * 60];
             const int nn = P.nd[e], n3 = 3 * nn;
             int in2[60];
             for (int i = 0; i < nn; ++i)
@@ -946,7 +1027,8 @@ template <class R> int elvals(Problem<R> &P, int inc, int nit)
                 for (int c = 0; c < 3; ++c) P.fc[k + c] = P.fc[k + c] + fl[3 * i + c];
             }
             if (P.lt[e] >= 9) {
-                P.sumcpiter = P.sumcpiter + P.erepmd_gp[P.lg[e]];
+                for (int ig = 0; ig < P.np[e]; ++ig)
+                    P.sumcpiter = P.sumcpiter + P.erepmd_gp[P.lg[(size_t)e * 8 + ig]];
                 P.last_mat = std::abs(P.le[e]);
             }
         }
@@ -1258,19 +1340,21 @@ int create(Problem<R> &P, const fas_mesh_desc *M, const fas_matl_desc *T, const 
         P.nd.assign(M->nd, M->nd + P.nlmnt);
         P.np.assign(M->np, M->np + P.nlmnt);
         P.ln.assign((size_t)P.nlmnt * P.ldn, 0);
-        P.lg.assign(P.nlmnt, 0);
+        P.lg.assign((size_t)P.nlmnt * 8, 0);
         for (int e = 0; e < P.nlmnt; ++e) {
-            if (!(P.lt[e] == 12 || P.lt[e] < 9)) return FAS_E_ELTYPE;
+            if (!(P.lt[e] == 12 || P.lt[e] == 22 || P.lt[e] < 9)) return FAS_E_ELTYPE;
             if (P.lt[e] == 12 && (P.nd[e] != 8 || P.np[e] != 1)) return FAS_E_ARG;
+            if (P.lt[e] == 22 && (P.nd[e] != 20 || P.np[e] != 8 || M->ld_lg < 8)) return FAS_E_ARG;
             for (int i = 0; i < P.nd[e]; ++i) {
                 int id = M->ln[(size_t)e * M->ld_ln + i];
                 if (id < 1 || id > P.nnod) return FAS_E_ARG;
                 P.ln[(size_t)e * P.ldn + i] = id - 1;
             }
-            if (P.np[e] > 0) {
-                int g = M->lg[(size_t)e * M->ld_lg];
+            if (P.np[e] < 0 || P.np[e] > 8) return FAS_E_ARG;
+            for (int ig = 0; ig < P.np[e]; ++ig) {
+                int g = M->lg[(size_t)e * M->ld_lg + ig];
                 if (g < 1 || g > P.ngps) return FAS_E_ARG;
-                P.lg[e] = g - 1;
+                P.lg[(size_t)e * 8 + ig] = g - 1;
                 P.gp_iel[g - 1] = P.le[e];
             }
         }
@@ -1719,6 +1803,24 @@ double ora_shape12(const double *x38, double *d38)
     for (int i = 0; i < 8; ++i)
         for (int k = 0; k < 3; ++k) d38[k + 3 * i] = dn[i][k];
     return w;
+}
+double ora_shape22(int g, const double *x320, double *d320)
+{
+    if (g < 0 || g > 7) return 0.0;
+    double xn[20][3], dn[20][3];
+    for (int i = 0; i < 20; ++i)
+        for (int k = 0; k < 3; ++k) xn[i][k] = x320[k + 3 * i];
+    double w = shape22<double>(g, xn, dn);
+    for (int i = 0; i < 20; ++i)
+        for (int k = 0; k < 3; ++k) d320[k + 3 * i] = dn[i][k];
+    return w;
+}
+void ora_shape22_table(double *dn)
+{
+    const Shape22Table &t = shape22_table();
+    for (int g = 0; g < 8; ++g)
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 20; ++i) dn[(g * 3 + j) * 20 + i] = t.dn[g][j][i];
 }
 
 }  // extern "C"

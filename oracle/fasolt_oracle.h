@@ -72,6 +72,10 @@ void    ora_ctmatrx(double ph1, double phi, double ph2, double *a9_colmajor,
 void    ora_elastc(const double *e9, const double *euler3, double *s36_colmajor);
 void    ora_tens_rot(const double *r3, const double *a6, double *b6);
 double  ora_shape12(const double *xnode_3x8_colmajor, double *dndx_3x8_colmajor);
+/* SHAPE_22 at Gauss point g (0-based) and its local-derivative table
+ * dn[(g*3 + j)*20 + i] = dndn(j+1, i+1, g+1). */
+double  ora_shape22(int g, const double *xnode_3x20_colmajor, double *dndx_3x20_colmajor);
+void    ora_shape22_table(double *dn_8x3x20);
 
 #ifdef __cplusplus
 }

@@ -50,7 +50,9 @@ def _load() -> C.CDLL:
                 ("ora_ctmatrx", [C.c_double] * 3 + [C.POINTER(C.c_double)] * 2, None),
                 ("ora_elastc", [C.POINTER(C.c_double)] * 3, None),
                 ("ora_tens_rot", [C.POINTER(C.c_double)] * 3, None),
-                ("ora_shape12", [C.POINTER(C.c_double)] * 2, C.c_double)):
+                ("ora_shape12", [C.POINTER(C.c_double)] * 2, C.c_double),
+                ("ora_shape22", [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_double),
+                ("ora_shape22_table", [C.POINTER(C.c_double)], None)):
             f = getattr(lib, name)
             f.argtypes, f.restype = args, res
         _lib = lib

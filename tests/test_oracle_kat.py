@@ -179,6 +179,41 @@ def test_shape12_patch(oracle_lib):
     np.testing.assert_allclose(grad, G.T, rtol=1e-12, atol=1e-13)
 
 
+def test_shape22_table(oracle_lib):
+    # SHAPE_22's tabulated local derivatives: serendipity functions at the
+    # GP coordinate 0.57735, rounded to 6 decimals.  Spot values of the
+    # reference table (Shapef.f90:259-264): dndn(1,1,1), dndn(1,2,1),
+    # dndn(2,1,1), dndn(3,9,1).
+    t = np.zeros(480)
+    oracle_lib.ora_shape22_table(t.ctypes.data_as(D))
+    dn = t.reshape(8, 3, 20)                       # [gp][local coord][node]
+    assert dn[0, 0, 0] == -0.407229
+    assert dn[0, 0, 1] == 0.718233
+    assert dn[0, 1, 0] == -0.407229
+    assert dn[0, 2, 8] == 0.718233
+    # every table entry has 6 decimals; each GP's derivatives sum to ~0
+    np.testing.assert_allclose(np.round(t * 1e6), t * 1e6, atol=1e-6)
+    np.testing.assert_allclose(dn.sum(axis=2), 0.0, atol=5e-6)
+
+
+@pytest.mark.parametrize("g", range(8))
+def test_shape22_patch(oracle_lib, g):
+    # SHAPE_22 on an affinely distorted 20-node brick: a linear displacement
+    # field gives its gradient and the eight weights add up to the volume,
+    # to the 6-decimal precision of the tabulated derivatives
+    rng = np.random.default_rng(5)
+    xi = generator.BRICK20_HALF.astype(float) / 2.0
+    F = np.eye(3) + 0.2 * rng.standard_normal((3, 3))
+    x = (xi - 0.5) @ F.T * 0.7 + 1.3
+    dn = np.zeros(60)
+    w = oracle_lib.ora_shape22(g, dp(x.reshape(-1)), dn.ctypes.data_as(D))
+    dndx = dn.reshape(20, 3)
+    assert w == pytest.approx(abs(np.linalg.det(F)) * 0.7 ** 3 / 8.0, rel=2e-5)
+    G = rng.standard_normal((3, 3))
+    grad = dndx.T @ (x @ G.T)
+    np.testing.assert_allclose(grad, G.T, rtol=0, atol=2e-5 * np.abs(G).max())
+
+
 def _point_problem(n, toler=1e-3, iel=1, seed=4, h0=150.0):
     from cpfem_code_b200.problem import Control
     mat = generator.fcc_aluminium(h0=h0)
@@ -259,3 +294,22 @@ def test_lattice_strain_is_compliance_times_stress(oracle_lib):
     e = o.lattice_strain()
     S = generator.rotated_compliance(mat["e"], p.sv[:, :3])
     np.testing.assert_allclose(e, np.einsum("nij,nj->ni", S, p.st), rtol=1e-13, atol=1e-20)
+
+
+def test_20_node_brick_increment_matches_8_node():
+    # One grain, one element, uniaxial tension: the field is close to
+    # homogeneous, which both bricks represent, so the 20-node, 8-GP brick
+    # (SHAPE_22) and the 8-node, 1-GP brick (SHAPE_12) give nearly the same
+    # mean stress; the 20-node Newton loop converges like the 8-node one
+    from oracle import OracleSolver
+    out = {}
+    for nodes in (8, 20):
+        p = generator.structured_cube(n=(1, 1, 1), nodes=nodes, ninc=2, seed=3)
+        o = OracleSolver(p, 8, threads=2)
+        for inc in (1, 2):
+            rep, _ = o.increment(inc)
+            assert len(rep) < p.ctrl.maxit and rep[-1]["sdx"] < p.ctrl.toler
+        o.download()
+        out[nodes] = p.st[:, 0].mean()
+        assert np.isfinite(p.st).all()
+    assert out[20] == pytest.approx(out[8], rel=2e-3)
