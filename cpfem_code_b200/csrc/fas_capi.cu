@@ -79,6 +79,8 @@ struct fas_handle {
     cudaStream_t stream = nullptr;
     uint32_t mode = 0;
     int nlmnt = 0, nnod = 0, ngps = 0;
+    int nn = 8, npg = 1;         // nodes and Gauss points per element (8, 1 or 20, 8)
+    int slots = SLOTS;           // block slots per row (27 or 81)
     int maxns = 0, nsvld = 0, nsv = 0, ns_tmpl = 12;
     bool point_mode = false, have_state = false;
     int last_mat = 1;            // mat_code the last element leaves behind
@@ -106,7 +108,8 @@ struct fas_handle {
     std::vector<int> col_start;
     std::vector<double> col_bytes, col_bytes32;   // algorithmic bytes per colour launch
     DVec<int> perm, rowof, nslot, bcol;
-    DVec<unsigned> bloc;
+    DVec<unsigned long long> bloc;
+    DVec<double> dn22;           // SHAPE_22's local-derivative table
     DVec<double> blk;
     DVec<float> blk32;           // FP32 copy for FAS_MODE_SOR_FP32
     DVec<double> sor_d, sor_r;   // correction and residual of the refinement
@@ -163,14 +166,16 @@ struct fas_handle {
     MeshDev mesh()
     {
         MeshDev m;
-        m.nlmnt = nlmnt; m.nnod = nnod; m.ln = ln.p; m.gpe = gpe.p; m.le = le.p; m.ib = ib.p;
+        m.nlmnt = nlmnt; m.nnod = nnod; m.nn = nn; m.npg = npg;
+        m.ln = ln.p; m.gpe = gpe.p; m.le = le.p; m.ib = ib.p;
         m.ne_elem = ne_elem.p; m.ne_loc = ne_loc.p; m.ne_cnt = ne_cnt.p;
         return m;
     }
     BlockDev block()
     {
         BlockDev b;
-        b.R = nnod; b.perm = perm.p; b.nslot = nslot.p; b.bcol = bcol.p; b.bloc = bloc.p; b.blk = blk.p;
+        b.R = nnod; b.slots = slots; b.brow = brow_of(slots); b.crow = crow_of(slots);
+        b.perm = perm.p; b.nslot = nslot.p; b.bcol = bcol.p; b.bloc = bloc.p; b.blk = blk.p;
         b.blk32 = (mode & FAS_MODE_SOR_FP32) ? blk32.p : nullptr;
         return b;
     }
@@ -267,8 +272,8 @@ int greedy_colouring(fas_handle *h, const std::vector<double> &xyz)
     for (int n : order) {
         for (int k = h->ne_ptr[n]; k < h->ne_ptr[n + 1]; ++k) {
             const int e = h->ne_list[k];
-            for (int a = 0; a < 8; ++a) {
-                const int c = h->h_colour[h->h_ln[(size_t)e * 8 + a]];
+            for (int a = 0; a < h->nn; ++a) {
+                const int c = h->h_colour[h->h_ln[(size_t)e * h->nn + a]];
                 if (c >= 0) {
                     if (c >= (int)used.size()) used.resize(c + 1, -1);
                     used[c] = n;
@@ -299,38 +304,49 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
     for (int p = 0; p < nn; ++p) h->col_start[h->h_colour[perm[p]] + 1] = p + 1;
     for (int c = 1; c <= h->ncol; ++c) h->col_start[c] = std::max(h->col_start[c], h->col_start[c - 1]);
 
-    std::vector<int> nslot(nn), bcol((size_t)CROW * nn, 0);
-    std::vector<unsigned> bloc((size_t)CROW * nn, 0xFFFFFFFFu);
+    // block neighbourhood of every row: the node itself, then the nodes it
+    // shares an element with, ascending
+    const int NN = h->nn;
+    std::vector<std::vector<int>> nbs(nn);
+    int maxs = 0;
     for (int p = 0; p < nn; ++p) {
         const int n = perm[p];
-        int nb[SLOTS];
-        int cnt = 0;
-        nb[cnt++] = n;
         std::vector<int> others;
         for (int k = h->ne_ptr[n]; k < h->ne_ptr[n + 1]; ++k) {
             const int e = h->ne_list[k];
-            for (int a = 0; a < 8; ++a) {
-                const int m = h->h_ln[(size_t)e * 8 + a];
+            for (int a = 0; a < NN; ++a) {
+                const int m = h->h_ln[(size_t)e * NN + a];
                 if (m != n && std::find(others.begin(), others.end(), m) == others.end()) others.push_back(m);
             }
         }
         std::sort(others.begin(), others.end());
-        if ((int)others.size() + 1 > SLOTS) return FAS_E_RANGE;
-        for (int m : others) nb[cnt++] = m;
+        nbs[p].reserve(others.size() + 1);
+        nbs[p].push_back(n);
+        nbs[p].insert(nbs[p].end(), others.begin(), others.end());
+        maxs = std::max(maxs, (int)nbs[p].size());
+    }
+    if (maxs > SLOTS20) return FAS_E_RANGE;
+    h->slots = maxs <= SLOTS ? SLOTS : SLOTS20;
+    const int crow = crow_of(h->slots), brow = brow_of(h->slots);
+    std::vector<int> nslot(nn), bcol((size_t)crow * nn, 0);
+    std::vector<unsigned long long> bloc((size_t)crow * nn, ~0ull);
+    for (int p = 0; p < nn; ++p) {
+        const int n = perm[p];
+        const int cnt = (int)nbs[p].size();
         nslot[p] = cnt;
-        bcol[sidx(p, CROW - 1)] = cnt;   // the pad slot carries the slot count
+        bcol[(size_t)p * crow + h->slots] = cnt;   // the pad slot carries the slot count
         for (int s = 0; s < cnt; ++s) {
-            bcol[sidx(p, s)] = nb[s];
-            unsigned word = 0xFFFFFFFFu;
+            bcol[(size_t)p * crow + s] = nbs[p][s];
+            unsigned long long word = ~0ull;
             int k = 0;
             for (int q = h->ne_ptr[n]; q < h->ne_ptr[n + 1]; ++q, ++k) {
                 const int e = h->ne_list[q];
-                unsigned b = 0xF;
-                for (int a = 0; a < 8; ++a)
-                    if (h->h_ln[(size_t)e * 8 + a] == nb[s]) { b = (unsigned)a; break; }
-                word = (word & ~(0xFu << (4 * k))) | (b << (4 * k));
+                unsigned long long b = 0xFF;
+                for (int a = 0; a < NN; ++a)
+                    if (h->h_ln[(size_t)e * NN + a] == nbs[p][s]) { b = (unsigned long long)a; break; }
+                word = (word & ~(0xFFull << (8 * k))) | (b << (8 * k));
             }
-            bloc[sidx(p, s)] = word;
+            bloc[(size_t)p * crow + s] = word;
         }
     }
     // algorithmic bytes of one colour launch: blocks and column ids of the
@@ -342,19 +358,19 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
             h->col_bytes[c] += nslot[p] * (72.0 + 4.0) + 8.0 + 72.0;
             h->col_bytes32[c] += nslot[p] * (36.0 + 4.0) + 8.0 + 72.0 + 24.0;
         }
-    // algorithmic bytes of one assembly launch: each element record read
-    // once (52 used doubles), each block written once, the slot tables and
-    // node adjacency read once, fc and ddx written
-    double ab = (double)h->nlmnt * 52.0 * 8.0 + (double)nn * (48.0 + 8.0 + 12.0 * MAXADJ);
-    for (int p = 0; p < nn; ++p) ab += nslot[p] * (72.0 + 8.0);
+    // algorithmic bytes of one assembly launch: each GP record read once
+    // (3 nn + 28 used doubles), each block written once, the slot tables
+    // and node adjacency read once, fc and ddx written
+    double ab = (double)h->nlmnt * h->npg * (3.0 * NN + 28.0) * 8.0 + (double)nn * (48.0 + 8.0 + 12.0 * MAXADJ);
+    for (int p = 0; p < nn; ++p) ab += nslot[p] * (72.0 + 4.0 + 8.0);
     h->asm_bytes = ab;
     cudaStream_t s = h->stream;
     CKA(h->perm.alloc(nn));
     CKA(h->rowof.alloc(nn));
     CKA(h->nslot.alloc(nn));
-    CKA(h->bcol.alloc((size_t)CROW * nn));
-    CKA(h->bloc.alloc((size_t)CROW * nn));
-    CKA(h->blk.alloc((size_t)BROW * nn));
+    CKA(h->bcol.alloc((size_t)crow * nn));
+    CKA(h->bloc.alloc((size_t)crow * nn));
+    CKA(h->blk.alloc((size_t)brow * nn));
     CK(h->perm.put(perm.data(), nn, s));
     CK(h->rowof.put(rowof.data(), nn, s));
     CK(h->nslot.put(nslot.data(), nn, s));
@@ -370,8 +386,9 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
         // chunks of TMA_ROWS rows; one wave of as many CTAs as the
         // shared-memory rings let reside per SM, which also keeps the
         // per-sweep partial sums few enough for a cheap deterministic check
+        const int cps = h->slots == SLOTS ? TMA_CTAS_PER_SM : tma_ctas_per_sm<SLOTS20, TMA_LPR81>();
         h->sor_nblk[c] = (int)std::min<long long>(nblocks(h->col_start[c + 1] - h->col_start[c], TMA_ROWS),
-                                                   (long long)h->nsm * TMA_CTAS_PER_SM);
+                                                   (long long)h->nsm * cps);
         tot += h->sor_nblk[c];
     }
     h->sor_nblk_tot = std::max(tot, 1);
@@ -379,9 +396,50 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
     if (FAS_SOR_RCP) CKA(h->rdiag.alloc((size_t)3 * nn));
     CKA(h->d_cstart.alloc(h->ncol + 1));
     CK(h->d_cstart.put(h->col_start.data(), h->ncol + 1, s));
-    h->sor_small = nn <= SOR_SMALL_ROWS;
+    h->sor_small = nn <= SOR_SMALL_ROWS && h->slots == SLOTS;   // one slot per lane
     CK(cudaStreamSynchronize(s));
     return 0;
+}
+
+// SHAPE_22's local-derivative table (src/fasolt/Shapef.f90:259-316),
+// t[(g*3 + j)*20 + i] = dndn(j+1, i+1, g+1): the serendipity functions of
+// the 20-node brick at the GP coordinate 0.57735, rounded to 6 decimals as
+// the reference tabulates them.  Node order is ADDEL_20NQ's; GPs 1-4 lie
+// anticlockwise from node 1 at zeta < 0, 5-8 above them.
+std::vector<double> shape22_table()
+{
+    static const int loc[20][3] = {{-1, -1, -1}, {0, -1, -1}, {1, -1, -1}, {1, 0, -1}, {1, 1, -1},
+                                   {0, 1, -1},   {-1, 1, -1}, {-1, 0, -1}, {-1, -1, 0}, {1, -1, 0},
+                                   {1, 1, 0},    {-1, 1, 0},  {-1, -1, 1}, {0, -1, 1},  {1, -1, 1},
+                                   {1, 0, 1},    {1, 1, 1},   {0, 1, 1},   {-1, 1, 1},  {-1, 0, 1}};
+    static const int gsign[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                                    {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+    const double a = 0.57735;
+    std::vector<double> t(480);
+    for (int g = 0; g < 8; ++g) {
+        const double q[3] = {gsign[g][0] * a, gsign[g][1] * a, gsign[g][2] * a};
+        for (int i = 0; i < 20; ++i) {
+            const int *c = loc[i];
+            double d[3];
+            if (c[0] && c[1] && c[2]) {   // corner
+                const double f[3] = {1 + q[0] * c[0], 1 + q[1] * c[1], 1 + q[2] * c[2]};
+                const double sum = q[0] * c[0] + q[1] * c[1] + q[2] * c[2] - 2;
+                for (int j = 0; j < 3; ++j) {
+                    const int j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+                    d[j] = 0.125 * c[j] * f[j1] * f[j2] * (sum + f[j]);
+                }
+            } else {                       // mid-edge along its zero coordinate
+                const int z = !c[0] ? 0 : (!c[1] ? 1 : 2);
+                const int z1 = (z + 1) % 3, z2 = (z + 2) % 3;
+                const double f1 = 1 + q[z1] * c[z1], f2 = 1 + q[z2] * c[z2], e = 1 - q[z] * q[z];
+                d[z] = 0.25 * (-2 * q[z]) * f1 * f2;
+                d[z1] = 0.25 * e * c[z1] * f2;
+                d[z2] = 0.25 * e * f1 * c[z2];
+            }
+            for (int j = 0; j < 3; ++j) t[(g * 3 + j) * 20 + i] = std::round(d[j] * 1e6) / 1e6;
+        }
+    }
+    return t;
 }
 
 int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, const fas_ctrl_desc *Cd)
@@ -394,10 +452,14 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
     if (prop.major != 10) return FAS_E_NODEVICE;
     h->nsm = prop.multiProcessorCount;
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-    CK(cudaFuncSetAttribute(k_sor_colour_tma<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            tma_smem_bytes<double>()));
-    CK(cudaFuncSetAttribute(k_sor_colour_tma<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            tma_smem_bytes<float>()));
+    CK(cudaFuncSetAttribute(k_sor_colour_tma<double, SLOTS, TMA_LPR>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem_bytes<double, SLOTS>()));
+    CK(cudaFuncSetAttribute(k_sor_colour_tma<float, SLOTS, TMA_LPR>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem_bytes<float, SLOTS>()));
+    CK(cudaFuncSetAttribute(k_sor_colour_tma<double, SLOTS20, TMA_LPR81>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem_bytes<double, SLOTS20>()));
+    CK(cudaFuncSetAttribute(k_sor_colour_tma<float, SLOTS20, TMA_LPR81>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem_bytes<float, SLOTS20>()));
     CK(cudaMallocHost((void **)&h->hc, sizeof(HostCtl)));
     CK(cudaEventCreate(&h->ev_t0));
     CK(cudaEventCreate(&h->ev_t1));
@@ -411,32 +473,41 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
     h->h_gp_iel.assign(h->ngps, 1);
     if (!h->point_mode) {
         if (!Md->le || !Md->lt || !Md->nd || !Md->np || !Md->ln || !Md->lg || !Md->ib) return FAS_E_ARG;
-        if (Md->ld_ln < 8 || Md->ld_lg < 1 || h->nnod < 1) return FAS_E_ARG;
         const int ne = h->nlmnt;
-        h->h_ln.resize((size_t)ne * 8);
-        h->h_gpe.resize(ne);
+        // one element family per mesh: 8-node one-GP bricks (lt 12) or
+        // 20-node eight-GP bricks (lt 22)
+        const int lt0 = ne ? Md->lt[0] : 12;
+        if (lt0 != 12 && lt0 != 22) return FAS_E_ELTYPE;
+        h->nn = lt0 == 12 ? 8 : 20;
+        h->npg = lt0 == 12 ? 1 : 8;
+        const int NN = h->nn, NG = h->npg;
+        if (Md->ld_ln < NN || Md->ld_lg < NG || h->nnod < 1) return FAS_E_ARG;
+        h->h_ln.resize((size_t)ne * NN);
+        h->h_gpe.resize((size_t)ne * NG);
         h->h_le.assign(Md->le, Md->le + ne);
         std::vector<int> gp_seen(h->ngps, 0);
         for (int e = 0; e < ne; ++e) {
-            if (Md->lt[e] != 12) return FAS_E_ELTYPE;
-            if (Md->nd[e] != 8 || Md->np[e] != 1) return FAS_E_ARG;
-            for (int a = 0; a < 8; ++a) {
+            if (Md->lt[e] != lt0) return FAS_E_ELTYPE;
+            if (Md->nd[e] != NN || Md->np[e] != NG) return FAS_E_ARG;
+            for (int a = 0; a < NN; ++a) {
                 const int id = Md->ln[(size_t)e * Md->ld_ln + a];
                 if (id < 1 || id > h->nnod) return FAS_E_ARG;
-                h->h_ln[(size_t)e * 8 + a] = id - 1;
+                h->h_ln[(size_t)e * NN + a] = id - 1;
             }
-            const int g = Md->lg[(size_t)e * Md->ld_lg];
-            if (g < 1 || g > h->ngps || gp_seen[g - 1]) return FAS_E_ARG;
-            gp_seen[g - 1] = 1;
-            h->h_gpe[e] = g - 1;
-            h->h_gp_iel[g - 1] = Md->le[e];
+            for (int q = 0; q < NG; ++q) {
+                const int g = Md->lg[(size_t)e * Md->ld_lg + q];
+                if (g < 1 || g > h->ngps || gp_seen[g - 1]) return FAS_E_ARG;
+                gp_seen[g - 1] = 1;
+                h->h_gpe[(size_t)e * NG + q] = g - 1;
+                h->h_gp_iel[g - 1] = Md->le[e];
+            }
         }
         if (std::abs(Md->le[ne - 1]) >= 1) h->last_mat = std::abs(Md->le[ne - 1]);
         h->h_ib.assign(Md->ib, Md->ib + h->nnod);
         // node -> element CSR (ascending element ids)
         h->ne_ptr.assign(h->nnod + 1, 0);
         for (int e = 0; e < ne; ++e)
-            for (int a = 0; a < 8; ++a) h->ne_ptr[h->h_ln[(size_t)e * 8 + a] + 1]++;
+            for (int a = 0; a < NN; ++a) h->ne_ptr[h->h_ln[(size_t)e * NN + a] + 1]++;
         for (int n = 0; n < h->nnod; ++n) {
             if (h->ne_ptr[n + 1] > MAXADJ) return FAS_E_RANGE;
             h->ne_ptr[n + 1] += h->ne_ptr[n];
@@ -445,16 +516,18 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
         h->ne_locl.resize(h->ne_ptr[h->nnod]);
         std::vector<int> fill(h->ne_ptr.begin(), h->ne_ptr.end() - 1);
         for (int e = 0; e < ne; ++e)
-            for (int a = 0; a < 8; ++a) {
-                const int n = h->h_ln[(size_t)e * 8 + a];
+            for (int a = 0; a < NN; ++a) {
+                const int n = h->h_ln[(size_t)e * NN + a];
                 h->ne_list[fill[n]] = e;
                 h->ne_locl[fill[n]] = a;
                 fill[n]++;
             }
-        std::vector<int> lnT((size_t)8 * ne), nee((size_t)MAXADJ * h->nnod, -1),
+        std::vector<int> lnT((size_t)NN * ne), gpeT((size_t)NG * ne), nee((size_t)MAXADJ * h->nnod, -1),
             nel((size_t)MAXADJ * h->nnod, 0), nec(h->nnod);
-        for (int e = 0; e < ne; ++e)
-            for (int a = 0; a < 8; ++a) lnT[(size_t)a * ne + e] = h->h_ln[(size_t)e * 8 + a];
+        for (int e = 0; e < ne; ++e) {
+            for (int a = 0; a < NN; ++a) lnT[(size_t)a * ne + e] = h->h_ln[(size_t)e * NN + a];
+            for (int q = 0; q < NG; ++q) gpeT[(size_t)q * ne + e] = h->h_gpe[(size_t)e * NG + q];
+        }
         for (int n = 0; n < h->nnod; ++n) {
             nec[n] = h->ne_ptr[n + 1] - h->ne_ptr[n];
             for (int k = 0; k < nec[n]; ++k) {
@@ -462,15 +535,20 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
                 nel[(size_t)k * h->nnod + n] = h->ne_locl[h->ne_ptr[n] + k];
             }
         }
+        if (NN == 20) {
+            const std::vector<double> t = shape22_table();
+            CKA(h->dn22.alloc(t.size()));
+            CK(h->dn22.put(t.data(), t.size(), s));
+        }
         CKA(h->ln.alloc(lnT.size()));
-        CKA(h->gpe.alloc(ne));
+        CKA(h->gpe.alloc(gpeT.size()));
         CKA(h->le.alloc(ne));
         CKA(h->ib.alloc(h->nnod));
         CKA(h->ne_elem.alloc(nee.size()));
         CKA(h->ne_loc.alloc(nel.size()));
         CKA(h->ne_cnt.alloc(nec.size()));
         CK(h->ln.put(lnT.data(), lnT.size(), s));
-        CK(h->gpe.put(h->h_gpe.data(), ne, s));
+        CK(h->gpe.put(gpeT.data(), gpeT.size(), s));
         CK(h->le.put(h->h_le.data(), ne, s));
         CK(h->ib.put(h->h_ib.data(), h->nnod, s));
         CK(h->ne_elem.put(nee.data(), nee.size(), s));
@@ -584,7 +662,7 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
         CKA(h->chi_pts.alloc(36 * ng));
         CK(h->chi_pts.zero(s));
     } else {
-        CKA(h->rec.alloc((size_t)REC * h->nlmnt));
+        CKA(h->rec.alloc((size_t)(3 * h->nn + 32) * h->nlmnt * h->npg));
         CK(h->rec.zero(s));
     }
     h->nr_nblk = (int)std::min<long long>(nblocks(std::max<long long>(h->nnod, h->ngps), 256), 1184);
@@ -725,7 +803,11 @@ int download_impl(fas_handle *h, const fas_state_desc *S)
 template <int NS> int launch_elem(fas_handle *h, int inc, int nit)
 {
     Span sp(h, &h->P.ms_constitutive);
-    if (!(h->mode & FAS_MODE_CP_WARP))
+    if (h->nn == 20)   // 20-node bricks: one thread per (element, GP)
+        k_elem22<NS><<<nblocks(8LL * h->nlmnt, 128), 128, 0, h->stream>>>(
+            h->mesh(), h->M, h->C, h->gp(), h->dn22.p, h->x.p, h->dx.p, h->rec.p, h->h_tiem[inc - 1], inc, nit,
+            h->ekey.p);
+    else if (!(h->mode & FAS_MODE_CP_WARP))
         k_elem<NS><<<nblocks(h->nlmnt, 128), 128, 0, h->stream>>>(
             h->mesh(), h->M, h->C, h->gp(), h->x.p, h->dx.p, h->rec.p, h->h_tiem[inc - 1], inc, nit, h->ekey.p);
     else
@@ -745,7 +827,7 @@ int ensure_fp32(fas_handle *h)
 {
     if (!(h->mode & FAS_MODE_SOR_FP32) || h->blk32.p || h->point_mode) return 0;
     const size_t nd3 = 3 * (size_t)h->nnod;
-    CKA(h->blk32.alloc((size_t)BROW * h->nnod));
+    CKA(h->blk32.alloc((size_t)brow_of(h->slots) * h->nnod));
     CKA(h->sor_d.alloc(nd3));
     CKA(h->sor_r.alloc(nd3));
     CK(h->blk32.zero(h->stream));
@@ -772,8 +854,9 @@ int elvals_impl(fas_handle *h, int inc, int nit, bool bc)
     if (rc) return rc;
     {
         Span sp(h, &h->P.ms_assembly);
-        const long long nthr = (long long)SLOTS * h->nnod;   // thread (row, slot), row-major
-        k_assemble<<<nblocks(nthr, 256), 256, 0, s>>>(
+        const long long nthr = (long long)h->slots * h->nnod;   // thread (row, slot), row-major
+        auto kern = h->nn == 20 ? k_assemble<20, 8> : k_assemble<8, 1>;
+        kern<<<nblocks(nthr, 256), 256, 0, s>>>(
             h->mesh(), h->block(), h->rec.p, h->x.p, h->dx.p, h->fc.p, h->ddx.p,
             h->xspec.p + (size_t)(inc - 1) * std::max(h->nxs, 1) * 15,
             h->fspec.p + (size_t)(inc - 1) * std::max(h->nfs, 1) * 3, h->nxs, h->nfs, h->C.efix,
@@ -833,21 +916,44 @@ void launch_pdl(void (*kern)(KArgs...), unsigned grid, unsigned block, size_t sm
     cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
 }
 
+// One colour-kernel launch of the row layout's instantiation (27 or 81
+// slots), with programmatic serialisation when `pdl` is set.
+template <typename T>
+void launch_colour_kernel(fas_handle *h, int c, bool pdl, const T *blk, const double *rhs, double *sol,
+                          const double *base, const double *rdiag, SorCtl *ctl, double *part)
+{
+    const int p0 = h->col_start[c], p1 = h->col_start[c + 1];
+    if (p1 <= p0) return;
+    if (h->slots == SLOTS) {
+        auto k = k_sor_colour_tma<T, SLOTS, TMA_LPR>;
+        if (pdl)
+            launch_pdl(k, h->sor_nblk[c], TMA_THREADS, tma_smem_bytes<T, SLOTS>(), h->stream, blk, h->bcol.p, p0,
+                       p1, rhs, sol, base, rdiag, ctl, part, h->sor_boff[c], h->sor_nblk_tot);
+        else
+            k<<<h->sor_nblk[c], TMA_THREADS, tma_smem_bytes<T, SLOTS>(), h->stream>>>(
+                blk, h->bcol.p, p0, p1, rhs, sol, base, rdiag, ctl, part, h->sor_boff[c], h->sor_nblk_tot);
+    } else {
+        auto k = k_sor_colour_tma<T, SLOTS20, TMA_LPR81>;
+        const unsigned nt = tma_threads<TMA_LPR81>();
+        if (pdl)
+            launch_pdl(k, h->sor_nblk[c], nt, tma_smem_bytes<T, SLOTS20>(), h->stream, blk, h->bcol.p, p0, p1,
+                       rhs, sol, base, rdiag, ctl, part, h->sor_boff[c], h->sor_nblk_tot);
+        else
+            k<<<h->sor_nblk[c], nt, tma_smem_bytes<T, SLOTS20>(), h->stream>>>(
+                blk, h->bcol.p, p0, p1, rhs, sol, base, rdiag, ctl, part, h->sor_boff[c], h->sor_nblk_tot);
+    }
+}
+
 // One colour phase: FP64 blocks on (rhs, sol), or the FP32 copy on the
 // refinement's (residual, correction) with the iterate as base.
 void launch_colour(fas_handle *h, int c, bool fp32)
 {
-    const int p0 = h->col_start[c], p1 = h->col_start[c + 1];
-    if (p1 <= p0) return;
     if (fp32)
-        launch_pdl(k_sor_colour_tma<float>, h->sor_nblk[c], TMA_THREADS, tma_smem_bytes<float>(), h->stream,
-                   h->blk32.p, h->bcol.p, p0, p1, h->sor_r.p, h->sor_d.p, h->ddx.p, (const double *)nullptr,
-                   h->sorctl.p, h->part_sor.p, h->sor_boff[c], h->sor_nblk_tot);
+        launch_colour_kernel<float>(h, c, true, h->blk32.p, h->sor_r.p, h->sor_d.p, h->ddx.p, nullptr,
+                                    h->sorctl.p, h->part_sor.p);
     else
-        launch_pdl(k_sor_colour_tma<double>, h->sor_nblk[c], TMA_THREADS, tma_smem_bytes<double>(), h->stream,
-                   h->blk.p, h->bcol.p, p0, p1, h->rhs.p, h->ddx.p, (const double *)nullptr,
-                   (const double *)(FAS_SOR_RCP ? h->rdiag.p : nullptr), h->sorctl.p, h->part_sor.p,
-                   h->sor_boff[c], h->sor_nblk_tot);
+        launch_colour_kernel<double>(h, c, true, h->blk.p, h->rhs.p, h->ddx.p, nullptr,
+                                     FAS_SOR_RCP ? h->rdiag.p : nullptr, h->sorctl.p, h->part_sor.p);
 }
 
 void launch_check(fas_handle *h, double tolerl)
@@ -1475,11 +1581,9 @@ int facsls_noalloc_impl(fas_handle *h, int *sweeps, double *error)
             const int k = std::min(chunk, 1000 - done);
             for (int it = 0; it < k; ++it) {
                 for (int c = 0; c < h->ncol; ++c) {
-                    const int p0 = h->col_start[c], p1 = h->col_start[c + 1];
-                    if (p1 <= p0) continue;
-                    k_sor_colour_tma<double><<<h->sor_nblk[c], TMA_THREADS, tma_smem_bytes<double>(), s>>>(
-                        h->blk.p, h->bcol.p, p0, p1, h->rhs.p, h->ddx.p, nullptr, nullptr, ctl, part,
-                        h->sor_boff[c], h->sor_nblk_tot);
+                    if (h->col_start[c + 1] <= h->col_start[c]) continue;
+                    launch_colour_kernel<double>(h, c, false, h->blk.p, h->rhs.p, h->ddx.p, nullptr, nullptr, ctl,
+                                                 part);
                     LAUNCHED(h);
                 }
                 k_sor_check<<<1, 1024, 0, s>>>(part, h->sor_nblk_tot, ctl, tolerl);

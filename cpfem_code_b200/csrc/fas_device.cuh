@@ -251,6 +251,49 @@ __device__ __forceinline__ double shape12(const double xn[8][3], double dndx[8][
     return 8.0 * det;
 }
 
+// INVERT_3, src/fasolt/Shapef.f90:499-537: inv = jac^-1 (cofactors / det),
+// returns det (inv left as the cofactors when det == 0).
+__device__ __forceinline__ double invert3(const double jac[3][3], double inv[3][3])
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const int ia = (i + 1) % 3, ib = (ia + 1) % 3;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const int ja = (j + 1) % 3, jb = (ja + 1) % 3;
+            inv[j][i] = jac[ia][ja] * jac[ib][jb] - jac[ia][jb] * jac[ib][ja];
+        }
+    }
+    const double det = inv[0][0] * jac[0][0] + inv[0][1] * jac[1][0] + inv[0][2] * jac[2][0];
+    if (det != 0.0) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) inv[i][j] = inv[i][j] / det;
+    }
+    return det;
+}
+
+// DSTRNS (src/fasolt/Sig_eps.f90:193-229) from the displacement gradient
+// g[a][b] = sum_i sfd(a,i) dxl(b,i).  Returns 0, 905 or 906.
+__device__ __forceinline__ int dstrns_grad(const double g[3][3], double smalr, double smale, double del[6],
+                                           double r[3], double &deff)
+{
+    double sum = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const int j = (i + 1) % 3, k = (j + 1) % 3;
+        del[i] = g[i][i];
+        del[i + 3] = g[k][j] + g[j][k];
+        r[i] = (g[k][j] - g[j][k]) / 2.0;
+        sum = sum + r[i] * r[i];
+    }
+    deff = fj2vom(false, del);
+    if (sum > smalr) return 905;
+    if (deff > smale) return 906;
+    return 0;
+}
+
 // DSTRNS, src/fasolt/Sig_eps.f90:193-229.  Returns 0, 905 or 906.
 __device__ __forceinline__ int dstrns(const double sfd[8][3], const double dxl[8][3],
                                       double smalr, double smale, double del[6], double r[3],

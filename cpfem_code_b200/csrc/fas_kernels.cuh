@@ -19,24 +19,34 @@
 
 namespace fasdev {
 
-constexpr int REC = 56;          // doubles per element record
-constexpr int REC_S = 24, REC_W = 30, REC_D = 32;
+// Gauss-point record of an NN-node element: sfd (3 NN), stress (6),
+// weight, pad, tangent upper triangle (21), pad.
+template <int NN> struct RecLayout {
+    static constexpr int S = 3 * NN, W = 3 * NN + 6, D = 3 * NN + 8, LEN = 3 * NN + 32;
+};
+constexpr int REC = RecLayout<8>::LEN;   // 56 doubles per 8-node element record
+constexpr int REC_S = RecLayout<8>::S, REC_W = RecLayout<8>::W, REC_D = RecLayout<8>::D;
 constexpr int SLOTS = 27;        // node blocks per row of an 8-node brick mesh
+constexpr int SLOTS20 = 81;      // node blocks per row of a 20-node brick mesh
 constexpr int MAXADJ = 8;        // elements per node
 
-// block matrix addressing
-constexpr int BROW = 244;        // values per block row (27 x 9 + 1 pad)
-constexpr int CROW = 28;         // column ids per block row (27 + 1 pad)
-__host__ __device__ __forceinline__ size_t sidx(int p, int s) { return (size_t)p * CROW + s; }
-__host__ __device__ __forceinline__ size_t bidx(int p, int s, int q) { return (size_t)p * BROW + q * 27 + s; }
+// block matrix addressing: a row of S slots holds 9 S values padded to an
+// even count (16-byte rows) and S column ids plus the slot count padded to
+// a multiple of 4
+__host__ __device__ constexpr int brow_of(int S) { return (S * 9 + 1) / 2 * 2; }
+__host__ __device__ constexpr int crow_of(int S) { return (S + 1 + 3) / 4 * 4; }
+constexpr int BROW = brow_of(SLOTS);   // 244
+constexpr int CROW = crow_of(SLOTS);   // 28
+static_assert(BROW == 244 && CROW == 28, "8-node row layout");
 
 // upper-triangle index of chi(i,j), i <= j (0-based)
 __host__ __device__ __forceinline__ int utri(int i, int j) { return i * 6 - (i * (i - 1)) / 2 + (j - i); }
 
 struct MeshDev {
     int nlmnt, nnod;
-    const int *ln;       // [8][nlmnt] 0-based node ids
-    const int *gpe;      // [nlmnt] 0-based GP of the element
+    int nn, npg;         // nodes and Gauss points per element (8, 1 or 20, 8)
+    const int *ln;       // [nn][nlmnt] 0-based node ids
+    const int *gpe;      // [npg][nlmnt] 0-based GPs of the element
     const int *le;       // [nlmnt]
     const int *ib;       // [nnod]
     const int *ne_elem;  // [MAXADJ][nnod] adjacent elements, ascending
@@ -46,13 +56,16 @@ struct MeshDev {
 
 struct BlockDev {
     int R;               // rows (= nnod)
+    int slots, brow, crow;   // slots per row and the row lengths (brow_of, crow_of)
     const int *perm;     // row -> node
     const int *nslot;    // [R]
-    const int *bcol;     // [R][SLOTS] column node of each slot
-    const unsigned *bloc;// [R][SLOTS] 4-bit local index of the column node in
-                         // each adjacent element of the row node (0xF: absent)
-    double *blk;         // [R][9][SLOTS]
+    const int *bcol;     // [R][crow] column node of each slot; [slots] = nslot
+    const unsigned long long *bloc;   // [R][crow] byte k: local index of the column node
+                                      // in the k-th adjacent element of the row node (0xFF: absent)
+    double *blk;         // [R][brow]: value (r, c) of slot s at (r*3+c)*slots + s
     float *blk32;        // FP32 copy of blk (tuned mode), or null
+    __host__ __device__ size_t si(int p, int s) const { return (size_t)p * crow + s; }
+    __host__ __device__ size_t bi(int p, int s, int q) const { return (size_t)p * brow + (size_t)q * slots + s; }
 };
 
 // ---------------------------------------------------------------- element pass
@@ -124,6 +137,102 @@ __global__ void __launch_bounds__(128) k_elem(MeshDev Mh, DevMat M, DevCtrl C, D
     for (int i = 0; i < 6; ++i)
 #pragma unroll
         for (int j = i; j < 6; ++j) R[REC_D + utri(i, j)] = o.chi[i][j];
+}
+
+// ELVALS per Gauss point of 20-node bricks (src/fasolt/Elvals.f90:82-126
+// with SHAPE_22, src/fasolt/Shapef.f90:210-342): one thread per (element,
+// GP).  dn22[(g*3 + j)*20 + i] = dndn(j+1, i+1, g+1) is the reference's
+// tabulated local-derivative table.  The element's 20 nodes are streamed
+// twice -- the Jacobian, then sfd (written straight to the GP record) and
+// the displacement gradient -- so no 20-node array is held in registers.
+// Errors are keyed by (element, GP) so the first one in the reference's
+// loop order wins.
+template <int NS>
+__global__ void __launch_bounds__(128) k_elem22(MeshDev Mh, DevMat M, DevCtrl C, DevGp G,
+                                                const double *__restrict__ dn22,
+                                                const double *__restrict__ x,
+                                                const double *__restrict__ dx, double *rec,
+                                                double dt, int inc, int nit,
+                                                unsigned long long *errkey)
+{
+    using L = RecLayout<20>;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 8LL * Mh.nlmnt) return;
+    const int e = (int)(t >> 3), gq = (int)(t & 7);
+    const int ne = Mh.nlmnt;
+    const unsigned long long key = (unsigned long long)t << 16;
+    const double *dn = dn22 + gq * 60;
+    double jac[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int i = 0; i < 20; ++i) {
+        const int n = Mh.ln[i * ne + e];
+        const double d0 = __ldg(dn + i), d1 = __ldg(dn + 20 + i), d2 = __ldg(dn + 40 + i);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const double xk = x[3 * n + k];
+            jac[0][k] = jac[0][k] + d0 * xk;
+            jac[1][k] = jac[1][k] + d1 * xk;
+            jac[2][k] = jac[2][k] + d2 * xk;
+        }
+    }
+    double inv[3][3];
+    const double w = 1.0 * invert3(jac, inv);
+    if (w < 1.e-7) {
+        atomicMin(errkey, key | 920ull);
+        return;
+    }
+    double *R = rec + (size_t)t * L::LEN;
+    double gr[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int i = 0; i < 20; ++i) {
+        const int n = Mh.ln[i * ne + e];
+        const double d0 = __ldg(dn + i), d1 = __ldg(dn + 20 + i), d2 = __ldg(dn + 40 + i);
+        double sf[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            sf[k] = inv[k][0] * d0 + inv[k][1] * d1 + inv[k][2] * d2;
+            R[3 * i + k] = sf[k];
+        }
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const double u = dx[3 * n + b];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) gr[a][b] = gr[a][b] + sf[a] * u;
+        }
+    }
+    double del[6], r[3], defl;
+    int rc = dstrns_grad(gr, C.smalr, C.smale, del, r, defl);
+    if (rc) {
+        atomicMin(errkey, key | (unsigned long long)rc);
+        return;
+    }
+    const int g = Mh.gpe[gq * ne + e];
+    const int ng = G.ngps;
+    double st[6], ds[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        st[k] = G.st[k * ng + g];
+        ds[k] = G.ds[k * ng + g];
+    }
+    GpOut o;
+    rc = dstrss<NS>(M, C, G, g, Mh.le[e], del, r, st, ds, dt, inc, nit, o);
+    if (rc) {
+        atomicMin(errkey, key | (unsigned long long)rc);
+        return;
+    }
+    G.dep[g] = o.deff;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        G.de[k * ng + g] = del[k];
+        G.ds[k * ng + g] = ds[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) G.dr[k * ng + g] = r[k];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) R[L::S + k] = o.t[k];
+    R[L::W] = w;
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int j = i; j < 6; ++j) R[L::D + utri(i, j)] = o.chi[i][j];
 }
 
 // Constitutive update of independent points (no mesh): DSTRSS with the
@@ -396,6 +505,7 @@ __device__ __forceinline__ int apply_bc(int ibc, int n, const double *x, const d
 // writes the 3x3 block once -- no atomics, no read-modify-write of the
 // matrix.  The diagonal-slot thread also forms the nodal force
 // (Elvals.f90:122-126,265-271) and, when `bc` is set, applies SUVALS.
+template <int NN, int NPG>
 __global__ void __launch_bounds__(256) k_assemble(MeshDev Mh, BlockDev B,
                                                   const double *__restrict__ rec,
                                                   const double *__restrict__ x,
@@ -404,41 +514,57 @@ __global__ void __launch_bounds__(256) k_assemble(MeshDev Mh, BlockDev B,
                                                   const double *fspec, int nxs, int nfs,
                                                   double efix, int bc, int *bad_bc)
 {
+    using L = RecLayout<NN>;
     const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int p = (int)(tid / SLOTS);
-    const int s = (int)(tid - (long long)p * SLOTS);
+    const int p = (int)(tid / B.slots);
+    const int s = (int)(tid - (long long)p * B.slots);
     if (p >= B.R) return;
     if (s >= B.nslot[p]) return;
     const int n = B.perm[p];
-    const unsigned bl = B.bloc[sidx(p, s)];
+    const unsigned long long bl = B.bloc[B.si(p, s)];
     const int cnt = Mh.ne_cnt[n];
     double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     double f[3] = {0, 0, 0};
     for (int k = 0; k < cnt; ++k) {
-        const int b = (bl >> (4 * k)) & 0xF;
-        if (b == 0xF) continue;
+        const int b = (int)((bl >> (8 * k)) & 0xFFull);
+        if (b == 0xFF) continue;
         const int e = Mh.ne_elem[k * Mh.nnod + n];
         const int a = Mh.ne_loc[k * Mh.nnod + n];
-        const double *Rr = rec + (size_t)e * REC;
-        double sa[3], sb[3], st[6], d[21];
+        // the element's contribution, summed over its GPs first
+        // (Elvals.f90:82-236), is added to the block in element order
+        double ae[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        double fe[3] = {0, 0, 0};
+        for (int g = 0; g < NPG; ++g) {
+            const double *Rr = rec + ((size_t)e * NPG + g) * L::LEN;
+            double sa[3], sb[3], st[6], d[21];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            sa[c] = __ldg(Rr + 3 * a + c);
-            sb[c] = __ldg(Rr + 3 * b + c);
+            for (int c = 0; c < 3; ++c) {
+                sa[c] = __ldg(Rr + 3 * a + c);
+                sb[c] = __ldg(Rr + 3 * b + c);
+            }
+#pragma unroll
+            for (int c = 0; c < 6; ++c) st[c] = __ldg(Rr + L::S + c);
+            const double w = __ldg(Rr + L::W);
+#pragma unroll
+            for (int c = 0; c < 21; ++c) d[c] = __ldg(Rr + L::D + c);
+            double gm[9];
+            gaussm_block(sa, sb, d, st, gm);
+            double *ta = NPG == 1 ? acc : ae;
+            double *tf = NPG == 1 ? f : fe;
+#pragma unroll
+            for (int q = 0; q < 9; ++q) ta[q] = ta[q] + w * gm[q];
+            if (s == 0) {
+                tf[0] = tf[0] + w * (st[0] * sa[0] + st[5] * sa[1] + st[4] * sa[2]);
+                tf[1] = tf[1] + w * (st[1] * sa[1] + st[3] * sa[2] + st[5] * sa[0]);
+                tf[2] = tf[2] + w * (st[2] * sa[2] + st[4] * sa[0] + st[3] * sa[1]);
+            }
         }
+        if (NPG > 1) {
 #pragma unroll
-        for (int c = 0; c < 6; ++c) st[c] = __ldg(Rr + REC_S + c);
-        const double w = __ldg(Rr + REC_W);
+            for (int q = 0; q < 9; ++q) acc[q] = acc[q] + ae[q];
+            if (s == 0)
 #pragma unroll
-        for (int c = 0; c < 21; ++c) d[c] = __ldg(Rr + REC_D + c);
-        double gm[9];
-        gaussm_block(sa, sb, d, st, gm);
-#pragma unroll
-        for (int q = 0; q < 9; ++q) acc[q] = acc[q] + w * gm[q];
-        if (s == 0) {
-            f[0] = f[0] + w * (st[0] * sa[0] + st[5] * sa[1] + st[4] * sa[2]);
-            f[1] = f[1] + w * (st[1] * sa[1] + st[3] * sa[2] + st[5] * sa[0]);
-            f[2] = f[2] + w * (st[2] * sa[2] + st[4] * sa[0] + st[3] * sa[1]);
+                for (int c = 0; c < 3; ++c) f[c] = f[c] + fe[c];
         }
     }
     if (s == 0) {
@@ -451,10 +577,10 @@ __global__ void __launch_bounds__(256) k_assemble(MeshDev Mh, BlockDev B,
         }
     }
 #pragma unroll
-    for (int q = 0; q < 9; ++q) B.blk[bidx(p, s, q)] = acc[q];
+    for (int q = 0; q < 9; ++q) B.blk[B.bi(p, s, q)] = acc[q];
     if (B.blk32) {
 #pragma unroll
-        for (int q = 0; q < 9; ++q) B.blk32[bidx(p, s, q)] = (float)acc[q];
+        for (int q = 0; q < 9; ++q) B.blk32[B.bi(p, s, q)] = (float)acc[q];
     }
 }
 
@@ -472,13 +598,13 @@ __global__ void k_suvals(MeshDev Mh, BlockDev B, const int *rowof, const double 
         const int p = rowof[n];
         double D[9];
 #pragma unroll
-        for (int q = 0; q < 9; ++q) D[q] = B.blk[bidx(p, 0, q)];
+        for (int q = 0; q < 9; ++q) D[q] = B.blk[B.bi(p, 0, q)];
         if (apply_bc(ibc, n, x, dx, xspec, fspec, nxs, nfs, efix, D, f)) *bad_bc = 1;
 #pragma unroll
-        for (int q = 0; q < 9; ++q) B.blk[bidx(p, 0, q)] = D[q];
+        for (int q = 0; q < 9; ++q) B.blk[B.bi(p, 0, q)] = D[q];
         if (B.blk32) {
 #pragma unroll
-            for (int q = 0; q < 9; ++q) B.blk32[bidx(p, 0, q)] = (float)D[q];
+            for (int q = 0; q < 9; ++q) B.blk32[B.bi(p, 0, q)] = (float)D[q];
         }
     }
 #pragma unroll
@@ -602,10 +728,10 @@ __device__ __forceinline__ void load_row(const BlockDev &B, const T *__restrict_
 {
     o.ns = B.nslot[p];
     const bool on = lane < o.ns;
-    const int m = on ? __ldcs(B.bcol + sidx(p, lane)) : 0;
+    const int m = on ? __ldcs(B.bcol + B.si(p, lane)) : 0;
     o.n = __shfl_sync(0xffffffffu, m, 0);
 #pragma unroll
-    for (int q = 0; q < 9; ++q) o.b[q] = on ? ld_stream(blk + bidx(p, lane, q)) : 0.0;
+    for (int q = 0; q < 9; ++q) o.b[q] = on ? ld_stream(blk + B.bi(p, lane, q)) : 0.0;
     o.x0 = on ? sol[3 * m] : 0.0;
     o.x1 = on ? sol[3 * m + 1] : 0.0;
     o.x2 = on ? sol[3 * m + 2] : 0.0;
@@ -804,29 +930,39 @@ __device__ __forceinline__ void sweep_test(const double *part, int nblk, SorCtl 
 #define FAS_TMA_PD 1
 #endif
 constexpr int TMA_ROWS = FAS_TMA_ROWS;       // rows per chunk
-constexpr int TMA_LPR = FAS_TMA_LPR;         // lanes per row (a power of two, at most 32)
-constexpr int TMA_SPL = (SLOTS + TMA_LPR - 1) / TMA_LPR;   // slots per lane
-constexpr int TMA_THREADS = TMA_ROWS * TMA_LPR;
+constexpr int TMA_LPR = FAS_TMA_LPR;         // lanes per row of 27-slot rows (a power of two, at most 32)
+constexpr int TMA_LPR81 = 16;                // lanes per row of 81-slot rows
 constexpr int TMA_STAGES = FAS_TMA_STAGES;   // chunks in flight per CTA
 constexpr int TMA_PD = FAS_TMA_PD;           // chunks whose gathers run ahead of the computed one
 static_assert(TMA_PD >= 1 && TMA_PD < TMA_STAGES, "gathers run ahead within the ring");
+template <int LPR> __host__ __device__ constexpr int tma_threads() { return TMA_ROWS * LPR; }
+constexpr int TMA_THREADS = tma_threads<TMA_LPR>();
 static_assert(TMA_LPR >= 1 && TMA_LPR <= 32 && (TMA_LPR & (TMA_LPR - 1)) == 0, "lanes per row");
-static_assert(TMA_THREADS % 32 == 0 && TMA_THREADS <= 1024, "whole warps per CTA");
+static_assert(TMA_THREADS % 32 == 0 && tma_threads<TMA_LPR81>() % 32 == 0, "whole warps per CTA");
 
-template <typename T> __host__ __device__ constexpr int tma_stage_bytes()
+template <typename T, int S = SLOTS> __host__ __device__ constexpr int tma_stage_bytes()
 {
-    return TMA_ROWS * BROW * (int)sizeof(T) + TMA_ROWS * CROW * 4;
+    return TMA_ROWS * brow_of(S) * (int)sizeof(T) + TMA_ROWS * crow_of(S) * 4;
 }
-template <typename T> __host__ __device__ constexpr int tma_smem_bytes()
+// the ring, its mbarriers and a 512-byte guard: lanes whose slots lie past
+// the row (q + LPR j >= S) skip their reads, and the guard keeps even a
+// speculated shared-memory read of the last row inside the allocation
+template <typename T, int S = SLOTS> __host__ __device__ constexpr int tma_smem_bytes()
 {
-    return TMA_STAGES * tma_stage_bytes<T>() + TMA_STAGES * 8;
+    return TMA_STAGES * tma_stage_bytes<T, S>() + TMA_STAGES * 8 + 512;
 }
 // CTAs of the FP64 kernel that fit on one SM (228 KB of shared memory,
-// 1 KB of it reserved per CTA); the colour grid is sized to fill them.
-constexpr int TMA_CTAS_PER_SM = (228 * 1024) / (tma_smem_bytes<double>() + 1024) < 32 / (TMA_THREADS / 32)
-                                    ? (228 * 1024) / (tma_smem_bytes<double>() + 1024)
-                                    : 32 / (TMA_THREADS / 32);
-static_assert(TMA_CTAS_PER_SM >= 1, "the ring must fit in shared memory");
+// 1 KB of it reserved per CTA, at most 32 warps); the colour grid is sized
+// to fill them.
+template <int S, int LPR> __host__ __device__ constexpr int tma_ctas_per_sm()
+{
+    return (228 * 1024) / (tma_smem_bytes<double, S>() + 1024) < 32 / (tma_threads<LPR>() / 32)
+               ? (228 * 1024) / (tma_smem_bytes<double, S>() + 1024)
+               : 32 / (tma_threads<LPR>() / 32);
+}
+constexpr int TMA_CTAS_PER_SM = tma_ctas_per_sm<SLOTS, TMA_LPR>();
+static_assert(TMA_CTAS_PER_SM >= 1 && tma_ctas_per_sm<SLOTS20, TMA_LPR81>() >= 1,
+              "the ring must fit in shared memory");
 
 // One colour phase of SOR with the colour's block rows streamed through a
 // TMA_STAGES-deep shared-memory ring by the bulk-copy engine (evict-first in
@@ -842,8 +978,8 @@ static_assert(TMA_CTAS_PER_SM >= 1, "the ring must fit in shared memory");
 // computed: one L2 round trip per chunk is hidden.  Every mbarrier
 // wait is bounded; on a timeout the CTA waits (bounded) for its own copies
 // still in flight, raises ctl->fault and leaves.
-template <typename T>
-__global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restrict__ blk,
+template <typename T, int S, int LPR>
+__global__ void __launch_bounds__(TMA_ROWS * LPR) k_sor_colour_tma(const T *__restrict__ blk,
                                                                 const int *__restrict__ bcol, int p0, int p1,
                                                                 const double *__restrict__ rhs, double *sol,
                                                                 const double *__restrict__ base,
@@ -852,12 +988,14 @@ __global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restr
 {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int s_pre, s_post;
-    constexpr int VB = TMA_ROWS * BROW * (int)sizeof(T);
-    constexpr int SB = tma_stage_bytes<T>();
+    constexpr int BR = brow_of(S), CR = crow_of(S);
+    constexpr int SPL = (S + LPR - 1) / LPR;   // slots per lane
+    constexpr int VB = TMA_ROWS * BR * (int)sizeof(T);
+    constexpr int SB = tma_stage_bytes<T, S>();
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TMA_STAGES * SB);
     const int lane = threadIdx.x & 31;
-    const int row = threadIdx.x / TMA_LPR;   // row of the chunk served by this group
-    const int q = threadIdx.x % TMA_LPR;     // lane within the group
+    const int row = threadIdx.x / LPR;   // row of the chunk served by this group
+    const int q = threadIdx.x % LPR;     // lane within the group
     const int nchunks = (p1 - p0 + TMA_ROWS - 1) / TMA_ROWS;
     const int myn = (int)blockIdx.x < nchunks ? (nchunks - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     const uint64_t stream_pol = l2_evict_first();
@@ -867,10 +1005,10 @@ __global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restr
         const int r0 = p0 + c * TMA_ROWS;
         const int nr = min(TMA_ROWS, p1 - r0);
         unsigned char *st = smem + (k % TMA_STAGES) * SB;
-        const unsigned bv = (unsigned)(nr * BROW * sizeof(T)), bc = (unsigned)(nr * CROW * 4);
+        const unsigned bv = (unsigned)(nr * BR * sizeof(T)), bc = (unsigned)(nr * CR * 4);
         mbar_expect_tx(&bars[k % TMA_STAGES], bv + bc);
-        bulk_g2s(st, blk + (size_t)r0 * BROW, bv, &bars[k % TMA_STAGES], stream_pol);
-        bulk_g2s(st + VB, bcol + (size_t)r0 * CROW, bc, &bars[k % TMA_STAGES], stream_pol);
+        bulk_g2s(st, blk + (size_t)r0 * BR, bv, &bars[k % TMA_STAGES], stream_pol);
+        bulk_g2s(st + VB, bcol + (size_t)r0 * CR, bc, &bars[k % TMA_STAGES], stream_pol);
     };
     // Prologue, overlapped with the previous kernel under a programmatic
     // launch.  The stopping flag only goes from 0 to 1 within a solve, so a
@@ -900,18 +1038,18 @@ __global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restr
     // to chunk k + j.  No row of a colour reads a value written by another
     // row of the same colour, so the gathers of the next TMA_PD chunks are
     // in flight while chunk k is computed.
-    double gx0[TMA_PD + 1][TMA_SPL] = {}, gx1[TMA_PD + 1][TMA_SPL] = {}, gx2[TMA_PD + 1][TMA_SPL] = {};
+    double gx0[TMA_PD + 1][SPL] = {}, gx1[TMA_PD + 1][SPL] = {}, gx2[TMA_PD + 1][SPL] = {};
     double gr[TMA_PD + 1][6] = {};   // right-hand side and reciprocal diagonal of the row's node
-    auto gather = [&](int kk, double (&g0)[TMA_SPL], double (&g1)[TMA_SPL], double (&g2)[TMA_SPL],
+    auto gather = [&](int kk, double (&g0)[SPL], double (&g1)[SPL], double (&g2)[SPL],
                       double (&grr)[6]) {
         const int c = blockIdx.x + kk * gridDim.x;
         const int nrow = min(TMA_ROWS, p1 - (p0 + c * TMA_ROWS));
         const bool live = row < nrow;
-        const int *cols = reinterpret_cast<const int *>(smem + (kk % TMA_STAGES) * SB + VB) + (live ? row : 0) * CROW;
-        const int ns = live ? cols[27] : 0;
+        const int *cols = reinterpret_cast<const int *>(smem + (kk % TMA_STAGES) * SB + VB) + (live ? row : 0) * CR;
+        const int ns = live ? cols[S] : 0;
 #pragma unroll
-        for (int j = 0; j < TMA_SPL; ++j) {
-            const int sl = q + TMA_LPR * j;
+        for (int j = 0; j < SPL; ++j) {
+            const int sl = q + LPR * j;
             const bool on = sl < ns;
             const int m = on ? cols[sl] : 0;
             g0[j] = on ? ld_keep(sol + 3 * m, keep_pol) : 0.0;
@@ -924,7 +1062,7 @@ __global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restr
         grr[1] = own ? ld_keep(rhs + 3 * n + 1, keep_pol) : 0.0;
         grr[2] = own ? ld_keep(rhs + 3 * n + 2, keep_pol) : 0.0;
         if (rdiag) {
-            const double *rd = rdiag + 3 * (size_t)(p0 + c * TMA_ROWS + row);
+            const double *rd = rdiag + 3 * (size_t)(own ? p0 + c * TMA_ROWS + row : p0);
             grr[3] = own ? rd[0] : 0.0;
             grr[4] = own ? rd[1] : 0.0;
             grr[5] = own ? rd[2] : 0.0;
@@ -960,22 +1098,22 @@ __global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restr
         const int c = blockIdx.x + k * gridDim.x;
         const int nrow = min(TMA_ROWS, p1 - (p0 + c * TMA_ROWS));
         const bool live = row < nrow;
-        const T *vals = reinterpret_cast<const T *>(smem + st * SB) + (live ? row : 0) * BROW;
-        const int *cols = reinterpret_cast<const int *>(smem + st * SB + VB) + (live ? row : 0) * CROW;
-        const int ns = live ? cols[27] : 0;
+        const T *vals = reinterpret_cast<const T *>(smem + st * SB) + (live ? row : 0) * BR;
+        const int *cols = reinterpret_cast<const int *>(smem + st * SB + VB) + (live ? row : 0) * CR;
+        const int ns = live ? cols[S] : 0;
         double a0 = 0.0, a1 = 0.0, a2 = 0.0;
 #pragma unroll
-        for (int j = 0; j < TMA_SPL; ++j) {
-            const int sl = q + TMA_LPR * j;
+        for (int j = 0; j < SPL; ++j) {
+            const int sl = q + LPR * j;
             if (sl >= 1 && sl < ns) {
                 const T *b = vals + sl;
-                a0 += (double)b[0 * 27] * gx0[0][j] + (double)b[1 * 27] * gx1[0][j] + (double)b[2 * 27] * gx2[0][j];
-                a1 += (double)b[3 * 27] * gx0[0][j] + (double)b[4 * 27] * gx1[0][j] + (double)b[5 * 27] * gx2[0][j];
-                a2 += (double)b[6 * 27] * gx0[0][j] + (double)b[7 * 27] * gx1[0][j] + (double)b[8 * 27] * gx2[0][j];
+                a0 += (double)b[0 * S] * gx0[0][j] + (double)b[1 * S] * gx1[0][j] + (double)b[2 * S] * gx2[0][j];
+                a1 += (double)b[3 * S] * gx0[0][j] + (double)b[4 * S] * gx1[0][j] + (double)b[5 * S] * gx2[0][j];
+                a2 += (double)b[6 * S] * gx0[0][j] + (double)b[7 * S] * gx1[0][j] + (double)b[8 * S] * gx2[0][j];
             }
         }
 #pragma unroll
-        for (int o = 1; o < TMA_LPR; o <<= 1) {
+        for (int o = 1; o < LPR; o <<= 1) {
             a0 += __shfl_xor_sync(0xffffffffu, a0, o);
             a1 += __shfl_xor_sync(0xffffffffu, a1, o);
             a2 += __shfl_xor_sync(0xffffffffu, a2, o);
@@ -984,7 +1122,7 @@ __global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restr
             const int n = cols[0];
             double D[9];
 #pragma unroll
-            for (int qq = 0; qq < 9; ++qq) D[qq] = (double)vals[qq * 27];
+            for (int qq = 0; qq < 9; ++qq) D[qq] = (double)vals[qq * S];
             const double o0 = gx0[0][0], o1 = gx1[0][0], o2 = gx2[0][0];
             double x0 = o0, x1 = o1, x2 = o2;
             double t;
@@ -1033,7 +1171,7 @@ __global__ void __launch_bounds__(TMA_THREADS) k_sor_colour_tma(const T *__restr
 #pragma unroll
         for (int i = 0; i < TMA_PD; ++i) {
 #pragma unroll
-            for (int j = 0; j < TMA_SPL; ++j) {
+            for (int j = 0; j < SPL; ++j) {
                 gx0[i][j] = gx0[i + 1][j];
                 gx1[i][j] = gx1[i + 1][j];
                 gx2[i][j] = gx2[i + 1][j];
@@ -1115,14 +1253,15 @@ __global__ void __launch_bounds__(256) k_residual(BlockDev B, const double *__re
     const int wpb = blockDim.x >> 5;
     for (int p = blockIdx.x * wpb + (threadIdx.x >> 5); p < B.R; p += gridDim.x * wpb) {
         const int ns = B.nslot[p];
+        const int S = B.slots;
         double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        if (lane < ns) {
-            const int m = B.bcol[sidx(p, lane)];
-            const double *b = B.blk + bidx(p, lane, 0);
+        for (int sl = lane; sl < ns; sl += 32) {
+            const int m = B.bcol[B.si(p, sl)];
+            const double *b = B.blk + B.bi(p, sl, 0);
             const double x0 = x[3 * m], x1 = x[3 * m + 1], x2 = x[3 * m + 2];
-            a0 = b[0 * 27] * x0 + b[1 * 27] * x1 + b[2 * 27] * x2;
-            a1 = b[3 * 27] * x0 + b[4 * 27] * x1 + b[5 * 27] * x2;
-            a2 = b[6 * 27] * x0 + b[7 * 27] * x1 + b[8 * 27] * x2;
+            a0 += b[0 * S] * x0 + b[1 * S] * x1 + b[2 * S] * x2;
+            a1 += b[3 * S] * x0 + b[4 * S] * x1 + b[5 * S] * x2;
+            a2 += b[6 * S] * x0 + b[7 * S] * x1 + b[8 * S] * x2;
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -1165,7 +1304,7 @@ __global__ void k_rdiag(BlockDev B, double *rdiag)
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= B.R) return;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) rdiag[3 * (size_t)p + c] = 1.0 / B.blk[bidx(p, 0, 4 * c)];
+    for (int c = 0; c < 3; ++c) rdiag[3 * (size_t)p + c] = 1.0 / B.blk[B.bi(p, 0, 4 * c)];
 }
 
 // 903 test (Stif_sol.f90:183-185): first DOF whose diagonal entry is zero.
@@ -1176,7 +1315,7 @@ __global__ void k_diag_check(BlockDev B, unsigned long long *firstbad)
     const int n = B.perm[p];
 #pragma unroll
     for (int c = 0; c < 3; ++c)
-        if (B.blk[bidx(p, 0, 4 * c)] == 0.0) atomicMin(firstbad, (unsigned long long)(3 * n + c));
+        if (B.blk[B.bi(p, 0, 4 * c)] == 0.0) atomicMin(firstbad, (unsigned long long)(3 * n + c));
 }
 
 // ---------------------------------------------------------------- updates
@@ -1339,7 +1478,7 @@ __global__ void k_setpta(MeshDev Mh, int ld, int *is, int *overflow)
     int cnt = 0;
     for (int k = 0; k < Mh.ne_cnt[n]; ++k) {
         const int e = Mh.ne_elem[k * Mh.nnod + n];
-        for (int a = 0; a < 8; ++a) {
+        for (int a = 0; a < Mh.nn; ++a) {
             const int m = Mh.ln[a * Mh.nlmnt + e];
             for (int c = 0; c < 3; ++c) {
                 const int col = 3 * m + c + 1;
@@ -1367,14 +1506,14 @@ __global__ void k_to_ell(BlockDev B, const int *rowof, int nnod, int ld, const i
     const int p = rowof[n];
     const int *ir = is + (size_t)row * ld;
     double *out = ss + (size_t)row * ld;
-    out[0] = B.blk[bidx(p, 0, r * 3 + r)];
+    out[0] = B.blk[B.bi(p, 0, r * 3 + r)];
     for (int k = 1; k <= ir[0]; ++k) {
         const int col = ir[k] - 1;
         const int m = col / 3, c = col % 3;
         int slot = -1;
         for (int s = 0; s < B.nslot[p]; ++s)
-            if (B.bcol[sidx(p, s)] == m) { slot = s; break; }
-        out[k] = slot >= 0 ? B.blk[bidx(p, slot, r * 3 + c)] : 0.0;
+            if (B.bcol[B.si(p, s)] == m) { slot = s; break; }
+        out[k] = slot >= 0 ? B.blk[B.bi(p, slot, r * 3 + c)] : 0.0;
     }
     for (int k = ir[0] + 1; k < ld; ++k) out[k] = 0.0;
 }

@@ -1,0 +1,81 @@
+"""20-node, 8-Gauss-point bricks (``lt = 22``, SHAPE_22) on the sm_100a path
+against the CPU checker, through the C ABI.
+
+Rows of a 20-node brick mesh hold up to 81 node blocks, so these meshes use
+the 81-slot row layout and always run the grid-wide colour kernels.  The
+tolerances are those of the 8-node parity tests: 1e-11 relative for FP64
+state after one pass, 1e-10 after whole increments, bit-exact for integers
+(pattern, colouring, iteration counts).
+"""
+import numpy as np
+import pytest
+
+from cpfem_code_b200 import GpuSolver, abi, generator
+from oracle import OracleSolver
+
+pytestmark = pytest.mark.gpu
+LD = 256          # >= 3 x 81 columns per DOF row
+
+
+def rel(a, b):
+    s = np.abs(b).max()
+    return float(np.abs(a - b).max() / s) if s > 0 else float(np.abs(a - b).max())
+
+
+def pair(p, threads=8, mode=abi.FAS_MODE_PLAIN):
+    pg, po = p.copy(), p.copy()
+    return GpuSolver(pg, mode=mode), OracleSolver(po, 8, threads=threads), pg, po
+
+
+@pytest.mark.parametrize("n", [(1, 1, 1), (2, 2, 2), (3, 2, 2)])
+def test_pattern_and_colouring_20_node(n):
+    p = generator.structured_cube(n=n, ninc=1, seed=1, nodes=20)
+    g, o, _, _ = pair(p)
+    np.testing.assert_array_equal(g.pattern(LD), o.pattern(LD))
+    cg, ng = g.colouring()
+    co, no = o.colouring()
+    np.testing.assert_array_equal(cg, co)
+    assert ng == no
+    col = cg[p.ln - 1]
+    assert all(len(set(r)) == 20 for r in col)   # no two nodes of an element share a colour
+
+
+def test_elvals_suvals_facsls_20_node():
+    p = generator.structured_cube(n=(2, 2, 2), ninc=2, seed=3, nodes=20)
+    g, o, pg, po = pair(p)
+    for s in (g, o):
+        s.update_node()
+        s.elvals(1, 1)
+    g.download()
+    o.download()
+    assert rel(pg.fc, po.fc) < 1e-11
+    assert rel(pg.ds, po.ds) < 1e-11
+    Kg, Ko = g.stiffness(LD), o.stiffness(LD)
+    assert rel(Kg, Ko) < 1e-11
+    for s in (g, o):
+        s.suvals(1)
+    g.download()
+    o.download()
+    assert rel(pg.ddx, po.ddx) < 1e-11
+    sg, so = g.facsls(), o.facsls()
+    assert sg[0] == so[0]
+    g.download()
+    o.download()
+    assert rel(pg.ddx, po.ddx) < 1e-10
+
+
+@pytest.mark.parametrize("n,ninc", [((1, 1, 1), 2), ((2, 2, 2), 2), ((3, 3, 2), 1)])
+def test_increments_match_20_node(n, ninc):
+    p = generator.structured_cube(n=n, ninc=ninc, seed=7, nodes=20)
+    g, o, pg, po = pair(p)
+    for inc in range(1, ninc + 1):
+        rg, _ = g.increment(inc)
+        ro, _ = o.increment(inc)
+        assert [r["sor_sweeps"] for r in rg] == [r["sor_sweeps"] for r in ro]
+        assert len(rg) == len(ro)
+        g.download()
+        o.download()
+        for name in ("st", "ep", "x", "dx", "eps"):
+            assert rel(getattr(pg, name), getattr(po, name)) < 1e-10, name
+        assert rel(pg.sv[:, :15], po.sv[:, :15]) < 1e-10
+        assert abs(pg.st[:, 0].mean() - po.st[:, 0].mean()) <= 1e-10 * abs(po.st[:, 0].mean())

@@ -32,11 +32,12 @@ def _facsls_noalloc(g: GpuSolver) -> tuple[int, float]:
     return sweeps.value, err.value
 
 
-@pytest.mark.parametrize("n,mode", [((4, 4, 4), abi.FAS_MODE_PLAIN),       # one-CTA solve
-                                    ((24, 24, 24), abi.FAS_MODE_PLAIN),    # colour kernels, 15,625 nodes
-                                    ((8, 8, 8), abi.FAS_MODE_SOR_GRID)])   # colour kernels forced
-def test_facsls_noalloc_matches_facsls(n, mode):
-    p = generator.structured_cube(n=n, ninc=1, seed=7)
+@pytest.mark.parametrize("n,mode,nodes", [((4, 4, 4), abi.FAS_MODE_PLAIN, 8),      # one-CTA solve
+                                          ((24, 24, 24), abi.FAS_MODE_PLAIN, 8),   # colour kernels, 15,625 nodes
+                                          ((8, 8, 8), abi.FAS_MODE_SOR_GRID, 8),   # colour kernels forced
+                                          ((3, 3, 3), abi.FAS_MODE_PLAIN, 20)])    # 81-slot rows
+def test_facsls_noalloc_matches_facsls(n, mode, nodes):
+    p = generator.structured_cube(n=n, ninc=1, seed=7, nodes=nodes)
     g = GpuSolver(p.copy(), mode=mode)
     try:
         g.update_node()
