@@ -43,6 +43,15 @@ METRIC = "GP updates/s at 64^3 (DSTRSS evaluations per second of whole Newton it
 SOR_TRAFFIC_PER_LAUNCH = 81.1e6   # DRAM bytes per colour launch, measured with ncu at 64^3
 DESC = ("64^3 FCC Al one-point bricks (262,144 GPs, 823,875 DOF), 2^3-element grains, "
         "uniaxial tension 1e-3 per increment")
+# other workloads (--workload): (metric, description); no ncu traffic figure
+OTHER_WORKLOADS = {
+    "brick20_32": ("GP updates/s, 32^3 20-node bricks (DSTRSS evaluations per second of whole Newton iterations)",
+                   "32^3 FCC Al 20-node eight-GP bricks (262,144 GPs, 421,443 DOF), 2^3-element grains, "
+                   "uniaxial tension 1e-3 per increment"),
+    "brick20_10": ("GP updates/s, 10^3 20-node bricks (DSTRSS evaluations per second of whole Newton iterations)",
+                   "10^3 FCC Al 20-node eight-GP bricks (the reference sample's mesh: 8,000 GPs), "
+                   "one grain per element, uniaxial tension 1e-3 per increment"),
+}
 
 
 def peaks() -> dict:
@@ -404,6 +413,7 @@ def run_gpu(args):
 
 
 def main():
+    global WORKLOAD, METRIC, DESC, SOR_TRAFFIC_PER_LAUNCH
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=4)
@@ -412,7 +422,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer (e2e) leg")
     ap.add_argument("--no-tuned", action="store_true", help="skip the tuned-form (FP32 SOR) leg")
+    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, *OTHER_WORKLOADS],
+                    help="the headline 64^3 workload (default) or a 20-node brick mesh")
     args = ap.parse_args()
+    if args.workload != WORKLOAD:
+        WORKLOAD = args.workload
+        METRIC, DESC = OTHER_WORKLOADS[WORKLOAD]
+        SOR_TRAFFIC_PER_LAUNCH = None
     if args.impl == "reference":
         return run_reference(args)
     return run_gpu(args)

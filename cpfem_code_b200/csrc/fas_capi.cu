@@ -90,7 +90,7 @@ struct fas_handle {
     std::vector<double> h_tiem;
     int ninc1 = 0, nxs = 0, nfs = 0;
     // device mesh
-    DVec<int> ln, gpe, le, ib, gp_iel, ne_elem, ne_loc, ne_cnt;
+    DVec<int> ln, gpe, le, lt, ib, gp_iel, ne_elem, ne_loc, ne_cnt;
     // materials / control
     DVec<double> m_e, m_ssang, m_ab, m_an, m_ampar, m_sm;
     DevMat M{};
@@ -167,7 +167,7 @@ struct fas_handle {
     {
         MeshDev m;
         m.nlmnt = nlmnt; m.nnod = nnod; m.nn = nn; m.npg = npg;
-        m.ln = ln.p; m.gpe = gpe.p; m.le = le.p; m.ib = ib.p;
+        m.ln = ln.p; m.gpe = gpe.p; m.le = le.p; m.lt = lt.p; m.ib = ib.p;
         m.ne_elem = ne_elem.p; m.ne_loc = ne_loc.p; m.ne_cnt = ne_cnt.p;
         return m;
     }
@@ -273,7 +273,9 @@ int greedy_colouring(fas_handle *h, const std::vector<double> &xyz)
         for (int k = h->ne_ptr[n]; k < h->ne_ptr[n + 1]; ++k) {
             const int e = h->ne_list[k];
             for (int a = 0; a < h->nn; ++a) {
-                const int c = h->h_colour[h->h_ln[(size_t)e * h->nn + a]];
+                const int m = h->h_ln[(size_t)e * h->nn + a];
+                if (m < 0) break;   // end of a tie element's 2 nodes
+                const int c = h->h_colour[m];
                 if (c >= 0) {
                     if (c >= (int)used.size()) used.resize(c + 1, -1);
                     used[c] = n;
@@ -316,6 +318,7 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
             const int e = h->ne_list[k];
             for (int a = 0; a < NN; ++a) {
                 const int m = h->h_ln[(size_t)e * NN + a];
+                if (m < 0) break;
                 if (m != n && std::find(others.begin(), others.end(), m) == others.end()) others.push_back(m);
             }
         }
@@ -474,19 +477,32 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
     if (!h->point_mode) {
         if (!Md->le || !Md->lt || !Md->nd || !Md->np || !Md->ln || !Md->lg || !Md->ib) return FAS_E_ARG;
         const int ne = h->nlmnt;
-        // one element family per mesh: 8-node one-GP bricks (lt 12) or
-        // 20-node eight-GP bricks (lt 22)
-        const int lt0 = ne ? Md->lt[0] : 12;
+        // one brick family per mesh -- 8-node one-GP bricks (lt 12) or
+        // 20-node eight-GP bricks (lt 22) -- plus 2-node tie elements (lt 1-6)
+        int lt0 = 0;
+        for (int e = 0; e < ne && !lt0; ++e)
+            if (Md->lt[e] >= 9) lt0 = Md->lt[e];
         if (lt0 != 12 && lt0 != 22) return FAS_E_ELTYPE;
         h->nn = lt0 == 12 ? 8 : 20;
         h->npg = lt0 == 12 ? 1 : 8;
         const int NN = h->nn, NG = h->npg;
         if (Md->ld_ln < NN || Md->ld_lg < NG || h->nnod < 1) return FAS_E_ARG;
-        h->h_ln.resize((size_t)ne * NN);
-        h->h_gpe.resize((size_t)ne * NG);
+        h->h_ln.assign((size_t)ne * NN, -1);
+        h->h_gpe.assign((size_t)ne * NG, -1);
         h->h_le.assign(Md->le, Md->le + ne);
+        std::vector<int> h_lt(Md->lt, Md->lt + ne);
         std::vector<int> gp_seen(h->ngps, 0);
         for (int e = 0; e < ne; ++e) {
+            if (Md->lt[e] >= 1 && Md->lt[e] <= 6) {   // tie element (Elvals.f90:62-77)
+                if (Md->nd[e] != 2 || Md->np[e] != 0) return FAS_E_ARG;
+                for (int a = 0; a < 2; ++a) {
+                    const int id = Md->ln[(size_t)e * Md->ld_ln + a];
+                    if (id < 1 || id > h->nnod) return FAS_E_ARG;
+                    h->h_ln[(size_t)e * NN + a] = id - 1;
+                }
+                if (h->h_ln[(size_t)e * NN] == h->h_ln[(size_t)e * NN + 1]) return FAS_E_ARG;
+                continue;
+            }
             if (Md->lt[e] != lt0) return FAS_E_ELTYPE;
             if (Md->nd[e] != NN || Md->np[e] != NG) return FAS_E_ARG;
             for (int a = 0; a < NN; ++a) {
@@ -502,12 +518,17 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
                 h->h_gp_iel[g - 1] = Md->le[e];
             }
         }
-        if (std::abs(Md->le[ne - 1]) >= 1) h->last_mat = std::abs(Md->le[ne - 1]);
+        // mat_code the last brick leaves behind (ties run no DSTRSS)
+        for (int e = ne - 1; e >= 0; --e)
+            if (Md->lt[e] >= 9) {
+                if (std::abs(Md->le[e]) >= 1) h->last_mat = std::abs(Md->le[e]);
+                break;
+            }
         h->h_ib.assign(Md->ib, Md->ib + h->nnod);
         // node -> element CSR (ascending element ids)
         h->ne_ptr.assign(h->nnod + 1, 0);
         for (int e = 0; e < ne; ++e)
-            for (int a = 0; a < NN; ++a) h->ne_ptr[h->h_ln[(size_t)e * NN + a] + 1]++;
+            for (int a = 0; a < NN && h->h_ln[(size_t)e * NN + a] >= 0; ++a) h->ne_ptr[h->h_ln[(size_t)e * NN + a] + 1]++;
         for (int n = 0; n < h->nnod; ++n) {
             if (h->ne_ptr[n + 1] > MAXADJ) return FAS_E_RANGE;
             h->ne_ptr[n + 1] += h->ne_ptr[n];
@@ -516,7 +537,7 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
         h->ne_locl.resize(h->ne_ptr[h->nnod]);
         std::vector<int> fill(h->ne_ptr.begin(), h->ne_ptr.end() - 1);
         for (int e = 0; e < ne; ++e)
-            for (int a = 0; a < NN; ++a) {
+            for (int a = 0; a < NN && h->h_ln[(size_t)e * NN + a] >= 0; ++a) {
                 const int n = h->h_ln[(size_t)e * NN + a];
                 h->ne_list[fill[n]] = e;
                 h->ne_locl[fill[n]] = a;
@@ -543,6 +564,7 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
         CKA(h->ln.alloc(lnT.size()));
         CKA(h->gpe.alloc(gpeT.size()));
         CKA(h->le.alloc(ne));
+        CKA(h->lt.alloc(ne));
         CKA(h->ib.alloc(h->nnod));
         CKA(h->ne_elem.alloc(nee.size()));
         CKA(h->ne_loc.alloc(nel.size()));
@@ -550,6 +572,7 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
         CK(h->ln.put(lnT.data(), lnT.size(), s));
         CK(h->gpe.put(gpeT.data(), gpeT.size(), s));
         CK(h->le.put(h->h_le.data(), ne, s));
+        CK(h->lt.put(h_lt.data(), ne, s));
         CK(h->ib.put(h->h_ib.data(), h->nnod, s));
         CK(h->ne_elem.put(nee.data(), nee.size(), s));
         CK(h->ne_loc.put(nel.data(), nel.size(), s));

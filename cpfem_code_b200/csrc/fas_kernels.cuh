@@ -30,10 +30,10 @@ constexpr int SLOTS = 27;        // node blocks per row of an 8-node brick mesh
 constexpr int SLOTS20 = 81;      // node blocks per row of a 20-node brick mesh
 constexpr int MAXADJ = 8;        // elements per node
 
-// block matrix addressing: a row of S slots holds 9 S values padded to an
-// even count (16-byte rows) and S column ids plus the slot count padded to
-// a multiple of 4
-__host__ __device__ constexpr int brow_of(int S) { return (S * 9 + 1) / 2 * 2; }
+// block matrix addressing: a row of S slots holds 9 S values padded to a
+// multiple of 4 (so FP64 and FP32 rows are both 16-byte multiples, as bulk
+// copies need) and S column ids plus the slot count padded to a multiple of 4
+__host__ __device__ constexpr int brow_of(int S) { return (S * 9 + 3) / 4 * 4; }
 __host__ __device__ constexpr int crow_of(int S) { return (S + 1 + 3) / 4 * 4; }
 constexpr int BROW = brow_of(SLOTS);   // 244
 constexpr int CROW = crow_of(SLOTS);   // 28
@@ -48,6 +48,7 @@ struct MeshDev {
     const int *ln;       // [nn][nlmnt] 0-based node ids
     const int *gpe;      // [npg][nlmnt] 0-based GPs of the element
     const int *le;       // [nlmnt]
+    const int *lt;       // [nlmnt] element type: the family's (12 or 22), or 1-6 for a tie
     const int *ib;       // [nnod]
     const int *ne_elem;  // [MAXADJ][nnod] adjacent elements, ascending
     const int *ne_loc;   // [MAXADJ][nnod] local index of the node in it
@@ -80,6 +81,7 @@ __global__ void __launch_bounds__(128) k_elem(MeshDev Mh, DevMat M, DevCtrl C, D
 {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= Mh.nlmnt) return;
+    if (Mh.lt[e] < 9) return;   // tie element: no Gauss point
     const int ne = Mh.nlmnt;
     double xl[8][3], dxl[8][3];
 #pragma unroll
@@ -159,6 +161,7 @@ __global__ void __launch_bounds__(128) k_elem22(MeshDev Mh, DevMat M, DevCtrl C,
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 8LL * Mh.nlmnt) return;
     const int e = (int)(t >> 3), gq = (int)(t & 7);
+    if (Mh.lt[e] < 9) return;   // tie element: no Gauss point
     const int ne = Mh.nlmnt;
     const unsigned long long key = (unsigned long long)t << 16;
     const double *dn = dn22 + gq * 60;
@@ -283,6 +286,7 @@ __global__ void __launch_bounds__(128) k_elem_wc(MeshDev Mh, DevMat M, DevCtrl C
     const int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (e >= Mh.nlmnt) return;           // whole warps only
+    if (Mh.lt[e] < 9) return;            // tie element: no Gauss point
     const int ne = Mh.nlmnt;
     double del[6], r[3], defl;
     double *R = rec + (size_t)e * REC;
@@ -530,6 +534,23 @@ __global__ void __launch_bounds__(256) k_assemble(MeshDev Mh, BlockDev B,
         if (b == 0xFF) continue;
         const int e = Mh.ne_elem[k * Mh.nnod + n];
         const int a = Mh.ne_loc[k * Mh.nnod + n];
+        const int itp = Mh.lt[e];
+        if (itp < 9) {
+            // tie element (Elvals.f90:62-77): +efix on the tied DOFs of its
+            // first node and -efix towards the same DOFs of its second, in
+            // the first node's rows only; no force
+            if (a == 0) {
+                const double v = b == 0 ? efix : -efix;
+                if (itp <= 3) {
+                    acc[(itp - 1) * 4] = acc[(itp - 1) * 4] + v;
+                } else {
+                    const int i1 = (itp - 3) % 3, i2 = (i1 + 1) % 3;   // 0-based DOFs
+                    acc[i1 * 4] = acc[i1 * 4] + v;
+                    acc[i2 * 4] = acc[i2 * 4] + v;
+                }
+            }
+            continue;
+        }
         // the element's contribution, summed over its GPs first
         // (Elvals.f90:82-236), is added to the block in element order
         double ae[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -989,6 +1010,7 @@ __global__ void __launch_bounds__(TMA_ROWS * LPR) k_sor_colour_tma(const T *__re
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int s_pre, s_post;
     constexpr int BR = brow_of(S), CR = crow_of(S);
+    static_assert((BR * sizeof(T)) % 16 == 0 && (CR * 4) % 16 == 0, "bulk copies move 16-byte multiples");
     constexpr int SPL = (S + LPR - 1) / LPR;   // slots per lane
     constexpr int VB = TMA_ROWS * BR * (int)sizeof(T);
     constexpr int SB = tma_stage_bytes<T, S>();
@@ -1480,6 +1502,7 @@ __global__ void k_setpta(MeshDev Mh, int ld, int *is, int *overflow)
         const int e = Mh.ne_elem[k * Mh.nnod + n];
         for (int a = 0; a < Mh.nn; ++a) {
             const int m = Mh.ln[a * Mh.nlmnt + e];
+            if (m < 0) break;   // a tie element's 2 nodes end its list
             for (int c = 0; c < 3; ++c) {
                 const int col = 3 * m + c + 1;
                 if (col == row + 1) continue;

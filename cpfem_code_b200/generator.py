@@ -229,6 +229,42 @@ def setbounds(x: np.ndarray, tolerance: float, xfree: int) -> np.ndarray:
     return ib
 
 
+def setties(x: np.ndarray, ib: np.ndarray, tolerance: float, tie=(True, True, True)) -> list:
+    """SETTIES, src/prepro/fs3p-bkc.f90:316-405: tie elements for periodic
+    boundary conditions.  For every node i1 on a lower face of a tied
+    direction j1 (nodes and directions in the reference's loop order), every
+    node i2 on the opposite face with the same other two coordinates gets a
+    tie element (i1, i2) whose type follows i1's boundary class ib/100:
+    classes 1-3 tie the two directions other than j1 (lt = j1 + 3), classes
+    6/18/20, 5/16/19 and 4/15/17 tie x, y and z alone (lt 1, 2, 3); other
+    classes get none.  Returns [(i1, i2, lt)] with 1-based node ids."""
+    xyz = x.reshape(-1, 3)
+    lo, hi = xyz.min(axis=0), xyz.max(axis=0)
+    cls = ib // 100
+    out = []
+    for i1 in range(xyz.shape[0]):
+        for j1 in range(3):
+            if not (tie[j1] and abs(xyz[i1, j1] - lo[j1]) < tolerance):
+                continue
+            j2, j3 = (j1 + 1) % 3, (j1 + 2) % 3
+            far = np.nonzero((np.abs(xyz[:, j1] - hi[j1]) < tolerance)
+                             & (np.abs(xyz[i1, j2] - xyz[:, j2]) < tolerance)
+                             & (np.abs(xyz[i1, j3] - xyz[:, j3]) < tolerance))[0]
+            c = int(cls[i1])
+            if c in (1, 2, 3):
+                lt = j1 + 1 + 3
+            elif c in (6, 18, 20):
+                lt = 1
+            elif c in (5, 16, 19):
+                lt = 2
+            elif c in (4, 15, 17):
+                lt = 3
+            else:
+                continue
+            out.extend((i1 + 1, int(i2) + 1, lt) for i2 in far)
+    return out
+
+
 def setkinc(xl, xfree: int, eps_inc, ninc1: int):
     """SETKINC, src/prepro/fs3p-bkc.f90:182-308: tiem and x_spec tables.
     `eps_inc` = (e11, e22, e33) increments; components the chosen `xfree`
@@ -276,12 +312,17 @@ def structured_cube(n=(8, 8, 8), lengths=(1.0, 1.0, 1.0), xfree: int = 3,
                     materials: list[dict] | None = None, fractions=None,
                     tau0: float | list[float] = 25.0, seed: int = 0,
                     twinlim: int = 0, twinprob: float = 0.0,
-                    ctrl: Control | None = None, nodes: int = 8) -> Problem:
+                    ctrl: Control | None = None, nodes: int = 8, ties=(False, False, False),
+                    euler_gp: np.ndarray | None = None) -> Problem:
     """An nx x ny x nz brick of bricks with fs3pre's numbering, boundary
     codes, loading and per-grain random orientations (see module docstring).
 
     `nodes` = 8 gives ADDEL_8NQ's one-point bricks (``lt = 12``), 20 gives
     ADDEL_20NQ's 20-node, 8-point bricks (``lt = 22``, fs3pre.f90:241-291).
+    `euler_gp` = [ngps, 3] Euler angles per Gauss point (an ``.ori`` file,
+    see inputs.read_ori) in place of the random grain orientations.
+    `ties` = (x, y, z) faces to tie for periodic boundary conditions: SETTIES's
+    2-node tie elements follow the bricks (fs3pre.f90:171).
     `grain` = edge of the cubic grains in elements.  With several materials,
     each grain draws its material from `fractions` (fs3p-matl.f90:33-57
     draws per element; here per grain so grains stay single-phase)."""
@@ -338,10 +379,23 @@ def structured_cube(n=(8, 8, 8), lengths=(1.0, 1.0, 1.0), xfree: int = 3,
     tiem, x_spec = setkinc(lengths, xfree, eps_inc, ninc)
     nsv = 3 + int(nss.max())
     ngps = npg * nel
+    lt = np.full(nel, 12 if nodes == 8 else 22, np.int32)
+    nd = np.full(nel, nodes, np.int32)
+    npa = np.full(nel, npg, np.int32)
+    lg = np.arange(1, ngps + 1, dtype=np.int32).reshape(nel, npg)
+    le_all = le
+    tl = setties(x, ib, tolerance, ties) if any(ties) else []
+    if tl:
+        nt = len(tl)
+        t = np.array(tl, np.int32)
+        ln = np.vstack([ln, np.pad(t[:, :2], ((0, 0), (0, nodes - 2)))])
+        lt = np.concatenate([lt, t[:, 2]])
+        nd = np.concatenate([nd, np.full(nt, 2, np.int32)])
+        npa = np.concatenate([npa, np.zeros(nt, np.int32)])
+        lg = np.vstack([lg, np.zeros((nt, npg), np.int32)])
+        le_all = np.concatenate([le, np.zeros(nt, np.int32)])
     prob = Problem(
-        nlmnt=nel, nnod=nnod, ngps=ngps, le=le, lt=np.full(nel, 12 if nodes == 8 else 22, np.int32),
-        nd=np.full(nel, nodes, np.int32), np_=np.full(nel, npg, np.int32), ln=ln,
-        lg=np.arange(1, ngps + 1, dtype=np.int32).reshape(nel, npg), ib=ib,
+        nlmnt=len(lt), nnod=nnod, ngps=ngps, le=le_all, lt=lt, nd=nd, np_=npa, ln=ln, lg=lg, ib=ib,
         nss=nss, e=e, ssang=ssang, ab=ab, an=an, ampar=ampar, smatrx=smatrx,
         nmpar=6, twinlim=twinlim, twinprob=twinprob, tiem=tiem, x_spec=x_spec,
         f_spec=np.zeros((ninc, abi.XSLD, 3)), nxs=50, nfs=0,
@@ -350,6 +404,11 @@ def structured_cube(n=(8, 8, 8), lengths=(1.0, 1.0, 1.0), xfree: int = 3,
     prob.x[:] = x
     gp_grain = np.repeat(grain_id, npg)      # the element's GPs share its grain
     prob.sv[:, 0:3] = euler[gp_grain]
+    if euler_gp is not None:
+        eg = np.asarray(euler_gp, float)
+        if eg.shape != (ngps, 3):
+            raise ValueError(f"euler_gp must be [{ngps}, 3]")
+        prob.sv[:, 0:3] = eg
     t0 = np.broadcast_to(np.asarray(tau0, float), (nm,))
     gp_le = np.repeat(le, npg)
     for k in range(nm):
@@ -359,6 +418,7 @@ def structured_cube(n=(8, 8, 8), lengths=(1.0, 1.0, 1.0), xfree: int = 3,
         else:
             prob.sv[sel, 3:3 + nss[k]] = t0[k]
     prob.meta.update(dict(n=(nx, ny, nz), lengths=tuple(lengths), xfree=xfree, grain=grain, nodes=nodes,
+                          ties=len(tl),
                           seed=seed, grain_id=grain_id.astype(np.int32),
                           materials=[m["name"] for m in materials]))
     return prob
@@ -446,12 +506,12 @@ def elastic_predictor(e9: np.ndarray, euler: np.ndarray, de: np.ndarray) -> np.n
 
 # ----------------------------------------------------------------- named workloads
 def cube_config(n: int, ninc: int, grain: int, seed: int, eps: float = 1.0e-3,
-                ctrl: Control | None = None) -> Problem:
+                ctrl: Control | None = None, nodes: int = 8) -> Problem:
     """FCC aluminium n^3 cube in uniaxial tension along x ("just x faces",
     xfree = 3), strain increment `eps` per increment, grains of grain^3
-    elements with seeded uniform-SO(3) orientations."""
+    elements with seeded uniform-SO(3) orientations; `nodes` = 8 or 20."""
     return structured_cube(n=(n, n, n), xfree=3, eps_inc=(eps, 0.0, 0.0), ninc=ninc,
-                           grain=grain, seed=seed, ctrl=ctrl)
+                           grain=grain, seed=seed, ctrl=ctrl, nodes=nodes)
 
 
 def mixed_config(n: int = 32, ninc: int = 20, seed: int = 32, eps: float = 1.0e-3,
@@ -472,6 +532,10 @@ WORKLOADS = {
     "cube16": dict(n=16, ninc=20, grain=1, seed=16),
     # 64^3 FCC, grains of 2^3 elements, 50 increments to 5 %
     "cube64": dict(n=64, ninc=50, grain=2, seed=64),
+    # the reference sample's mesh: 10^3 20-node bricks, one grain per element
+    "brick20_10": dict(n=10, ninc=10, grain=1, seed=10, nodes=20),
+    # 32^3 20-node bricks (262,144 GPs), grains of 2^3 elements
+    "brick20_32": dict(n=32, ninc=50, grain=2, seed=32, nodes=20),
 }
 
 

@@ -160,3 +160,39 @@ def test_hcp_material_and_mixed_workload():
     assert (p.sv[hcp, 3:33] == z["tau0"][None, :]).all()
     assert (p.sv[~hcp, 3:15] == 25.0).all() and (p.sv[~hcp, 15:33] == 0).all()
     assert p.nsv == 33 and p.twinprob == 1.0 and p.twinlim == 1
+
+
+def _setties_literal(x, ib, tol, tie):
+    """SETTIES (fs3p-bkc.f90:316-405) as the reference's nested loops."""
+    xyz = x.reshape(-1, 3)
+    lo, hi = xyz.min(axis=0), xyz.max(axis=0)
+    out = []
+    for i1 in range(len(xyz)):
+        for j1 in range(3):
+            if tie[j1] and abs(xyz[i1, j1] - lo[j1]) < tol:
+                j2, j3 = (j1 + 1) % 3, (j1 + 2) % 3
+                for i2 in range(len(xyz)):
+                    if (abs(xyz[i2, j1] - hi[j1]) < tol and abs(xyz[i1, j2] - xyz[i2, j2]) < tol
+                            and abs(xyz[i1, j3] - xyz[i2, j3]) < tol):
+                        c = ib[i1] // 100
+                        lt = {1: j1 + 4, 2: j1 + 4, 3: j1 + 4, 6: 1, 18: 1, 20: 1,
+                              5: 2, 16: 2, 19: 2, 4: 3, 15: 3, 17: 3}.get(c)
+                        if lt:
+                            out.append((i1 + 1, i2 + 1, lt))
+    return out
+
+
+@pytest.mark.parametrize("nodes,xfree,tie", [(8, 1, (True, True, True)), (8, 3, (False, True, True)),
+                                             (20, 1, (True, False, True))])
+def test_ties_match_literal_setties(nodes, xfree, tie):
+    p = generator.structured_cube(n=(2, 3, 2), ninc=1, xfree=xfree, nodes=nodes, ties=tie)
+    nb = 12
+    x = p.x
+    tol = 0.5 * min(1 / 2, 1 / 3, 1 / 2) / (1 if nodes == 8 else 2)
+    ref = _setties_literal(x, p.ib, tol, tie)
+    assert p.nlmnt == nb + len(ref) and p.meta["ties"] == len(ref) > 0
+    t = np.array(ref)
+    np.testing.assert_array_equal(p.ln[nb:, :2], t[:, :2])
+    np.testing.assert_array_equal(p.lt[nb:], t[:, 2])
+    assert (p.nd[nb:] == 2).all() and (p.np_[nb:] == 0).all() and (p.le[nb:] == 0).all()
+    assert (p.ln[nb:, 2:] == 0).all() and (p.lg[nb:] == 0).all()
