@@ -181,8 +181,12 @@ struct fas_handle {
     }
 };
 
-// meshes with at most this many nodes run each SOR solve in one CTA
+// meshes with at most this many nodes run each SOR solve in one CTA: 8192
+// for 27-slot rows (1024 threads, a slot per lane); 512 for 81-slot rows,
+// whose three slots per lane on 256 threads make a row about 12x slower than
+// in the colour kernels, which cost about 64 us per sweep at that size
 constexpr int SOR_SMALL_ROWS = 8192;
+constexpr int SOR_SMALL_ROWS81 = 512;
 
 #define CK(expr)                                      \
     do {                                              \
@@ -390,7 +394,8 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
         // shared-memory rings let reside per SM, which also keeps the
         // per-sweep partial sums few enough for a cheap deterministic check
         const int cps = h->slots == SLOTS ? TMA_CTAS_PER_SM : tma_ctas_per_sm<SLOTS20, TMA_LPR81>();
-        h->sor_nblk[c] = (int)std::min<long long>(nblocks(h->col_start[c + 1] - h->col_start[c], TMA_ROWS),
+        const int rows = h->slots == SLOTS ? tma_rows<SLOTS>() : tma_rows<SLOTS20>();
+        h->sor_nblk[c] = (int)std::min<long long>(nblocks(h->col_start[c + 1] - h->col_start[c], rows),
                                                    (long long)h->nsm * cps);
         tot += h->sor_nblk[c];
     }
@@ -399,7 +404,7 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
     if (FAS_SOR_RCP) CKA(h->rdiag.alloc((size_t)3 * nn));
     CKA(h->d_cstart.alloc(h->ncol + 1));
     CK(h->d_cstart.put(h->col_start.data(), h->ncol + 1, s));
-    h->sor_small = nn <= SOR_SMALL_ROWS && h->slots == SLOTS;   // one slot per lane
+    h->sor_small = nn <= (h->slots == SLOTS ? SOR_SMALL_ROWS : SOR_SMALL_ROWS81);
     CK(cudaStreamSynchronize(s));
     return 0;
 }
@@ -957,7 +962,7 @@ void launch_colour_kernel(fas_handle *h, int c, bool pdl, const T *blk, const do
                 blk, h->bcol.p, p0, p1, rhs, sol, base, rdiag, ctl, part, h->sor_boff[c], h->sor_nblk_tot);
     } else {
         auto k = k_sor_colour_tma<T, SLOTS20, TMA_LPR81>;
-        const unsigned nt = tma_threads<TMA_LPR81>();
+        const unsigned nt = tma_threads<TMA_LPR81, TMA_ROWS81>();
         if (pdl)
             launch_pdl(k, h->sor_nblk[c], nt, tma_smem_bytes<T, SLOTS20>(), h->stream, blk, h->bcol.p, p0, p1,
                        rhs, sol, base, rdiag, ctl, part, h->sor_boff[c], h->sor_nblk_tot);
@@ -965,6 +970,17 @@ void launch_colour_kernel(fas_handle *h, int c, bool pdl, const T *blk, const do
             k<<<h->sor_nblk[c], nt, tma_smem_bytes<T, SLOTS20>(), h->stream>>>(
                 blk, h->bcol.p, p0, p1, rhs, sol, base, rdiag, ctl, part, h->sor_boff[c], h->sor_nblk_tot);
     }
+}
+
+// The whole solve in one CTA (meshes of at most SOR_SMALL_ROWS nodes).
+void launch_sor_small(fas_handle *h, const BlockDev &B, SorCtl *ctl, double tolerl)
+{
+    if (h->slots == SLOTS)
+        k_sor_small<1, 1024><<<1, 1024, 0, h->stream>>>(B, h->d_cstart.p, h->ncol, h->rhs.p, h->ddx.p, ctl,
+                                                         tolerl, 1000);
+    else
+        k_sor_small<3, 256><<<1, 256, 0, h->stream>>>(B, h->d_cstart.p, h->ncol, h->rhs.p, h->ddx.p, ctl,
+                                                       tolerl, 1000);
 }
 
 // One colour phase: FP64 blocks on (rhs, sol), or the FP32 copy on the
@@ -1061,7 +1077,7 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
     }
     if (small) {
         Span sp(h, &h->P.ms_sor_colour);
-        k_sor_small<<<1, 1024, 0, s>>>(B, h->d_cstart.p, h->ncol, h->rhs.p, h->ddx.p, h->sorctl.p, tolerl, 1000);
+        launch_sor_small(h, B, h->sorctl.p, tolerl);
         sp.end();
         keep(h, sp);
         LAUNCHED(h);
@@ -1596,7 +1612,7 @@ int facsls_noalloc_impl(fas_handle *h, int *sweeps, double *error)
     if (h->hc->ekey[1] != ~0ull) return 903;
     const double tolerl = h->C.toler * h->C.toler;
     if (h->sor_small && !(h->mode & FAS_MODE_SOR_GRID)) {
-        k_sor_small<<<1, 1024, 0, s>>>(B, h->d_cstart.p, h->ncol, h->rhs.p, h->ddx.p, ctl, tolerl, 1000);
+        launch_sor_small(h, B, ctl, tolerl);
         LAUNCHED(h);
     } else {
         int done = 0, chunk = 4;

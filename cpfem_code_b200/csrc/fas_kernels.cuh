@@ -831,6 +831,96 @@ __device__ __forceinline__ void sor_rows(const BlockDev &B, const T *__restrict_
     }
 }
 
+// The same warp-per-row update for rows of more than 32 slots: lane l holds
+// slots l, l + 32, ... (K per lane); lane 0's first slot is the diagonal.
+template <int K> struct RowOpsK {
+    int ns, n;
+    double b[K][9];
+    double x0[K], x1[K], x2[K];
+    double r0, r1, r2;
+};
+
+template <typename T, int K>
+__device__ __forceinline__ void load_row_k(const BlockDev &B, const T *__restrict__ blk, int p, int lane,
+                                           const double *__restrict__ rhs, const double *sol, RowOpsK<K> &o)
+{
+    o.ns = B.nslot[p];
+    int m0 = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int sl = lane + 32 * k;
+        const bool on = sl < o.ns;
+        const int m = on ? __ldcs(B.bcol + B.si(p, sl)) : 0;
+        if (k == 0) m0 = m;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) o.b[k][q] = on ? ld_stream(blk + B.bi(p, sl, q)) : 0.0;
+        o.x0[k] = on ? sol[3 * m] : 0.0;
+        o.x1[k] = on ? sol[3 * m + 1] : 0.0;
+        o.x2[k] = on ? sol[3 * m + 2] : 0.0;
+    }
+    o.n = __shfl_sync(0xffffffffu, m0, 0);
+    if (lane == 0) {
+        o.r0 = rhs[3 * m0];
+        o.r1 = rhs[3 * m0 + 1];
+        o.r2 = rhs[3 * m0 + 2];
+    }
+}
+
+template <int K>
+__device__ __forceinline__ void sor_update_k(const RowOpsK<K> &o, int lane, double *sol,
+                                             const double *__restrict__ base, double &dv, double &vv)
+{
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        if (lane + 32 * k >= 1) {
+            a0 += o.b[k][0] * o.x0[k] + o.b[k][1] * o.x1[k] + o.b[k][2] * o.x2[k];
+            a1 += o.b[k][3] * o.x0[k] + o.b[k][4] * o.x1[k] + o.b[k][5] * o.x2[k];
+            a2 += o.b[k][6] * o.x0[k] + o.b[k][7] * o.x1[k] + o.b[k][8] * o.x2[k];
+        }
+    }
+#pragma unroll
+    for (int k = 16; k > 0; k >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, k);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, k);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, k);
+    }
+    if (lane == 0) {
+        const double *D = o.b[0];
+        const int n = o.n;
+        double x0 = o.x0[0], x1 = o.x1[0], x2 = o.x2[0];
+        double t = (o.r0 - (a0 + D[1] * x1 + D[2] * x2)) / D[0];
+        x0 = x0 + 1.2 * (t - x0);
+        t = (o.r1 - (a1 + D[3] * x0 + D[5] * x2)) / D[4];
+        x1 = x1 + 1.2 * (t - x1);
+        t = (o.r2 - (a2 + D[6] * x0 + D[7] * x1)) / D[8];
+        x2 = x2 + 1.2 * (t - x2);
+        sol[3 * n] = x0;
+        sol[3 * n + 1] = x1;
+        sol[3 * n + 2] = x2;
+        dv += (x0 - o.x0[0]) * (x0 - o.x0[0]) + (x1 - o.x1[0]) * (x1 - o.x1[0]) + (x2 - o.x2[0]) * (x2 - o.x2[0]);
+        if (base) {
+            x0 += base[3 * n];
+            x1 += base[3 * n + 1];
+            x2 += base[3 * n + 2];
+        }
+        vv += x0 * x0 + x1 * x1 + x2 * x2;
+    }
+}
+
+template <typename T, int K>
+__device__ __forceinline__ void sor_rows_k(const BlockDev &B, const T *__restrict__ blk, int p, int p1,
+                                           int stride, int lane, const double *__restrict__ rhs,
+                                           double *sol, const double *__restrict__ base, double &dv,
+                                           double &vv)
+{
+    for (; p < p1; p += stride) {
+        RowOpsK<K> o;
+        load_row_k<T, K>(B, blk, p, lane, rhs, sol, o);
+        sor_update_k<K>(o, lane, sol, base, dv, vv);
+    }
+}
+
 // ---------------------------------------------------------------- bulk-copy SOR
 // Shared-memory staging of block rows with the bulk-copy (TMA) engine:
 // cp.async.bulk global -> shared, completion counted on an mbarrier.
@@ -952,18 +1042,27 @@ __device__ __forceinline__ void sweep_test(const double *part, int nblk, SorCtl 
 #endif
 constexpr int TMA_ROWS = FAS_TMA_ROWS;       // rows per chunk
 constexpr int TMA_LPR = FAS_TMA_LPR;         // lanes per row of 27-slot rows (a power of two, at most 32)
-constexpr int TMA_LPR81 = 16;                // lanes per row of 81-slot rows
+#ifndef FAS_TMA_LPR81
+#define FAS_TMA_LPR81 16
+#endif
+#ifndef FAS_TMA_ROWS81
+#define FAS_TMA_ROWS81 8
+#endif
+constexpr int TMA_LPR81 = FAS_TMA_LPR81;     // lanes per row of 81-slot rows
+constexpr int TMA_ROWS81 = FAS_TMA_ROWS81;   // rows per chunk of 81-slot rows
 constexpr int TMA_STAGES = FAS_TMA_STAGES;   // chunks in flight per CTA
 constexpr int TMA_PD = FAS_TMA_PD;           // chunks whose gathers run ahead of the computed one
 static_assert(TMA_PD >= 1 && TMA_PD < TMA_STAGES, "gathers run ahead within the ring");
-template <int LPR> __host__ __device__ constexpr int tma_threads() { return TMA_ROWS * LPR; }
+template <int LPR, int ROWS = TMA_ROWS> __host__ __device__ constexpr int tma_threads() { return ROWS * LPR; }
 constexpr int TMA_THREADS = tma_threads<TMA_LPR>();
 static_assert(TMA_LPR >= 1 && TMA_LPR <= 32 && (TMA_LPR & (TMA_LPR - 1)) == 0, "lanes per row");
-static_assert(TMA_THREADS % 32 == 0 && tma_threads<TMA_LPR81>() % 32 == 0, "whole warps per CTA");
+static_assert(TMA_THREADS % 32 == 0 && tma_threads<TMA_LPR81, TMA_ROWS81>() % 32 == 0, "whole warps per CTA");
 
+// rows per chunk of the S-slot layout
+template <int S> __host__ __device__ constexpr int tma_rows() { return S == SLOTS ? TMA_ROWS : TMA_ROWS81; }
 template <typename T, int S = SLOTS> __host__ __device__ constexpr int tma_stage_bytes()
 {
-    return TMA_ROWS * brow_of(S) * (int)sizeof(T) + TMA_ROWS * crow_of(S) * 4;
+    return tma_rows<S>() * brow_of(S) * (int)sizeof(T) + tma_rows<S>() * crow_of(S) * 4;
 }
 // the ring, its mbarriers and a 512-byte guard: lanes whose slots lie past
 // the row (q + LPR j >= S) skip their reads, and the guard keeps even a
@@ -977,9 +1076,9 @@ template <typename T, int S = SLOTS> __host__ __device__ constexpr int tma_smem_
 // to fill them.
 template <int S, int LPR> __host__ __device__ constexpr int tma_ctas_per_sm()
 {
-    return (228 * 1024) / (tma_smem_bytes<double, S>() + 1024) < 32 / (tma_threads<LPR>() / 32)
+    return (228 * 1024) / (tma_smem_bytes<double, S>() + 1024) < 32 / (tma_threads<LPR, tma_rows<S>()>() / 32)
                ? (228 * 1024) / (tma_smem_bytes<double, S>() + 1024)
-               : 32 / (tma_threads<LPR>() / 32);
+               : 32 / (tma_threads<LPR, tma_rows<S>()>() / 32);
 }
 constexpr int TMA_CTAS_PER_SM = tma_ctas_per_sm<SLOTS, TMA_LPR>();
 static_assert(TMA_CTAS_PER_SM >= 1 && tma_ctas_per_sm<SLOTS20, TMA_LPR81>() >= 1,
@@ -1000,7 +1099,7 @@ static_assert(TMA_CTAS_PER_SM >= 1 && tma_ctas_per_sm<SLOTS20, TMA_LPR81>() >= 1
 // wait is bounded; on a timeout the CTA waits (bounded) for its own copies
 // still in flight, raises ctl->fault and leaves.
 template <typename T, int S, int LPR>
-__global__ void __launch_bounds__(TMA_ROWS * LPR) k_sor_colour_tma(const T *__restrict__ blk,
+__global__ void __launch_bounds__(tma_rows<S>() * LPR) k_sor_colour_tma(const T *__restrict__ blk,
                                                                 const int *__restrict__ bcol, int p0, int p1,
                                                                 const double *__restrict__ rhs, double *sol,
                                                                 const double *__restrict__ base,
@@ -1012,20 +1111,21 @@ __global__ void __launch_bounds__(TMA_ROWS * LPR) k_sor_colour_tma(const T *__re
     constexpr int BR = brow_of(S), CR = crow_of(S);
     static_assert((BR * sizeof(T)) % 16 == 0 && (CR * 4) % 16 == 0, "bulk copies move 16-byte multiples");
     constexpr int SPL = (S + LPR - 1) / LPR;   // slots per lane
-    constexpr int VB = TMA_ROWS * BR * (int)sizeof(T);
+    constexpr int ROWS = tma_rows<S>();
+    constexpr int VB = ROWS * BR * (int)sizeof(T);
     constexpr int SB = tma_stage_bytes<T, S>();
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TMA_STAGES * SB);
     const int lane = threadIdx.x & 31;
     const int row = threadIdx.x / LPR;   // row of the chunk served by this group
     const int q = threadIdx.x % LPR;     // lane within the group
-    const int nchunks = (p1 - p0 + TMA_ROWS - 1) / TMA_ROWS;
+    const int nchunks = (p1 - p0 + ROWS - 1) / ROWS;
     const int myn = (int)blockIdx.x < nchunks ? (nchunks - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     const uint64_t stream_pol = l2_evict_first();
     const uint64_t keep_pol = l2_evict_last();
     auto issue = [&](int k) {
         const int c = blockIdx.x + k * gridDim.x;
-        const int r0 = p0 + c * TMA_ROWS;
-        const int nr = min(TMA_ROWS, p1 - r0);
+        const int r0 = p0 + c * ROWS;
+        const int nr = min(ROWS, p1 - r0);
         unsigned char *st = smem + (k % TMA_STAGES) * SB;
         const unsigned bv = (unsigned)(nr * BR * sizeof(T)), bc = (unsigned)(nr * CR * 4);
         mbar_expect_tx(&bars[k % TMA_STAGES], bv + bc);
@@ -1065,7 +1165,7 @@ __global__ void __launch_bounds__(TMA_ROWS * LPR) k_sor_colour_tma(const T *__re
     auto gather = [&](int kk, double (&g0)[SPL], double (&g1)[SPL], double (&g2)[SPL],
                       double (&grr)[6]) {
         const int c = blockIdx.x + kk * gridDim.x;
-        const int nrow = min(TMA_ROWS, p1 - (p0 + c * TMA_ROWS));
+        const int nrow = min(ROWS, p1 - (p0 + c * ROWS));
         const bool live = row < nrow;
         const int *cols = reinterpret_cast<const int *>(smem + (kk % TMA_STAGES) * SB + VB) + (live ? row : 0) * CR;
         const int ns = live ? cols[S] : 0;
@@ -1084,7 +1184,7 @@ __global__ void __launch_bounds__(TMA_ROWS * LPR) k_sor_colour_tma(const T *__re
         grr[1] = own ? ld_keep(rhs + 3 * n + 1, keep_pol) : 0.0;
         grr[2] = own ? ld_keep(rhs + 3 * n + 2, keep_pol) : 0.0;
         if (rdiag) {
-            const double *rd = rdiag + 3 * (size_t)(own ? p0 + c * TMA_ROWS + row : p0);
+            const double *rd = rdiag + 3 * (size_t)(own ? p0 + c * ROWS + row : p0);
             grr[3] = own ? rd[0] : 0.0;
             grr[4] = own ? rd[1] : 0.0;
             grr[5] = own ? rd[2] : 0.0;
@@ -1118,7 +1218,7 @@ __global__ void __launch_bounds__(TMA_ROWS * LPR) k_sor_colour_tma(const T *__re
         }
         const int st = k % TMA_STAGES;
         const int c = blockIdx.x + k * gridDim.x;
-        const int nrow = min(TMA_ROWS, p1 - (p0 + c * TMA_ROWS));
+        const int nrow = min(ROWS, p1 - (p0 + c * ROWS));
         const bool live = row < nrow;
         const T *vals = reinterpret_cast<const T *>(smem + st * SB) + (live ? row : 0) * BR;
         const int *cols = reinterpret_cast<const int *>(smem + st * SB + VB) + (live ? row : 0) * CR;
@@ -1220,10 +1320,12 @@ __global__ void __launch_bounds__(TMA_ROWS * LPR) k_sor_colour_tma(const T *__re
 // point update as k_sor_colour_tma, colours separated by __syncthreads, and the
 // stopping test (Stif_sol.f90:206-210) evaluated in-block after every sweep.
 // Bounded by maxitl sweeps.  cstart[c] .. cstart[c+1] are the colour ranges.
-__global__ void __launch_bounds__(1024) k_sor_small(BlockDev B, const int *__restrict__ cstart,
-                                                    int ncol, const double *__restrict__ rhs,
-                                                    double *sol, SorCtl *ctl, double tolerl,
-                                                    int maxitl)
+// K = slots per lane (1: rows of at most 32 slots, 3: up to 96), NT threads.
+template <int K, int NT>
+__global__ void __launch_bounds__(NT) k_sor_small(BlockDev B, const int *__restrict__ cstart,
+                                                  int ncol, const double *__restrict__ rhs,
+                                                  double *sol, SorCtl *ctl, double tolerl,
+                                                  int maxitl)
 {
     __shared__ double red[2][32];
     __shared__ int s_conv;
@@ -1236,7 +1338,10 @@ __global__ void __launch_bounds__(1024) k_sor_small(BlockDev B, const int *__res
         double v0 = 0.0, v1 = 0.0;
         for (int c = 0; c < ncol; ++c) {
             const int p1 = cstart[c + 1];
-            sor_rows<double>(B, B.blk, cstart[c] + wid, p1, nw, lane, rhs, sol, nullptr, v0, v1);
+            if (K == 1)
+                sor_rows<double>(B, B.blk, cstart[c] + wid, p1, nw, lane, rhs, sol, nullptr, v0, v1);
+            else
+                sor_rows_k<double, K>(B, B.blk, cstart[c] + wid, p1, nw, lane, rhs, sol, nullptr, v0, v1);
             __syncthreads();   // the next colour reads this colour's values
         }
         if (lane == 0) {

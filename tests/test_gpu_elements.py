@@ -2,7 +2,8 @@
 against the CPU checker, through the C ABI.
 
 Rows of a 20-node brick mesh hold up to 81 node blocks, so these meshes use
-the 81-slot row layout and always run the grid-wide colour kernels.  The
+the 81-slot row layout; small meshes solve in one CTA (three slots per
+lane), FAS_MODE_SOR_GRID forces the 81-slot colour kernels.  The
 tolerances are those of the 8-node parity tests: 1e-11 relative for FP64
 state after one pass, 1e-10 after whole increments, bit-exact for integers
 (pattern, colouring, iteration counts).
@@ -64,10 +65,14 @@ def test_elvals_suvals_facsls_20_node():
     assert rel(pg.ddx, po.ddx) < 1e-10
 
 
-@pytest.mark.parametrize("n,ninc", [((1, 1, 1), 2), ((2, 2, 2), 2), ((3, 3, 2), 1)])
-def test_increments_match_20_node(n, ninc):
+@pytest.mark.parametrize("n,ninc,mode", [((1, 1, 1), 2, abi.FAS_MODE_PLAIN),      # one-CTA solve
+                                         ((2, 2, 2), 2, abi.FAS_MODE_PLAIN),
+                                         ((3, 3, 2), 1, abi.FAS_MODE_PLAIN),
+                                         ((2, 2, 2), 2, abi.FAS_MODE_SOR_GRID),   # 81-slot colour kernels
+                                         ((3, 3, 2), 1, abi.FAS_MODE_SOR_GRID)])
+def test_increments_match_20_node(n, ninc, mode):
     p = generator.structured_cube(n=n, ninc=ninc, seed=7, nodes=20)
-    g, o, pg, po = pair(p)
+    g, o, pg, po = pair(p, mode=mode)
     for inc in range(1, ninc + 1):
         rg, _ = g.increment(inc)
         ro, _ = o.increment(inc)
@@ -107,7 +112,7 @@ def test_fp32_sor_refinement_20_node():
     81-slot rows: FP32 rows are bulk-copied like FP64 rows; the stress stays
     within the stated error of the FP64 checker."""
     p = generator.structured_cube(n=(3, 3, 2), ninc=1, seed=5, nodes=20)
-    g, o, pg, po = pair(p, mode=abi.FAS_MODE_SOR_FP32)
+    g, o, pg, po = pair(p, mode=abi.FAS_MODE_SOR_GRID | abi.FAS_MODE_SOR_FP32)
     g.increment(1)
     o.increment(1)
     g.download()

@@ -35,7 +35,8 @@ def _facsls_noalloc(g: GpuSolver) -> tuple[int, float]:
 @pytest.mark.parametrize("n,mode,nodes", [((4, 4, 4), abi.FAS_MODE_PLAIN, 8),      # one-CTA solve
                                           ((24, 24, 24), abi.FAS_MODE_PLAIN, 8),   # colour kernels, 15,625 nodes
                                           ((8, 8, 8), abi.FAS_MODE_SOR_GRID, 8),   # colour kernels forced
-                                          ((3, 3, 3), abi.FAS_MODE_PLAIN, 20)])    # 81-slot rows
+                                          ((3, 3, 3), abi.FAS_MODE_PLAIN, 20),     # 81-slot rows, one CTA
+                                          ((3, 3, 3), abi.FAS_MODE_SOR_GRID, 20)]) # 81-slot colour kernels
 def test_facsls_noalloc_matches_facsls(n, mode, nodes):
     p = generator.structured_cube(n=n, ninc=1, seed=7, nodes=nodes)
     g = GpuSolver(p.copy(), mode=mode)
