@@ -107,6 +107,37 @@ __device__ __forceinline__ void lu_solve(int n, const double *w, double *x)
     }
 }
 
+// The same factorisation and solve for an n x n matrix stored with row
+// stride n (the active-set matrices: only nsa x nsa of them are live, and a
+// packed copy touches far fewer cache lines than a fixed stride).
+__device__ __forceinline__ int lu_factor_n(int n, double *w)
+{
+    for (int k = 0; k < n - 1; ++k) {
+        const double pk = w[k * n + k];
+        if (pk == 0.0) return 1;
+        for (int i = k + 1; i < n; ++i) {
+            const double l = w[i * n + k] / pk;
+            w[i * n + k] = l;
+            for (int j = k + 1; j < n; ++j) w[i * n + j] = w[i * n + j] - l * w[k * n + j];
+        }
+    }
+    return w[(n - 1) * n + (n - 1)] == 0.0 ? 1 : 0;
+}
+__device__ __forceinline__ void lu_solve_n(int n, const double *w, double *x)
+{
+    for (int i = 1; i < n; ++i) {
+        double xi = x[i];
+        for (int j = 0; j < i; ++j) xi = xi - w[i * n + j] * x[j];
+        x[i] = xi;
+    }
+    x[n - 1] = x[n - 1] / w[(n - 1) * n + (n - 1)];
+    for (int i = n - 2; i >= 0; --i) {
+        double xi = x[i];
+        for (int j = i + 1; j < n; ++j) xi = xi - w[i * n + j] * x[j];
+        x[i] = xi / w[i * n + i];
+    }
+}
+
 // CTMATRX, src/fasolt/crys_math.f90:25-62 (a[i][j] = a(i+1,j+1)).
 __device__ __forceinline__ void ctmatrx(double ph1, double phi, double ph2, double a[3][3],
                                         double aug[3])
@@ -360,10 +391,21 @@ __device__ __forceinline__ void btmatrx(const DevMat &M, const double a[3][3], C
     }
 }
 
+// x^y with the two exponents hardening laws use most taken exactly: x^0 = 1
+// (A6 = 0: a rate-independent saturation stress) and x^1 = x (A4 = 1: Voce).
+__device__ __forceinline__ double pow_exact01(double x, double y)
+{
+    if (y == 0.0) return 1.0;
+    if (y == 1.0) return x;
+    return pow(x, y);
+}
+
 // PLASTC, src/fasolt/ela-plas.f90:110-201: s1 and the log-hardening matrix
-// of the active systems (ah(i,j) = sgn(gam_j) h_ij / s1_i).
+// of the active systems (ah(i,j) = sgn(gam_j) h_ij / s1_i).  Kept out of
+// line: SLPFTA calls it in and after its loop, and one copy of its code
+// spares the instruction cache.
 template <int NS>
-__device__ __forceinline__ void plastc(const DevMat &M, CpScratch<NS> &w, double dt)
+__device__ __noinline__ void plastc(const DevMat &M, CpScratch<NS> &w, double dt)
 {
     const int ns = w.ns;
     const double *amp = M.ampar + (size_t)w.mc * MAXSS * 6;
@@ -372,11 +414,11 @@ __device__ __forceinline__ void plastc(const DevMat &M, CpScratch<NS> &w, double
     for (int i = 0; i < ns; ++i) sumss = sumss + fabs(w.gam[i]);
     double gradh[NS];
     for (int i = 0; i < ns; ++i) {
-        const double sst = ld_ro(amp + 6 * i + 4) * pow(sumss / dt, ld_ro(amp + 6 * i + 5));
+        const double sst = ld_ro(amp + 6 * i + 4) * pow_exact01(sumss / dt, ld_ro(amp + 6 * i + 5));
         double arg = (sst != 0.0) ? 1.0 - (w.s0[i] / sst) : 0.0;
         if (arg < 0.0) arg = 0.0;
         gradh[i] = ld_ro(amp + 6 * i + 2) +
-                   ld_ro(amp + 6 * i + 1) * copysign(pow(fabs(arg), ld_ro(amp + 6 * i + 3)), arg);
+                   ld_ro(amp + 6 * i + 1) * copysign(pow_exact01(fabs(arg), ld_ro(amp + 6 * i + 3)), arg);
     }
     for (int i = 0; i < ns; ++i) {
         double s = w.s0[i];
@@ -389,7 +431,7 @@ __device__ __forceinline__ void plastc(const DevMat &M, CpScratch<NS> &w, double
         for (int j = 0; j < w.nsa; ++j) {
             const int js = w.isa[j];
             const double g = w.gam[js];
-            w.ah[i * NS + j] = fabs(g) > 1.e-14
+            w.ah[i * w.nsa + j] = fabs(g) > 1.e-14
                                    ? (copysign(1.0, g) * (ld_ro(sm + is * ns + js) * gradh[js])) / inv_s1
                                    : 0.0;
         }
@@ -481,10 +523,10 @@ __device__ __forceinline__ int slpfta(const DevMat &M, CpScratch<NS> &w, const D
         plastc(M, w, dt);
         for (int i = 0; i < n; ++i) {
             const double gamn = w.gam[w.isa[i]];
-            for (int j = 0; j < n; ++j) w.ah[j * NS + i] = gamn * w.ah[j * NS + i];
-            w.ah[i * NS + i] = w.ah[i * NS + i] + w.am[w.isa[i]];
+            for (int j = 0; j < n; ++j) w.ah[j * n + i] = gamn * w.ah[j * n + i];
+            w.ah[i * n + i] = w.ah[i * n + i] + w.am[w.isa[i]];
         }
-        if (lu_factor<NS>(n, w.ah)) { ninner = iter; return 910; }
+        if (lu_factor_n(n, w.ah)) { ninner = iter; return 910; }
         for (int i = 0; i < n; ++i) {
             const int ii = w.isa[i];
             const double taufg = w.s1[ii] * spower(w.gam[ii] / dt, w.am[ii]);
@@ -493,7 +535,7 @@ __device__ __forceinline__ int slpfta(const DevMat &M, CpScratch<NS> &w, const D
         tauerr = 0.0;
         for (int i = 0; i < n; ++i) tauerr = tauerr + errtau[i] * errtau[i];
         tauerr = sqrt(tauerr);
-        lu_solve<NS>(n, w.ah, errtau);
+        lu_solve_n(n, w.ah, errtau);
         double errmax = 0.0;
         for (int i = 0; i < n; ++i)
             if (fabs(errtau[i]) > errmax) errmax = fabs(errtau[i]);
@@ -509,9 +551,9 @@ __device__ __forceinline__ int slpfta(const DevMat &M, CpScratch<NS> &w, const D
     plastc(M, w, dt);
     for (int i = 0; i < n; ++i) {
         const int ii = w.isa[i];
-        for (int j = 0; j < n; ++j) w.ah[j * NS + i] = w.tau[w.isa[j]] * w.ah[j * NS + i];
+        for (int j = 0; j < n; ++j) w.ah[j * n + i] = w.tau[w.isa[j]] * w.ah[j * n + i];
         const double g = w.gam[ii];
-        w.ah[i * NS + i] = w.ah[i * NS + i] +
+        w.ah[i * n + i] = w.ah[i * n + i] +
                            (fabs(g) > 1.e-12 ? w.am[ii] * w.tau[ii] / g : w.am[ii] / 1.e-12);
     }
     return 0;
@@ -610,12 +652,12 @@ __device__ int dstrss(const DevMat &M, const DevCtrl &C, const DevGp &G, int g, 
                 erreps[k] = de[k] - epl[k] - acc;
             }
             const int n = w.nsa;
-            if (lu_factor<NS>(n, w.ah)) { rc = 910; break; }
+            if (lu_factor_n(n, w.ah)) { rc = 910; break; }
             // djac = b_a X^-1 b_a^T: one solve per column j
             for (int j = 0; j < 6; ++j) {
                 double wk[NS];
                 for (int k = 0; k < n; ++k) wk[k] = w.b[w.isa[k]][j];
-                lu_solve<NS>(n, w.ah, wk);
+                lu_solve_n(n, w.ah, wk);
                 for (int i = 0; i < 6; ++i) {
                     double sum = 0.0;
                     for (int k = 0; k < n; ++k) sum = sum + w.b[w.isa[k]][i] * wk[k];

@@ -170,10 +170,10 @@ __device__ __forceinline__ void plastc_sys(Sys &y, const double *smrow, int ns, 
     const double sumss = wsum(y.on ? fabs(y.gam) : 0.0);
     double gh = 0.0;
     if (y.on) {
-        const double sst = y.A5 * pow(sumss / dt, y.A6);
+        const double sst = y.A5 * pow_exact01(sumss / dt, y.A6);
         double arg = (sst != 0.0) ? 1.0 - (y.s0 / sst) : 0.0;
         if (arg < 0.0) arg = 0.0;
-        gh = y.A3 + y.A2 * copysign(pow(fabs(arg), y.A4), arg);
+        gh = y.A3 + y.A2 * copysign(pow_exact01(fabs(arg), y.A4), arg);
     }
     y.gradh = gh;
     double s = y.s0;
