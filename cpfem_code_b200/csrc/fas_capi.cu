@@ -26,6 +26,10 @@ using namespace fasdev;
 #ifndef FAS_SOR_RCP
 #define FAS_SOR_RCP 1
 #endif
+// Constitutive kernels launched in work-sorted order (1) or natural order (0).
+#ifndef FAS_WORK_SORT
+#define FAS_WORK_SORT 1
+#endif
 
 namespace {
 
@@ -114,6 +118,7 @@ struct fas_handle {
     DVec<float> blk32;           // FP32 copy for FAS_MODE_SOR_FP32
     DVec<double> sor_d, sor_r;   // correction and residual of the refinement
     DVec<double> rdiag;          // reciprocals of the diagonal entries, row order
+    DVec<int> work_order, work_hist;   // work-sorted constitutive launch order
     int refine_every = 16;       // FP32 sweeps per FP64 residual
     cudaGraphExec_t sor_graph = nullptr;   // GRAPH_SWEEPS plain sweeps
     cudaGraphExec_t sor32_graph = nullptr; // one refinement cycle of the FP32 form
@@ -828,6 +833,25 @@ int download_impl(fas_handle *h, const fas_state_desc *S)
 }
 
 // ---------------------------------------------------------------- phases
+// The work-sorted order of n items (elements whose GP is gp_of[i], or points
+// when gp_of is null), from the operation counts of their last update; null
+// when sorting is off.
+const int *work_order(fas_handle *h, int n, const int *gp_of)
+{
+    if (!FAS_WORK_SORT || n <= 0) return nullptr;
+    if ((int)h->work_order.n < n) {
+        if (h->work_order.alloc(n) != cudaSuccess) return nullptr;
+    }
+    if (!h->work_hist.p && h->work_hist.alloc(WORK_BINS) != cudaSuccess) return nullptr;
+    cudaStream_t s = h->stream;
+    if (cudaMemsetAsync(h->work_hist.p, 0, WORK_BINS * sizeof(int), s) != cudaSuccess) return nullptr;
+    k_work_hist<<<nblocks(n, 256), 256, 0, s>>>(n, gp_of, h->ops.p, h->work_hist.p);
+    k_work_scan<<<1, WORK_BINS, 0, s>>>(h->work_hist.p);
+    k_work_scatter<<<nblocks(n, 256), 256, 0, s>>>(n, gp_of, h->ops.p, h->work_hist.p, h->work_order.p);
+    h->launches += 3;
+    return h->work_order.p;
+}
+
 template <int NS> int launch_elem(fas_handle *h, int inc, int nit)
 {
     Span sp(h, &h->P.ms_constitutive);
@@ -835,9 +859,12 @@ template <int NS> int launch_elem(fas_handle *h, int inc, int nit)
         k_elem22<NS><<<nblocks(8LL * h->nlmnt, 128), 128, 0, h->stream>>>(
             h->mesh(), h->M, h->C, h->gp(), h->dn22.p, h->x.p, h->dx.p, h->rec.p, h->h_tiem[inc - 1], inc, nit,
             h->ekey.p);
-    else if (!(h->mode & FAS_MODE_CP_WARP))
+    else if (!(h->mode & FAS_MODE_CP_WARP)) {
+        const int *order = work_order(h, h->nlmnt, h->gpe.p);
         k_elem<NS><<<nblocks(h->nlmnt, 128), 128, 0, h->stream>>>(
-            h->mesh(), h->M, h->C, h->gp(), h->x.p, h->dx.p, h->rec.p, h->h_tiem[inc - 1], inc, nit, h->ekey.p);
+            h->mesh(), h->M, h->C, h->gp(), h->x.p, h->dx.p, h->rec.p, h->h_tiem[inc - 1], inc, nit, h->ekey.p,
+            order);
+    }
     else
         k_elem_wc<(NS > 12 ? 32 : 12)><<<nblocks(32LL * h->nlmnt, 128), 128, 0, h->stream>>>(
             h->mesh(), h->M, h->C, h->gp(), h->x.p, h->dx.p, h->rec.p, h->h_tiem[inc - 1], inc, nit, h->ekey.p);
@@ -1440,16 +1467,17 @@ int32_t fas_gpu_constitutive(fas_handle *h, int32_t inc, int32_t nit)
     const unsigned nb = nblocks(h->ngps, 128);
     const unsigned nbw = nblocks(32LL * h->ngps, 128);
     const bool thr = !(h->mode & FAS_MODE_CP_WARP) || h->maxns > 32;
+    const int *order = thr ? work_order(h, h->ngps, nullptr) : nullptr;
     switch (h->ns_tmpl) {
     case 12:
-        if (thr) k_points<12><<<nb, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p);
+        if (thr) k_points<12><<<nb, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order);
         else k_points_wc<12><<<nbw, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p);
         break;
     case 32:
-        if (thr) k_points<32><<<nb, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p);
+        if (thr) k_points<32><<<nb, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order);
         else k_points_wc<32><<<nbw, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p);
         break;
-    default: k_points<60><<<nb, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p); break;
+    default: k_points<60><<<nb, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order); break;
     }
     sp.end();
     keep(h, sp);

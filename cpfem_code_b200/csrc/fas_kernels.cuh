@@ -77,10 +77,11 @@ __global__ void __launch_bounds__(128) k_elem(MeshDev Mh, DevMat M, DevCtrl C, D
                                               const double *__restrict__ x,
                                               const double *__restrict__ dx, double *rec,
                                               double dt, int inc, int nit,
-                                              unsigned long long *errkey)
+                                              unsigned long long *errkey, const int *__restrict__ order)
 {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= Mh.nlmnt) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= Mh.nlmnt) return;
+    const int e = order ? order[t] : t;   // work-sorted element order, or the natural one
     if (Mh.lt[e] < 9) return;   // tie element: no Gauss point
     const int ne = Mh.nlmnt;
     double xl[8][3], dxl[8][3];
@@ -238,15 +239,59 @@ __global__ void __launch_bounds__(128) k_elem22(MeshDev Mh, DevMat M, DevCtrl C,
         for (int j = i; j < 6; ++j) R[L::D + utri(i, j)] = o.chi[i][j];
 }
 
+// Work-sorted launch order for the constitutive kernels: items (elements or
+// points) grouped by the operation count of their GP's last update, so the
+// lanes of a warp take similar iteration counts and active-set sizes.  A
+// counting sort in WORK_BINS bins of 512 counted operations; the order within
+// a bin is whatever the atomics give, which no result depends on (every GP
+// is updated independently, errors are reduced with atomicMin).
+constexpr int WORK_BINS = 256;
+__device__ __forceinline__ int work_bin(int g, const double *ops)
+{
+    if (g < 0) return 0;
+    const double b = ops[g] * (1.0 / 512.0);
+    return b < (double)(WORK_BINS - 1) ? (int)b : WORK_BINS - 1;
+}
+__global__ void k_work_hist(int n, const int *__restrict__ gp_of, const double *__restrict__ ops, int *hist)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    atomicAdd(&hist[work_bin(gp_of ? gp_of[i] : i, ops)], 1);
+}
+__global__ void __launch_bounds__(WORK_BINS) k_work_scan(int *hist)
+{
+    __shared__ int v[WORK_BINS];
+    v[threadIdx.x] = hist[threadIdx.x];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int b = 0; b < WORK_BINS; ++b) {
+            const int c = v[b];
+            v[b] = acc;
+            acc += c;
+        }
+    }
+    __syncthreads();
+    hist[threadIdx.x] = v[threadIdx.x];
+}
+__global__ void k_work_scatter(int n, const int *__restrict__ gp_of, const double *__restrict__ ops, int *offs,
+                               int *order)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    order[atomicAdd(&offs[work_bin(gp_of ? gp_of[i] : i, ops)], 1)] = i;
+}
+
 // Constitutive update of independent points (no mesh): DSTRSS with the
 // stored de / dr; the full tangent goes to chi[36][ngps] (column-major 6x6).
 template <int NS>
 __global__ void __launch_bounds__(128) k_points(DevMat M, DevCtrl C, DevGp G, const int *gp_iel,
                                                 double *chi, double dt, int inc, int nit,
-                                                unsigned long long *errkey)
+                                                unsigned long long *errkey, const int *__restrict__ order)
 {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= G.ngps) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= G.ngps) return;
+    const int g = order ? order[t] : t;   // work-sorted point order, or the natural one
     const int ng = G.ngps;
     double de[6], r[3], st[6], ds[6];
 #pragma unroll
