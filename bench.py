@@ -48,6 +48,9 @@ OTHER_WORKLOADS = {
     "brick20_32": ("GP updates/s, 32^3 20-node bricks (DSTRSS evaluations per second of whole Newton iterations)",
                    "32^3 FCC Al 20-node eight-GP bricks (262,144 GPs, 421,443 DOF), 2^3-element grains, "
                    "uniaxial tension 1e-3 per increment"),
+    "mixed32": ("GP updates/s, 32^3 mixed FCC/HCP (DSTRSS evaluations per second of whole Newton iterations)",
+                "32^3 one-point bricks (32,768 GPs), 50/50 random HCP-Zr (30 systems incl. twins) / FCC-Al grains "
+                "of 2^3 elements, uniaxial tension 1e-3 per increment"),
     "brick20_10": ("GP updates/s, 10^3 20-node bricks (DSTRSS evaluations per second of whole Newton iterations)",
                    "10^3 FCC Al 20-node eight-GP bricks (the reference sample's mesh: 8,000 GPs), "
                    "one grain per element, uniaxial tension 1e-3 per increment"),

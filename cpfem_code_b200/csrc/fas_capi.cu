@@ -119,15 +119,17 @@ struct fas_handle {
     DVec<double> sor_d, sor_r;   // correction and residual of the refinement
     DVec<double> rdiag;          // reciprocals of the diagonal entries, row order
     DVec<int> work_order, work_hist;   // work-sorted constitutive launch order
+    DVec<int> gp_item;           // GP of item e*npg + g (20-node bricks; -1 for ties)
     int refine_every = 16;       // FP32 sweeps per FP64 residual
     cudaGraphExec_t sor_graph = nullptr;   // GRAPH_SWEEPS plain sweeps
     cudaGraphExec_t sor32_graph = nullptr; // one refinement cycle of the FP32 form
     bool blk32_fresh = false;    // the last assembly wrote blk32
     // reductions and control
-    std::vector<int> sor_boff, sor_nblk;
+    std::vector<int> sor_boff, sor_nblk;       // FP64 colour grids and their partial offsets
+    std::vector<int> sor_boff32, sor_nblk32;   // FP32 colour grids (smaller rings, more CTAs)
     DVec<int> d_cstart;          // colour ranges for the one-CTA SOR
     bool sor_small = false;      // whole solve in one CTA (small meshes)
-    int sor_nblk_tot = 0, nr_nblk = 0;
+    int sor_nblk_tot = 0, sor_nblk_tot32 = 0, nr_nblk = 0;
     DVec<double> part_sor, part_nr, sums;
     DVec<unsigned long long> ekey;
     DVec<int> flags;
@@ -405,7 +407,21 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
         tot += h->sor_nblk[c];
     }
     h->sor_nblk_tot = std::max(tot, 1);
-    CKA(h->part_sor.alloc((size_t)2 * h->sor_nblk_tot));
+    // the FP32 copies' rings are half as large, so twice as many CTAs reside
+    h->sor_boff32.assign(h->ncol, 0);
+    h->sor_nblk32.assign(h->ncol, 0);
+    int tot32 = 0;
+    for (int c = 0; c < h->ncol; ++c) {
+        h->sor_boff32[c] = tot32;
+        const int cps = h->slots == SLOTS ? tma_ctas_per_sm<SLOTS, TMA_LPR, float>()
+                                          : tma_ctas_per_sm<SLOTS20, TMA_LPR81, float>();
+        const int rows = h->slots == SLOTS ? tma_rows<SLOTS>() : tma_rows<SLOTS20>();
+        h->sor_nblk32[c] = (int)std::min<long long>(nblocks(h->col_start[c + 1] - h->col_start[c], rows),
+                                                     (long long)h->nsm * cps);
+        tot32 += h->sor_nblk32[c];
+    }
+    h->sor_nblk_tot32 = std::max(tot32, 1);
+    CKA(h->part_sor.alloc((size_t)2 * std::max(h->sor_nblk_tot, h->sor_nblk_tot32)));
     if (FAS_SOR_RCP) CKA(h->rdiag.alloc((size_t)3 * nn));
     CKA(h->d_cstart.alloc(h->ncol + 1));
     CK(h->d_cstart.put(h->col_start.data(), h->ncol + 1, s));
@@ -570,6 +586,8 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
             const std::vector<double> t = shape22_table();
             CKA(h->dn22.alloc(t.size()));
             CK(h->dn22.put(t.data(), t.size(), s));
+            CKA(h->gp_item.alloc(h->h_gpe.size()));
+            CK(h->gp_item.put(h->h_gpe.data(), h->h_gpe.size(), s));
         }
         CKA(h->ln.alloc(lnT.size()));
         CKA(h->gpe.alloc(gpeT.size()));
@@ -855,10 +873,12 @@ const int *work_order(fas_handle *h, int n, const int *gp_of)
 template <int NS> int launch_elem(fas_handle *h, int inc, int nit)
 {
     Span sp(h, &h->P.ms_constitutive);
-    if (h->nn == 20)   // 20-node bricks: one thread per (element, GP)
+    if (h->nn == 20) {   // 20-node bricks: one thread per (element, GP)
+        const int *order = work_order(h, 8 * h->nlmnt, h->gp_item.p);
         k_elem22<NS><<<nblocks(8LL * h->nlmnt, 128), 128, 0, h->stream>>>(
             h->mesh(), h->M, h->C, h->gp(), h->dn22.p, h->x.p, h->dx.p, h->rec.p, h->h_tiem[inc - 1], inc, nit,
-            h->ekey.p);
+            h->ekey.p, order);
+    }
     else if (!(h->mode & FAS_MODE_CP_WARP)) {
         const int *order = work_order(h, h->nlmnt, h->gpe.p);
         k_elem<NS><<<nblocks(h->nlmnt, 128), 128, 0, h->stream>>>(
@@ -979,23 +999,27 @@ void launch_colour_kernel(fas_handle *h, int c, bool pdl, const T *blk, const do
 {
     const int p0 = h->col_start[c], p1 = h->col_start[c + 1];
     if (p1 <= p0) return;
+    const bool f32 = sizeof(T) == 4;
+    const int nblk = f32 ? h->sor_nblk32[c] : h->sor_nblk[c];
+    const int boff = f32 ? h->sor_boff32[c] : h->sor_boff[c];
+    const int ntot = f32 ? h->sor_nblk_tot32 : h->sor_nblk_tot;
     if (h->slots == SLOTS) {
         auto k = k_sor_colour_tma<T, SLOTS, TMA_LPR>;
         if (pdl)
-            launch_pdl(k, h->sor_nblk[c], TMA_THREADS, tma_smem_bytes<T, SLOTS>(), h->stream, blk, h->bcol.p, p0,
-                       p1, rhs, sol, base, rdiag, ctl, part, h->sor_boff[c], h->sor_nblk_tot);
+            launch_pdl(k, nblk, TMA_THREADS, tma_smem_bytes<T, SLOTS>(), h->stream, blk, h->bcol.p, p0,
+                       p1, rhs, sol, base, rdiag, ctl, part, boff, ntot);
         else
-            k<<<h->sor_nblk[c], TMA_THREADS, tma_smem_bytes<T, SLOTS>(), h->stream>>>(
-                blk, h->bcol.p, p0, p1, rhs, sol, base, rdiag, ctl, part, h->sor_boff[c], h->sor_nblk_tot);
+            k<<<nblk, TMA_THREADS, tma_smem_bytes<T, SLOTS>(), h->stream>>>(
+                blk, h->bcol.p, p0, p1, rhs, sol, base, rdiag, ctl, part, boff, ntot);
     } else {
         auto k = k_sor_colour_tma<T, SLOTS20, TMA_LPR81>;
         const unsigned nt = tma_threads<TMA_LPR81, TMA_ROWS81>();
         if (pdl)
-            launch_pdl(k, h->sor_nblk[c], nt, tma_smem_bytes<T, SLOTS20>(), h->stream, blk, h->bcol.p, p0, p1,
-                       rhs, sol, base, rdiag, ctl, part, h->sor_boff[c], h->sor_nblk_tot);
+            launch_pdl(k, nblk, nt, tma_smem_bytes<T, SLOTS20>(), h->stream, blk, h->bcol.p, p0, p1,
+                       rhs, sol, base, rdiag, ctl, part, boff, ntot);
         else
-            k<<<h->sor_nblk[c], nt, tma_smem_bytes<T, SLOTS20>(), h->stream>>>(
-                blk, h->bcol.p, p0, p1, rhs, sol, base, rdiag, ctl, part, h->sor_boff[c], h->sor_nblk_tot);
+            k<<<nblk, nt, tma_smem_bytes<T, SLOTS20>(), h->stream>>>(
+                blk, h->bcol.p, p0, p1, rhs, sol, base, rdiag, ctl, part, boff, ntot);
     }
 }
 
@@ -1022,9 +1046,10 @@ void launch_colour(fas_handle *h, int c, bool fp32)
                                      FAS_SOR_RCP ? h->rdiag.p : nullptr, h->sorctl.p, h->part_sor.p);
 }
 
-void launch_check(fas_handle *h, double tolerl)
+void launch_check(fas_handle *h, double tolerl, bool fp32 = false)
 {
-    launch_pdl(k_sor_check, 1, 1024, 0, h->stream, h->part_sor.p, h->sor_nblk_tot, h->sorctl.p, tolerl);
+    launch_pdl(k_sor_check, 1, 1024, 0, h->stream, h->part_sor.p, fp32 ? h->sor_nblk_tot32 : h->sor_nblk_tot,
+               h->sorctl.p, tolerl);
 }
 
 void launch_plain_sweep(fas_handle *h, const BlockDev &B, double tolerl)
@@ -1058,7 +1083,7 @@ void launch_fp32_cycle(fas_handle *h, const BlockDev &B, double tolerl, int swee
     const unsigned rblk = (unsigned)std::min<long long>(nblocks(h->nnod, 8), (long long)h->nsm * 8);
     for (int it = 0; it < sweeps; ++it) {
         for (int c = 0; c < h->ncol; ++c) launch_colour(h, c, true);
-        launch_check(h, tolerl);
+        launch_check(h, tolerl, true);
     }
     k_fold<<<nblocks((long long)nd3, 256), 256, 0, h->stream>>>((int)nd3, h->ddx.p, h->sor_d.p);
     k_residual<<<rblk, 256, 0, h->stream>>>(B, h->rhs.p, h->ddx.p, h->sor_r.p, h->sorctl.p);
@@ -1139,7 +1164,7 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
                         keep(h, sp);
                         LAUNCHED(h);
                     }
-                    launch_check(h, tolerl);
+                    launch_check(h, tolerl, true);
                     LAUNCHED(h);
                 }
                 done += k;

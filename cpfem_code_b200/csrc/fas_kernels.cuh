@@ -156,11 +156,12 @@ __global__ void __launch_bounds__(128) k_elem22(MeshDev Mh, DevMat M, DevCtrl C,
                                                 const double *__restrict__ x,
                                                 const double *__restrict__ dx, double *rec,
                                                 double dt, int inc, int nit,
-                                                unsigned long long *errkey)
+                                                unsigned long long *errkey, const int *__restrict__ order)
 {
     using L = RecLayout<20>;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 8LL * Mh.nlmnt) return;
+    const long long ti = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ti >= 8LL * Mh.nlmnt) return;
+    const long long t = order ? order[ti] : ti;   // item e*8 + gq, work-sorted or natural
     const int e = (int)(t >> 3), gq = (int)(t & 7);
     if (Mh.lt[e] < 9) return;   // tie element: no Gauss point
     const int ne = Mh.nlmnt;
@@ -1119,10 +1120,10 @@ template <typename T, int S = SLOTS> __host__ __device__ constexpr int tma_smem_
 // CTAs of the FP64 kernel that fit on one SM (228 KB of shared memory,
 // 1 KB of it reserved per CTA, at most 32 warps); the colour grid is sized
 // to fill them.
-template <int S, int LPR> __host__ __device__ constexpr int tma_ctas_per_sm()
+template <int S, int LPR, typename T = double> __host__ __device__ constexpr int tma_ctas_per_sm()
 {
-    return (228 * 1024) / (tma_smem_bytes<double, S>() + 1024) < 32 / (tma_threads<LPR, tma_rows<S>()>() / 32)
-               ? (228 * 1024) / (tma_smem_bytes<double, S>() + 1024)
+    return (228 * 1024) / (tma_smem_bytes<T, S>() + 1024) < 32 / (tma_threads<LPR, tma_rows<S>()>() / 32)
+               ? (228 * 1024) / (tma_smem_bytes<T, S>() + 1024)
                : 32 / (tma_threads<LPR, tma_rows<S>()>() / 32);
 }
 constexpr int TMA_CTAS_PER_SM = tma_ctas_per_sm<SLOTS, TMA_LPR>();
