@@ -5,7 +5,11 @@
 // Everything runs on one CUDA stream per handle.  Host synchronisation
 // happens once per global Newton iteration (to read the error key and the
 // norms that decide the loop) and once per chunk of SOR sweeps (to read the
-// convergence flag); nothing else waits for the device.
+// convergence flag); nothing else waits for the device.  Chunks of sweeps
+// are CUDA graphs whose colour and check kernels carry programmatic
+// dependencies, so each colour's matrix stream starts while the previous
+// colour drains.  A mesh is one brick family (8-node lt 12 or 20-node lt 22)
+// plus optional tie elements (lt 1-6).
 
 #include "../../include/fasolt_gpu.h"
 #include "fas_kernels.cuh"

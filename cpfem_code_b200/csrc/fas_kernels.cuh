@@ -3,15 +3,26 @@
 // Data layout in HBM (all FP64 unless noted):
 //   * nodal vectors x, dx, fc, ddx, rhs: reference DOF order 3*node+comp;
 //   * Gauss-point state: structure of arrays field[k * ngps + g];
-//   * element record rec[e * REC + .]: sfd (24), stress (6), weight, tangent
-//     upper triangle (21) -- written once per Newton iteration by the element
-//     kernel and read by the row-gather assembly;
+//   * Gauss-point record rec[item * RecLayout<NN>::LEN + .] (item = element
+//     for 8-node bricks, element*8 + GP for 20-node bricks): sfd (3 NN),
+//     stress (6), weight, tangent upper triangle (21) -- written once per
+//     Newton iteration by the element kernel, read by the row-gather
+//     assembly;
 //   * stiffness: block-ELL of 3x3 node blocks, rows permuted so each SOR
-//     colour is a contiguous row range.  A row is BROW = 244 values (the 27
-//     blocks, component-major, plus one pad value): blk[row*244 + (r*3+c)*27
-//     + slot], so one component of all slots is 216 contiguous bytes and a
-//     row is 1952 bytes, a multiple of 16 as bulk copies need.  Slot 0 = the
-//     diagonal block; bcol[row*28 + slot] = column node (28 ints per row).
+//     colour is a contiguous row range.  A row of S slots (27 for 8-node,
+//     81 for 20-node bricks) holds brow_of(S) values, component-major:
+//     blk[row*brow + (r*3+c)*S + slot], padded so FP64 and FP32 rows are
+//     16-byte multiples as bulk copies need (244 and 732 values).  Slot 0 is
+//     the diagonal block; bcol[row*crow + slot] is the column node and
+//     bcol[row*crow + S] the row's slot count (crow = 28 or 84).
+//
+// Kernels: the element pass (k_elem, k_elem22, the opt-in warp variants),
+// the work-sorted launch order of the constitutive kernels (k_work_*), the
+// row-gather assembly with fused SUVALS (k_assemble), the SOR colour phase
+// streamed by the bulk-copy engine (k_sor_colour_tma, launched with
+// programmatic serialisation) and its stopping test (k_sor_check), the
+// one-CTA solve of small meshes (k_sor_small), the FP32 refinement pieces,
+// the increment commit, twin reorientation, ELASEPS and the exports.
 #pragma once
 
 #include "fas_device.cuh"
