@@ -1141,6 +1141,129 @@ constexpr int TMA_CTAS_PER_SM = tma_ctas_per_sm<SLOTS, TMA_LPR>();
 static_assert(TMA_CTAS_PER_SM >= 1 && tma_ctas_per_sm<SLOTS20, TMA_LPR81>() >= 1,
               "the ring must fit in shared memory");
 
+// Operands of one chunk row for one lane, gathered before its point
+// update: the solution at the lane's slots (x0, x1, x2) and, on the row's
+// first lane, the right-hand side and reciprocal diagonal of the row's node (r).
+template <int SPL> struct SorOps {
+    double x0[SPL], x1[SPL], x2[SPL], r[6];
+};
+
+// Gather of lane q of chunk row `row` from a landed stage's column ids.
+// r0 is the chunk's first row and nrow its row count.
+template <int S, int LPR>
+__device__ __forceinline__ void sor_gather(const int *stage_cols, int r0, int nrow, int row, int q,
+                                           const double *sol, const double *__restrict__ rhs,
+                                           const double *__restrict__ rdiag, uint64_t keep_pol,
+                                           SorOps<(S + LPR - 1) / LPR> &g)
+{
+    constexpr int SPL = (S + LPR - 1) / LPR, CR = crow_of(S);
+    const bool live = row < nrow;
+    const int *cols = stage_cols + (live ? row : 0) * CR;
+    const int ns = live ? cols[S] : 0;
+#pragma unroll
+    for (int j = 0; j < SPL; ++j) {
+        const int sl = q + LPR * j;
+        const bool on = sl < ns;
+        const int m = on ? cols[sl] : 0;
+        g.x0[j] = on ? ld_keep(sol + 3 * m, keep_pol) : 0.0;
+        g.x1[j] = on ? ld_keep(sol + 3 * m + 1, keep_pol) : 0.0;
+        g.x2[j] = on ? ld_keep(sol + 3 * m + 2, keep_pol) : 0.0;
+    }
+    const bool own = live && q == 0;
+    const int n = cols[0];
+    g.r[0] = own ? ld_keep(rhs + 3 * n, keep_pol) : 0.0;
+    g.r[1] = own ? ld_keep(rhs + 3 * n + 1, keep_pol) : 0.0;
+    g.r[2] = own ? ld_keep(rhs + 3 * n + 2, keep_pol) : 0.0;
+    if (rdiag) {
+        const double *rd = rdiag + 3 * (size_t)(own ? r0 + row : r0);
+        g.r[3] = own ? rd[0] : 0.0;
+        g.r[4] = own ? rd[1] : 0.0;
+        g.r[5] = own ? rd[2] : 0.0;
+    }
+}
+
+// Point update of chunk row `row` from a landed stage and its gathered
+// operands: lane q multiplies the blocks of slots q, q+LPR, ... (slot 0,
+// the diagonal, excluded), the LPR lanes of the row sum their products, and
+// the first lane updates x, y and z in turn (omega = 1.2), stores them and
+// adds |x_new - x_old|^2 to v0 and |x_new + base|^2 to v1.  With `rcp` the
+// quotients come from the gathered reciprocal diagonal.
+template <typename T, int S, int LPR>
+__device__ __forceinline__ void sor_update(const unsigned char *stage, int nrow, int row, int q,
+                                           const SorOps<(S + LPR - 1) / LPR> &g, bool rcp,
+                                           const double *__restrict__ base, double *sol, double &v0,
+                                           double &v1)
+{
+    constexpr int SPL = (S + LPR - 1) / LPR, BR = brow_of(S), CR = crow_of(S);
+    constexpr int VB = tma_rows<S>() * BR * (int)sizeof(T);
+    const bool live = row < nrow;
+    const T *vals = reinterpret_cast<const T *>(stage) + (live ? row : 0) * BR;
+    const int *cols = reinterpret_cast<const int *>(stage + VB) + (live ? row : 0) * CR;
+    const int ns = live ? cols[S] : 0;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+#pragma unroll
+    for (int j = 0; j < SPL; ++j) {
+        const int sl = q + LPR * j;
+        if (sl >= 1 && sl < ns) {
+            const T *b = vals + sl;
+            a0 += (double)b[0 * S] * g.x0[j] + (double)b[1 * S] * g.x1[j] + (double)b[2 * S] * g.x2[j];
+            a1 += (double)b[3 * S] * g.x0[j] + (double)b[4 * S] * g.x1[j] + (double)b[5 * S] * g.x2[j];
+            a2 += (double)b[6 * S] * g.x0[j] + (double)b[7 * S] * g.x1[j] + (double)b[8 * S] * g.x2[j];
+        }
+    }
+#pragma unroll
+    for (int o = 1; o < LPR; o <<= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+    }
+    if (live && q == 0) {
+        const int n = cols[0];
+        double D[9];
+#pragma unroll
+        for (int qq = 0; qq < 9; ++qq) D[qq] = (double)vals[qq * S];
+        const double o0 = g.x0[0], o1 = g.x1[0], o2 = g.x2[0];
+        double x0 = o0, x1 = o1, x2 = o2;
+        double t;
+        if (rcp) {
+            // num / D from the correctly rounded reciprocal of D: with
+            // q0 = num * (1/D) and the exact remainder e = num - q0 * D
+            // (one FMA), q0 + e * (1/D) rounds to the correctly rounded
+            // quotient (Markstein, IBM J. Res. Dev. 34 (1990) 111-119).
+            const double i0 = g.r[3], i1 = g.r[4], i2 = g.r[5];
+            double nm = g.r[0] - (a0 + D[1] * x1 + D[2] * x2);
+            double q0 = nm * i0;
+            t = fma(fma(-q0, D[0], nm), i0, q0);
+            x0 = x0 + 1.2 * (t - x0);
+            nm = g.r[1] - (a1 + D[3] * x0 + D[5] * x2);
+            q0 = nm * i1;
+            t = fma(fma(-q0, D[4], nm), i1, q0);
+            x1 = x1 + 1.2 * (t - x1);
+            nm = g.r[2] - (a2 + D[6] * x0 + D[7] * x1);
+            q0 = nm * i2;
+            t = fma(fma(-q0, D[8], nm), i2, q0);
+            x2 = x2 + 1.2 * (t - x2);
+        } else {
+            t = (g.r[0] - (a0 + D[1] * x1 + D[2] * x2)) / D[0];
+            x0 = x0 + 1.2 * (t - x0);
+            t = (g.r[1] - (a1 + D[3] * x0 + D[5] * x2)) / D[4];
+            x1 = x1 + 1.2 * (t - x1);
+            t = (g.r[2] - (a2 + D[6] * x0 + D[7] * x1)) / D[8];
+            x2 = x2 + 1.2 * (t - x2);
+        }
+        sol[3 * n] = x0;
+        sol[3 * n + 1] = x1;
+        sol[3 * n + 2] = x2;
+        v0 += (x0 - o0) * (x0 - o0) + (x1 - o1) * (x1 - o1) + (x2 - o2) * (x2 - o2);
+        if (base) {
+            x0 += base[3 * n];
+            x1 += base[3 * n + 1];
+            x2 += base[3 * n + 2];
+        }
+        v1 += x0 * x0 + x1 * x1 + x2 * x2;
+    }
+}
+
 // One colour phase of SOR with the colour's block rows streamed through a
 // TMA_STAGES-deep shared-memory ring by the bulk-copy engine (evict-first in
 // L2).  CTA b takes chunks b, b + grid, ... of TMA_ROWS consecutive rows;
@@ -1217,35 +1340,11 @@ __global__ void __launch_bounds__(tma_rows<S>() * LPR) k_sor_colour_tma(const T 
     // to chunk k + j.  No row of a colour reads a value written by another
     // row of the same colour, so the gathers of the next TMA_PD chunks are
     // in flight while chunk k is computed.
-    double gx0[TMA_PD + 1][SPL] = {}, gx1[TMA_PD + 1][SPL] = {}, gx2[TMA_PD + 1][SPL] = {};
-    double gr[TMA_PD + 1][6] = {};   // right-hand side and reciprocal diagonal of the row's node
-    auto gather = [&](int kk, double (&g0)[SPL], double (&g1)[SPL], double (&g2)[SPL],
-                      double (&grr)[6]) {
-        const int c = blockIdx.x + kk * gridDim.x;
-        const int nrow = min(ROWS, p1 - (p0 + c * ROWS));
-        const bool live = row < nrow;
-        const int *cols = reinterpret_cast<const int *>(smem + (kk % TMA_STAGES) * SB + VB) + (live ? row : 0) * CR;
-        const int ns = live ? cols[S] : 0;
-#pragma unroll
-        for (int j = 0; j < SPL; ++j) {
-            const int sl = q + LPR * j;
-            const bool on = sl < ns;
-            const int m = on ? cols[sl] : 0;
-            g0[j] = on ? ld_keep(sol + 3 * m, keep_pol) : 0.0;
-            g1[j] = on ? ld_keep(sol + 3 * m + 1, keep_pol) : 0.0;
-            g2[j] = on ? ld_keep(sol + 3 * m + 2, keep_pol) : 0.0;
-        }
-        const bool own = live && q == 0;
-        const int n = cols[0];
-        grr[0] = own ? ld_keep(rhs + 3 * n, keep_pol) : 0.0;
-        grr[1] = own ? ld_keep(rhs + 3 * n + 1, keep_pol) : 0.0;
-        grr[2] = own ? ld_keep(rhs + 3 * n + 2, keep_pol) : 0.0;
-        if (rdiag) {
-            const double *rd = rdiag + 3 * (size_t)(own ? p0 + c * ROWS + row : p0);
-            grr[3] = own ? rd[0] : 0.0;
-            grr[4] = own ? rd[1] : 0.0;
-            grr[5] = own ? rd[2] : 0.0;
-        }
+    SorOps<SPL> g[TMA_PD + 1] = {};
+    auto gather = [&](int kk, SorOps<SPL> &o) {
+        const int r0 = p0 + (blockIdx.x + kk * gridDim.x) * ROWS;
+        sor_gather<S, LPR>(reinterpret_cast<const int *>(smem + (kk % TMA_STAGES) * SB + VB), r0,
+                           min(ROWS, p1 - r0), row, q, sol, rhs, rdiag, keep_pol, o);
     };
     // chunks [0, waited) have landed; chunks [0, min(myn, k + TMA_STAGES))
     // have been issued when iteration k starts
@@ -1256,7 +1355,7 @@ __global__ void __launch_bounds__(tma_rows<S>() * LPR) k_sor_colour_tma(const T 
         if (!fault && i < myn) {
             if (__syncthreads_and(mbar_wait_bounded(&bars[i], 0u) ? 1 : 0)) {
                 waited = i + 1;
-                gather(i, gx0[i], gx1[i], gx2[i], gr[i]);
+                gather(i, g[i]);
             } else {
                 fault = true;
             }
@@ -1271,93 +1370,18 @@ __global__ void __launch_bounds__(tma_rows<S>() * LPR) k_sor_colour_tma(const T 
                 break;
             }
             waited = kk + 1;
-            gather(kk, gx0[TMA_PD], gx1[TMA_PD], gx2[TMA_PD], gr[TMA_PD]);
+            gather(kk, g[TMA_PD]);
         }
         const int st = k % TMA_STAGES;
-        const int c = blockIdx.x + k * gridDim.x;
-        const int nrow = min(ROWS, p1 - (p0 + c * ROWS));
-        const bool live = row < nrow;
-        const T *vals = reinterpret_cast<const T *>(smem + st * SB) + (live ? row : 0) * BR;
-        const int *cols = reinterpret_cast<const int *>(smem + st * SB + VB) + (live ? row : 0) * CR;
-        const int ns = live ? cols[S] : 0;
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-#pragma unroll
-        for (int j = 0; j < SPL; ++j) {
-            const int sl = q + LPR * j;
-            if (sl >= 1 && sl < ns) {
-                const T *b = vals + sl;
-                a0 += (double)b[0 * S] * gx0[0][j] + (double)b[1 * S] * gx1[0][j] + (double)b[2 * S] * gx2[0][j];
-                a1 += (double)b[3 * S] * gx0[0][j] + (double)b[4 * S] * gx1[0][j] + (double)b[5 * S] * gx2[0][j];
-                a2 += (double)b[6 * S] * gx0[0][j] + (double)b[7 * S] * gx1[0][j] + (double)b[8 * S] * gx2[0][j];
-            }
-        }
-#pragma unroll
-        for (int o = 1; o < LPR; o <<= 1) {
-            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
-        }
-        if (live && q == 0) {
-            const int n = cols[0];
-            double D[9];
-#pragma unroll
-            for (int qq = 0; qq < 9; ++qq) D[qq] = (double)vals[qq * S];
-            const double o0 = gx0[0][0], o1 = gx1[0][0], o2 = gx2[0][0];
-            double x0 = o0, x1 = o1, x2 = o2;
-            double t;
-            if (rdiag) {
-                // num / D from the correctly rounded reciprocal of D: with
-                // q0 = num * (1/D) and the exact remainder e = num - q0 * D
-                // (one FMA), q0 + e * (1/D) rounds to the correctly rounded
-                // quotient (Markstein, IBM J. Res. Dev. 34 (1990) 111-119).
-                const double i0 = gr[0][3], i1 = gr[0][4], i2 = gr[0][5];
-                double nm = gr[0][0] - (a0 + D[1] * x1 + D[2] * x2);
-                double q0 = nm * i0;
-                t = fma(fma(-q0, D[0], nm), i0, q0);
-                x0 = x0 + 1.2 * (t - x0);
-                nm = gr[0][1] - (a1 + D[3] * x0 + D[5] * x2);
-                q0 = nm * i1;
-                t = fma(fma(-q0, D[4], nm), i1, q0);
-                x1 = x1 + 1.2 * (t - x1);
-                nm = gr[0][2] - (a2 + D[6] * x0 + D[7] * x1);
-                q0 = nm * i2;
-                t = fma(fma(-q0, D[8], nm), i2, q0);
-                x2 = x2 + 1.2 * (t - x2);
-            } else {
-                t = (gr[0][0] - (a0 + D[1] * x1 + D[2] * x2)) / D[0];
-                x0 = x0 + 1.2 * (t - x0);
-                t = (gr[0][1] - (a1 + D[3] * x0 + D[5] * x2)) / D[4];
-                x1 = x1 + 1.2 * (t - x1);
-                t = (gr[0][2] - (a2 + D[6] * x0 + D[7] * x1)) / D[8];
-                x2 = x2 + 1.2 * (t - x2);
-            }
-            sol[3 * n] = x0;
-            sol[3 * n + 1] = x1;
-            sol[3 * n + 2] = x2;
-            v0 += (x0 - o0) * (x0 - o0) + (x1 - o1) * (x1 - o1) + (x2 - o2) * (x2 - o2);
-            if (base) {
-                x0 += base[3 * n];
-                x1 += base[3 * n + 1];
-                x2 += base[3 * n + 2];
-            }
-            v1 += x0 * x0 + x1 * x1 + x2 * x2;
-        }
+        const int nrow = min(ROWS, p1 - (p0 + (int)(blockIdx.x + k * gridDim.x) * ROWS));
+        sor_update<T, S, LPR>(smem + st * SB, nrow, row, q, g[0], rdiag != nullptr, base, sol, v0, v1);
         __syncthreads();   // every row of this stage is done
         if (threadIdx.x == 0 && k + TMA_STAGES < myn) {
             fence_proxy_async();
             issue(k + TMA_STAGES);
         }
 #pragma unroll
-        for (int i = 0; i < TMA_PD; ++i) {
-#pragma unroll
-            for (int j = 0; j < SPL; ++j) {
-                gx0[i][j] = gx0[i + 1][j];
-                gx1[i][j] = gx1[i + 1][j];
-                gx2[i][j] = gx2[i + 1][j];
-            }
-#pragma unroll
-            for (int j = 0; j < 6; ++j) gr[i][j] = gr[i + 1][j];
-        }
+        for (int i = 0; i < TMA_PD; ++i) g[i] = g[i + 1];
     }
     (void)lane;
     if (fault) {
