@@ -23,6 +23,7 @@ FAS_E_RANGE = -6
 FAS_E_STATE = -7
 FAS_E_TIMEOUT = -8
 FAS_MAXSS = 60
+FAS_MAXSVS = 63    # leading dimension of the adjoint's g_sv
 SVLD = 63          # maxsvs, src/fasolt/fas-com-mod.f90:14
 XSLD = 99          # second dimension of x_spec / f_spec (fas-com-mod.f90:30-31)
 
@@ -111,6 +112,12 @@ class FasProfile(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class FasReplay(C.Structure):
+    _fields_ = [("ninc", C.c_int32), ("chk_every", C.c_int32),
+                ("de", _p), ("dr", _p), ("dt", _p), ("w", _p), ("y", _p),
+                ("q", C.c_double * 3)]
+
+
 class FasTwinEvent(C.Structure):
     _fields_ = [("inc", C.c_int32), ("gp", C.c_int32), ("sys", C.c_int32), ("pad", C.c_int32),
                 ("euler_old", C.c_double * 3), ("euler_new", C.c_double * 3)]
@@ -178,8 +185,11 @@ def declare(lib: C.CDLL, prefix: str) -> None:
         "get_cp_ops": (i32, [H, C.POINTER(C.c_double)]),
         "lattice_strain": (i32, [H, _p, i32]) if prefix == "fas_gpu" else (i32, [H, _p]),
     }
+    _dp = C.POINTER(C.c_double)
+    sig["adjoint_forward"] = (i32, [H, C.POINTER(FasReplay), _dp, _dp])
     if prefix == "fas_gpu":
         sig["profile"] = (i32, [H, i32, C.POINTER(FasProfile)])
+        sig["adjoint_grad"] = (i32, [H, C.POINTER(FasReplay), _dp, _dp, _dp, _dp])
     for name, (res, args) in sig.items():
         fn = getattr(lib, f"{prefix}_{name}")
         fn.restype = res

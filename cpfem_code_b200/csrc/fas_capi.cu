@@ -13,6 +13,7 @@
 
 #include "../../include/fasolt_gpu.h"
 #include "fas_kernels.cuh"
+#include "fas_adjoint.cuh"
 
 #include <algorithm>
 #include <climits>
@@ -81,6 +82,16 @@ struct HostCtl {                 // pinned mirror of the small device results
 };
 
 }  // namespace
+
+// Device buffers of the replay behind fas_gpu_adjoint_forward / _grad:
+// the history and objective, checkpoints, per-GP records of the segment
+// being swept back, the adjoints, and a private copy of the GP state that
+// DSTRSS reads and writes (the handle's own state is left as it was).
+struct ReplayBufs {
+    DVec<double> de, dr, dt, w, y, chk, rec;
+    DVec<double> sv, dsv, srate, erepmd, ops, jg, eq, gst, gsv, gp;
+    DVec<int> twinsys, timestwinned, cp_iters, tflag;
+};
 
 struct fas_handle {
     int dev = 0, nsm = 148;
@@ -151,6 +162,7 @@ struct fas_handle {
     cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;
     double asm_bytes = 0.0;      // algorithmic bytes of one assembly launch
     int64_t launches = 0;
+    ReplayBufs rp;
 
     ~fas_handle()
     {
@@ -1316,6 +1328,118 @@ int pattern_device(fas_handle *h, int ld, DVec<int> &isd)
     return h->hc->flags[2] ? 955 : 0;
 }
 
+// ------------------------------------------------------------------ adjoint
+// Grow-only allocation of a replay buffer.
+template <class T> cudaError_t ensure(DVec<T> &v, size_t n)
+{
+    return v.n >= n && v.p ? cudaSuccess : v.alloc(std::max<size_t>(n, 1));
+}
+
+// Uploads a replay's history, copies the GP state the replay works on and
+// sizes its buffers; fills the kernels' descriptors.
+int replay_prepare(fas_handle *h, const fas_replay_desc *d, bool grad, ReplayDev &H, DevGp &G, int &rs)
+{
+    if (!h || !d || !d->de || !d->dr || !d->dt || !d->w || !d->y) return FAS_E_ARG;
+    if (!h->have_state) return FAS_E_STATE;
+    if (d->ninc < 1 || d->chk_every < 1) return FAS_E_ARG;
+    if (h->ns_tmpl > 32) return FAS_E_RANGE;
+    const double qn = std::sqrt(d->q[0] * d->q[0] + d->q[1] * d->q[1] + d->q[2] * d->q[2]);
+    if (!(qn > 0.0) || !std::isfinite(qn)) return FAS_E_ARG;
+    ReplayBufs &B = h->rp;
+    cudaStream_t s = h->stream;
+    const size_t ng = h->ngps, ninc = d->ninc;
+    const int chk = std::min(d->chk_every, d->ninc);
+    const int nseg = (d->ninc + chk - 1) / chk;
+    const int zs = 9 + h->maxns;
+    rs = zs + 7 + h->ns_tmpl;
+    CKA(ensure(B.de, 6 * ng * ninc));
+    CKA(ensure(B.dr, 3 * ng * ninc));
+    CKA(ensure(B.dt, ninc));
+    CKA(ensure(B.w, ng));
+    CKA(ensure(B.y, ng));
+    CKA(ensure(B.chk, (size_t)nseg * zs * ng));
+    if (grad) {
+        CKA(ensure(B.rec, (size_t)chk * rs * ng));
+        CKA(ensure(B.gst, 6 * ng));
+        CKA(ensure(B.gsv, (size_t)(zs - 6) * ng));
+        CKA(ensure(B.gp, (size_t)ADJ_NP * ng));
+    }
+    CKA(ensure(B.sv, (size_t)h->nsvld * ng));
+    CKA(ensure(B.dsv, (size_t)h->nsvld * ng));
+    CKA(ensure(B.srate, (size_t)h->maxns * ng));
+    CKA(ensure(B.erepmd, ng));
+    CKA(ensure(B.ops, ng));
+    CKA(ensure(B.jg, ng));
+    CKA(ensure(B.eq, ng));
+    CKA(ensure(B.twinsys, ng));
+    CKA(ensure(B.timestwinned, ng));
+    CKA(ensure(B.cp_iters, ng));
+    CKA(ensure(B.tflag, 1));
+    CK(cudaMemcpyAsync(B.de.p, d->de, 6 * ng * ninc * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(B.dr.p, d->dr, 3 * ng * ninc * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(B.dt.p, d->dt, ninc * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(B.w.p, d->w, ng * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(B.y.p, d->y, ng * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(B.sv.p, h->sv.p, (size_t)h->nsvld * ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(B.twinsys.p, h->twinsys.p, ng * sizeof(int), cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(B.timestwinned.p, h->timestwinned.p, ng * sizeof(int), cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemsetAsync(B.tflag.p, 0, sizeof(int), s));
+    CK(cudaMemsetAsync(h->ekey.p, 0xFF, sizeof(unsigned long long), s));
+    H.de = B.de.p;
+    H.dr = B.dr.p;
+    H.dt = B.dt.p;
+    H.w = B.w.p;
+    H.y = B.y.p;
+    for (int k = 0; k < 3; ++k) H.q[k] = d->q[k] / qn;
+    H.ninc = d->ninc;
+    H.chk = chk;
+    H.zs = zs;
+    G = DevGp{};
+    G.ngps = h->ngps;
+    G.ldsv = h->nsvld;
+    G.ldsl = h->maxns;
+    G.sv = B.sv.p;
+    G.dsv = B.dsv.p;
+    G.srate = B.srate.p;
+    G.erepmd = B.erepmd.p;
+    G.ops = B.ops.p;
+    G.cp_iters = B.cp_iters.p;
+    G.twinsys = B.twinsys.p;
+    G.timestwinned = B.timestwinned.p;
+    G.tflag = B.tflag.p;
+    return 0;
+}
+
+template <int NS>
+void launch_replay_fwd(fas_handle *h, const ReplayDev &H, const DevGp &G)
+{
+    k_replay_fwd<NS><<<nblocks(h->ngps, 128), 128, 0, h->stream>>>(h->M, h->C, G, h->gp_iel.p, h->st.p, H,
+                                                                  h->rp.chk.p, h->rp.jg.p, h->rp.eq.p,
+                                                                  h->ekey.p);
+}
+
+template <int NS>
+void launch_replay_adj(fas_handle *h, const ReplayDev &H, const DevGp &G, int rs)
+{
+    k_replay_adj<NS><<<nblocks(h->ngps, 128), 128, 0, h->stream>>>(h->M, h->C, G, h->gp_iel.p, H, h->rp.chk.p,
+                                                                  h->rp.rec.p, rs, h->rp.jg.p, h->rp.gst.p,
+                                                                  h->rp.gsv.p, h->rp.gp.p, h->ekey.p);
+}
+
+// Waits for the replay kernels; the objective summed over the GPs in GP order.
+int replay_finish(fas_handle *h, double *J)
+{
+    std::vector<double> jg(h->ngps);
+    CK(cudaMemcpyAsync(h->hc->ekey, h->ekey.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(jg.data(), h->rp.jg.p, jg.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->hc->ekey[0] != ~0ull) return (int)(h->hc->ekey[0] & 0xFFFFull);
+    double acc = 0.0;
+    for (double v : jg) acc += v;
+    if (J) *J = acc;
+    return 0;
+}
+
 }  // namespace
 
 // ================================================================ C ABI
@@ -1568,6 +1692,69 @@ int32_t fas_gpu_lattice_strain(fas_handle *h, void *strain, int32_t real_bytes)
     k_elaseps<<<nblocks(h->ngps, 128), 128, 0, h->stream>>>(h->M, h->gp(), h->gp_iel.p, d.p);
     LAUNCHED(h);
     return down_field(h, strain, real_bytes, 6, 6, h->ngps, d.p);
+}
+
+int32_t fas_gpu_adjoint_forward(fas_handle *h, const fas_replay_desc *d, double *J, double *eq)
+{
+    ReplayDev H;
+    DevGp G;
+    int rs = 0;
+    int rc = replay_prepare(h, d, false, H, G, rs);
+    if (rc) return rc;
+    if (h->ns_tmpl == 12) launch_replay_fwd<12>(h, H, G);
+    else launch_replay_fwd<32>(h, H, G);
+    LAUNCHED(h);
+    rc = replay_finish(h, J);
+    if (rc) return rc;
+    if (eq) CK(cudaMemcpy(eq, h->rp.eq.p, h->ngps * sizeof(double), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int32_t fas_gpu_adjoint_grad(fas_handle *h, const fas_replay_desc *d, double *J, double *g_st, double *g_sv,
+                             double *g_ampar)
+{
+    ReplayDev H;
+    DevGp G;
+    int rs = 0;
+    int rc = replay_prepare(h, d, true, H, G, rs);
+    if (rc) return rc;
+    const size_t ng = h->ngps;
+    if (h->ns_tmpl == 12) launch_replay_fwd<12>(h, H, G);
+    else launch_replay_fwd<32>(h, H, G);
+    LAUNCHED(h);
+    // the reverse sweep starts from the same twin state as the forward one
+    CK(cudaMemcpyAsync(h->rp.twinsys.p, h->twinsys.p, ng * sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
+    if (h->ns_tmpl == 12) launch_replay_adj<12>(h, H, G, rs);
+    else launch_replay_adj<32>(h, H, G, rs);
+    LAUNCHED(h);
+    rc = replay_finish(h, J);
+    if (rc) return rc;
+    const int nsv = 3 + h->maxns;
+    if (g_st) {
+        std::vector<double> t(6 * ng);
+        CK(cudaMemcpy(t.data(), h->rp.gst.p, t.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for (size_t g = 0; g < ng; ++g)
+            for (int k = 0; k < 6; ++k) g_st[g * 6 + k] = t[(size_t)k * ng + g];
+    }
+    if (g_sv) {
+        std::vector<double> t((size_t)nsv * ng);
+        CK(cudaMemcpy(t.data(), h->rp.gsv.p, t.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for (size_t g = 0; g < ng; ++g) {
+            const int ns = h->M.ns[std::abs(h->h_gp_iel[g]) - 1];
+            for (int k = 0; k < FAS_MAXSVS; ++k) g_sv[g * FAS_MAXSVS + k] = k < 3 + ns ? t[(size_t)k * ng + g] : 0.0;
+        }
+    }
+    if (g_ampar) {
+        std::vector<double> t((size_t)ADJ_NP * ng);
+        CK(cudaMemcpy(t.data(), h->rp.gp.p, t.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int m = 0; m < h->M.nmatl; ++m)
+            for (int k = 0; k < 10; ++k) g_ampar[m * 10 + k] = 0.0;
+        for (size_t g = 0; g < ng; ++g) {
+            const int m = std::abs(h->h_gp_iel[g]) - 1;
+            for (int j = 0; j < ADJ_NP; ++j) g_ampar[m * 10 + adj_ampar_index(j)] += t[(size_t)j * ng + g];
+        }
+    }
+    return 0;
 }
 
 int32_t fas_gpu_get_cp_ops(fas_handle *h, double *ops)

@@ -174,12 +174,55 @@ class _SolverBase:
         self._call("get_cp_ops", out.ctypes.data_as(C.POINTER(C.c_double)))
         return out
 
+    def adjoint_forward(self, hist: "ReplayHistory") -> tuple[float, np.ndarray]:
+        """The replay of `hist` from the current state: (J, final lattice
+        strain q^T e q of every GP)."""
+        d = hist.desc()
+        J = C.c_double(0.0)
+        eq = np.zeros(self.prob.ngps, np.float64)
+        self._call("adjoint_forward", C.byref(d), C.byref(J), eq.ctypes.data_as(C.POINTER(C.c_double)))
+        return J.value, eq
+
     def cp_stats(self) -> tuple[np.ndarray, np.ndarray]:
         it = np.zeros(self.prob.ngps, np.int32)
         er = np.zeros(self.prob.ngps, np.float64)
         self._call("get_cp_stats", abi.iptr(it),
                    er.ctypes.data_as(C.POINTER(C.c_double)))
         return it, er
+
+
+class ReplayHistory:
+    """A strain history for the adjoint replay and the objective on its end
+    state, in the layouts of ``fas_replay_desc``.
+
+    de [ninc, ngps, 6] strain increments (engineering shears), dr [ninc,
+    ngps, 3] spins, dt [ninc] time increments, w / y [ngps] weight and target
+    lattice strain of every GP, q the scattering direction, chk_every the
+    checkpoint interval of the reverse sweep."""
+
+    def __init__(self, de, dr, dt, w, y, q=(1.0, 0.0, 0.0), chk_every: int = 4):
+        f8 = np.float64
+        self.de = np.ascontiguousarray(de, f8)
+        self.dr = np.ascontiguousarray(dr, f8)
+        self.dt = np.ascontiguousarray(dt, f8).reshape(-1)
+        self.w = np.ascontiguousarray(w, f8).reshape(-1)
+        self.y = np.ascontiguousarray(y, f8).reshape(-1)
+        self.q = tuple(float(v) for v in q)
+        self.chk_every = int(chk_every)
+        ninc, ngps = self.de.shape[0], self.de.shape[1]
+        if self.de.shape != (ninc, ngps, 6) or self.dr.shape != (ninc, ngps, 3):
+            raise ValueError("de must be [ninc, ngps, 6] and dr [ninc, ngps, 3]")
+        if self.dt.shape != (ninc,) or self.w.shape != (ngps,) or self.y.shape != (ngps,):
+            raise ValueError("dt must be [ninc], w and y [ngps]")
+
+    @property
+    def ninc(self) -> int:
+        return int(self.de.shape[0])
+
+    def desc(self) -> abi.FasReplay:
+        return abi.FasReplay(self.ninc, self.chk_every, abi.ptr(self.de), abi.ptr(self.dr),
+                             abi.ptr(self.dt), abi.ptr(self.w), abi.ptr(self.y),
+                             (C.c_double * 3)(*self.q))
 
 
 def _report(rep, n) -> list[dict]:
@@ -206,6 +249,22 @@ class GpuSolver(_SolverBase):
         super().__init__(lib, prob, h)
         if upload:
             self.upload()
+
+    def adjoint_grad(self, hist: ReplayHistory) -> dict:
+        """J of the replay and its gradients: ``st`` [ngps, 6] (starting
+        stress), ``sv`` [ngps, FAS_MAXSVS] (starting Euler angles in columns
+        0-2, slip resistances from column 3), ``ampar`` [nmatl, 10] (uniform
+        shift of ampar(k) over a material's systems; k = 1, 2, 3, 5 filled)."""
+        d = hist.desc()
+        J = C.c_double(0.0)
+        ng = self.prob.ngps
+        out = dict(st=np.zeros((ng, 6)), sv=np.zeros((ng, abi.FAS_MAXSVS)),
+                   ampar=np.zeros((self.prob.nmatl, 10)))
+        dp = C.POINTER(C.c_double)
+        self._call("adjoint_grad", C.byref(d), C.byref(J), out["st"].ctypes.data_as(dp),
+                   out["sv"].ctypes.data_as(dp), out["ampar"].ctypes.data_as(dp))
+        out["J"] = J.value
+        return out
 
     def profile(self, level: int) -> dict:
         """Start device-side profiling (1: counters and region time, 2: also

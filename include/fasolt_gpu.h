@@ -52,6 +52,7 @@ extern "C" {
 #define FAS_E_TIMEOUT      (-8)  /* a device-side bounded wait gave up       */
 
 #define FAS_MAXSS  60            /* maxss, src/fasolt/fas-com-mod.f90:57     */
+#define FAS_MAXSVS 63            /* maxsvs, src/fasolt/fas-com-mod.f90:14    */
 
 /* ---- mode flags for fas_gpu_create / fas_gpu_set_mode ------------------ */
 #define FAS_MODE_PLAIN        0u  /* FP64 everywhere, reference tangent      */
@@ -240,6 +241,54 @@ FAS_API int32_t fas_gpu_get_cp_stats(fas_handle *h, int32_t *iters, double *erep
  * (column-major, element size real_bytes).  The forward map of csvmkr's
  * el_eps columns. */
 FAS_API int32_t fas_gpu_lattice_strain(fas_handle *h, void *strain, int32_t real_bytes);
+
+/* Adjoint of the constitutive update (no counterpart in the reference).
+ *
+ * A replay drives every GP through a recorded history of ninc increments:
+ * DSTRSS from the uploaded stress st and state sv with the increment's
+ * strain increment, spin and time step, then UPDATE_GPTV's commit.  Each
+ * increment starts from its own orientation and slip resistances and from
+ * the elastic predictor as the stress guess, as an increment's first
+ * Newton iteration does.  Twins are flagged but not reoriented.  The
+ * handle's own state is not changed.
+ *
+ * The objective is J = sum_g w(g) (q^T e_g q - y(g))^2 / 2, where e_g is the
+ * lattice strain S(sv(1:3)) st of GP g after the last increment (as
+ * fas_gpu_lattice_strain gives it) and q the scattering direction.  The
+ * weights select and scale GPs, e.g. 1/count for the GPs of one orientation
+ * bin and 0 elsewhere.
+ *
+ * Gradients come from the implicit function theorem at each increment's
+ * converged CPSTRS system, swept backwards over the increments from
+ * checkpoints taken every chk_every increments (a segment is recomputed
+ * from its checkpoint before it is swept).  They are exact for the replay
+ * as converged: a tight toler makes them agree with finite differences of
+ * fas_gpu_adjoint_forward.  Materials of at most 32 slip systems. */
+typedef struct fas_replay_desc {
+    int32_t ninc;          /* increments in the history (>= 1)                 */
+    int32_t chk_every;     /* checkpoint interval of the reverse sweep (>= 1)  */
+    const double *de;      /* de(6, ngps, ninc): strain increments, eng. shears */
+    const double *dr;      /* dr(3, ngps, ninc): spins, as DSTRNS returns them  */
+    const double *dt;      /* dt(ninc): time increments (tiem)                 */
+    const double *w;       /* w(ngps): objective weight of each GP             */
+    const double *y;       /* y(ngps): target lattice strain of each GP        */
+    double q[3];           /* scattering direction (normalised by the call)    */
+} fas_replay_desc;
+
+/* The replay and its objective: J, and when eq is non-null the final
+ * lattice strain q^T e_g q of every GP into eq(ngps).  Returns 0, a FAFERR
+ * code of DSTRSS, or an ABI error (FAS_E_RANGE for more than 32 systems). */
+FAS_API int32_t fas_gpu_adjoint_forward(fas_handle *h, const fas_replay_desc *d, double *J, double *eq);
+
+/* J and its gradients with respect to the replay's starting stress
+ * g_st(6, ngps), starting state g_sv(FAS_MAXSVS, ngps) (Euler angles in rows 1-3,
+ * slip resistances in rows 4..3+ns, zero elsewhere) and hardening
+ * parameters g_ampar(10, nmatl): entry k of material m is dJ/dc for
+ * ampar(k, i, m) + c on every slip system i, filled for k = 1 (rate
+ * exponent), 2, 3 and 5 (saturation stress), zero for the others.  Column-
+ * major; any of the three may be null. */
+FAS_API int32_t fas_gpu_adjoint_grad(fas_handle *h, const fas_replay_desc *d, double *J, double *g_st,
+                                     double *g_sv, double *g_ampar);
 
 /* Per-GP algorithmic operation count of the last constitutive pass (the
  * formulas of fas_flops.h summed over the iterations each GP took). */

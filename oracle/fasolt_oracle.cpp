@@ -1534,6 +1534,61 @@ template <class R> int constitutive(Problem<R> &P, int inc, int nit)
     return 0;
 }
 
+// Replay of Gauss-point strain histories (the checker of the GPU library's
+// fas_gpu_adjoint_forward, which has no counterpart in the reference): per
+// increment DSTRSS (src/fasolt/Sig_eps.f90:252-319) with dsv = 0 and the
+// elastic predictor S^-1 de as the stress guess, then the commit of
+// UPDATE_GPTV (src/fasolt/Fasolt3.f90:254-284).  Works on a copy of the
+// problem; J and the final lattice strains q^T e q (ELASEPS,
+// src/csvmkr/data_out.f90:263-361) as the GPU library defines them.
+template <class R> int replay(const Problem<R> &P0, const fas_replay_desc *d, double *J, double *eq)
+{
+    if (!d || !d->de || !d->dr || !d->dt || !d->w || !d->y || d->ninc < 1) return FAS_E_ARG;
+    if (!P0.have_state) return FAS_E_STATE;
+    const double qn = std::sqrt(d->q[0] * d->q[0] + d->q[1] * d->q[1] + d->q[2] * d->q[2]);
+    if (!(qn > 0.0)) return FAS_E_ARG;
+    const double q[3] = {d->q[0] / qn, d->q[1] / qn, d->q[2] / qn};
+    const double qq[6] = {q[0] * q[0], q[1] * q[1], q[2] * q[2], q[1] * q[2], q[2] * q[0], q[0] * q[1]};
+    Problem<R> P = P0;
+    P.tiem.assign(d->dt, d->dt + d->ninc);
+    const size_t ng = P.ngps;
+    double jsum = 0.0;
+    for (size_t g = 0; g < ng; ++g) {
+        const int iel = P.gp_iel[g];
+        const Material<R> &m = P.mat[std::abs(iel) - 1];
+        R st[6];
+        for (int k = 0; k < 6; ++k) st[k] = P.st[g * 6 + k];
+        R *sv = &P.sv[g * SVLD];
+        R *dsv = &P.dsv[g * SVLD];
+        for (int n = 0; n < d->ninc; ++n) {
+            R de[6], r[3], ds[6], t[6], chi[6][6], S[6][6], deff = 0;
+            for (int k = 0; k < 6; ++k) de[k] = (R)d->de[((size_t)n * ng + g) * 6 + k];
+            for (int k = 0; k < 3; ++k) r[k] = (R)d->dr[((size_t)n * ng + g) * 3 + k];
+            for (int k = 0; k < 3 + m.ns; ++k) dsv[k] = 0;
+            elastc(m.e, sv[0], sv[1], sv[2], S);
+            if (factor(6, &S[0][0], 6)) return 910;
+            for (int k = 0; k < 6; ++k) ds[k] = de[k];
+            solver(6, &S[0][0], 6, ds);
+            const int rc = dstrss(P, iel, (int)g, deff, de, st, ds, t, r, chi, n + 1, 1);
+            if (rc) return rc;
+            for (int k = 0; k < 6; ++k) st[k] = t[k];
+            for (int k = 0; k < 3 + m.ns; ++k) sv[k] = sv[k] + dsv[k];
+        }
+        R S[6][6];
+        elastc(m.e, sv[0], sv[1], sv[2], S);
+        double e = 0.0;
+        for (int i = 0; i < 6; ++i) {
+            double ei = 0.0;
+            for (int c = 0; c < 6; ++c) ei += (double)S[i][c] * (double)st[c];
+            e += qq[i] * ei;
+        }
+        if (eq) eq[g] = e;
+        jsum += 0.5 * d->w[g] * (e - d->y[g]) * (e - d->y[g]);
+    }
+    if (J) *J = jsum;
+    return 0;
+}
+
 struct AnyProblem {
     int rb;
     std::unique_ptr<Problem<double>> d;
@@ -1766,6 +1821,11 @@ int32_t ora_lattice_strain(ora_problem *p, double *out)
         }
     });
     return 0;
+}
+
+int32_t ora_adjoint_forward(ora_problem *p, const fas_replay_desc *d, double *J, double *eq)
+{
+    DISPATCH(p, return replay(P, d, J, eq));
 }
 
 double ora_spower(double a, double b) { return spower<double>(a, b); }

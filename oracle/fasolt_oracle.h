@@ -63,6 +63,10 @@ int32_t ora_get_cp_ops(ora_problem *p, double *ops);
 /* ELASEPS (src/csvmkr/data_out.f90:263-361): out[g*6 + k]. */
 int32_t ora_lattice_strain(ora_problem *p, double *out);
 
+/* The replay of fas_gpu_adjoint_forward (its checker): DSTRSS per
+ * increment from the elastic predictor, then UPDATE_GPTV's commit. */
+int32_t ora_adjoint_forward(ora_problem *p, const fas_replay_desc *d, double *J, double *eq);
+
 /* Low-level single-routine checks for the known-answer tests (double). */
 double  ora_spower(double a, double b);
 double  ora_fj2vom(int32_t stress, const double *x6);
