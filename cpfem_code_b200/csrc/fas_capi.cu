@@ -31,6 +31,11 @@ using namespace fasdev;
 #ifndef FAS_SOR_RCP
 #define FAS_SOR_RCP 1
 #endif
+// Constitutive passes pull their items from a device queue on a persistent
+// grid (1), or launch one thread per item (0, the tuned choice).
+#ifndef FAS_CP_QUEUE
+#define FAS_CP_QUEUE 0
+#endif
 // Constitutive kernels launched in work-sorted order (1) or natural order (0).
 #ifndef FAS_WORK_SORT
 #define FAS_WORK_SORT 1
@@ -134,6 +139,7 @@ struct fas_handle {
     DVec<double> sor_d, sor_r;   // correction and residual of the refinement
     DVec<double> rdiag;          // reciprocals of the diagonal entries, row order
     DVec<int> work_order, work_hist;   // work-sorted constitutive launch order
+    DVec<int> cp_queue;          // head of the constitutive pass's device queue
     DVec<int> gp_item;           // GP of item e*npg + g (20-node bricks; -1 for ties)
     int refine_every = 16;       // FP32 sweeps per FP64 residual
     cudaGraphExec_t sor_graph = nullptr;   // GRAPH_SWEEPS plain sweeps
@@ -886,20 +892,40 @@ const int *work_order(fas_handle *h, int n, const int *gp_of)
     return h->work_order.p;
 }
 
+// Grid of a constitutive pass over n items (for_each_item).  With the
+// queue: as many 128-thread CTAs as reside at once, at most one item per
+// thread, and the queue head zeroed; otherwise one thread per item.
+template <typename K> unsigned cp_grid(fas_handle *h, K kern, long long n, int **queue)
+{
+    *queue = nullptr;
+    const unsigned full = nblocks(n, 128);
+    if (!FAS_CP_QUEUE) return full;
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 128, 0) != cudaSuccess || occ < 1) return full;
+    if (!h->cp_queue.p && h->cp_queue.alloc(1) != cudaSuccess) return full;
+    if (cudaMemsetAsync(h->cp_queue.p, 0, sizeof(int), h->stream) != cudaSuccess) return full;
+    *queue = h->cp_queue.p;
+    return std::min<unsigned>(full, (unsigned)occ * (unsigned)h->nsm);
+}
+
 template <int NS> int launch_elem(fas_handle *h, int inc, int nit)
 {
     Span sp(h, &h->P.ms_constitutive);
     if (h->nn == 20) {   // 20-node bricks: one thread per (element, GP)
         const int *order = work_order(h, 8 * h->nlmnt, h->gp_item.p);
-        k_elem22<NS><<<nblocks(8LL * h->nlmnt, 128), 128, 0, h->stream>>>(
+        int *queue = nullptr;
+        const unsigned grid = cp_grid(h, k_elem22<NS>, 8LL * h->nlmnt, &queue);
+        k_elem22<NS><<<grid, 128, 0, h->stream>>>(
             h->mesh(), h->M, h->C, h->gp(), h->dn22.p, h->x.p, h->dx.p, h->rec.p, h->h_tiem[inc - 1], inc, nit,
-            h->ekey.p, order);
+            h->ekey.p, order, queue);
     }
     else if (!(h->mode & FAS_MODE_CP_WARP)) {
         const int *order = work_order(h, h->nlmnt, h->gpe.p);
-        k_elem<NS><<<nblocks(h->nlmnt, 128), 128, 0, h->stream>>>(
+        int *queue = nullptr;
+        const unsigned grid = cp_grid(h, k_elem<NS>, h->nlmnt, &queue);
+        k_elem<NS><<<grid, 128, 0, h->stream>>>(
             h->mesh(), h->M, h->C, h->gp(), h->x.p, h->dx.p, h->rec.p, h->h_tiem[inc - 1], inc, nit, h->ekey.p,
-            order);
+            order, queue);
     }
     else
         k_elem_wc<(NS > 12 ? 32 : 12)><<<nblocks(32LL * h->nlmnt, 128), 128, 0, h->stream>>>(
@@ -1617,20 +1643,32 @@ int32_t fas_gpu_constitutive(fas_handle *h, int32_t inc, int32_t nit)
     CK(cudaMemsetAsync(h->ekey.p, 0xFF, sizeof(unsigned long long), s));
     Span sp(h, &h->P.ms_constitutive);
     const double dt = h->h_tiem[inc - 1];
-    const unsigned nb = nblocks(h->ngps, 128);
     const unsigned nbw = nblocks(32LL * h->ngps, 128);
     const bool thr = !(h->mode & FAS_MODE_CP_WARP) || h->maxns > 32;
     const int *order = thr ? work_order(h, h->ngps, nullptr) : nullptr;
     switch (h->ns_tmpl) {
     case 12:
-        if (thr) k_points<12><<<nb, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order);
+        if (thr) {
+            int *queue = nullptr;
+            const unsigned grid = cp_grid(h, k_points<12>, h->ngps, &queue);
+            k_points<12><<<grid, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order, queue);
+        }
         else k_points_wc<12><<<nbw, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p);
         break;
     case 32:
-        if (thr) k_points<32><<<nb, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order);
+        if (thr) {
+            int *queue = nullptr;
+            const unsigned grid = cp_grid(h, k_points<32>, h->ngps, &queue);
+            k_points<32><<<grid, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order, queue);
+        }
         else k_points_wc<32><<<nbw, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p);
         break;
-    default: k_points<60><<<nb, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order); break;
+    default: {
+        int *queue = nullptr;
+        const unsigned grid = cp_grid(h, k_points<60>, h->ngps, &queue);
+        k_points<60><<<grid, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order, queue);
+        break;
+    }
     }
     sp.end();
     keep(h, sp);

@@ -80,6 +80,30 @@ struct BlockDev {
     __host__ __device__ size_t bi(int p, int s, int q) const { return (size_t)p * brow + (size_t)q * slots + s; }
 };
 
+// The items of a constitutive pass, entry t of the launch order (`order`,
+// or the natural order when it is null).  With a device queue (`queue`
+// non-null, a persistent grid) every warp takes the next 32 entries until
+// the order is exhausted, so the work-sorted order is served heaviest first
+// and no CTA slot idles behind one slow warp; otherwise thread t takes
+// entry t.
+template <typename F>
+__device__ __forceinline__ void for_each_item(int n, const int *__restrict__ order, int *queue, F &&f)
+{
+    if (queue) {
+        const int lane = threadIdx.x & 31;
+        for (;;) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(queue, 32);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base >= n) return;
+            const int t = base + lane;
+            if (t < n) f(order ? order[t] : t);
+        }
+    }
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) f(order ? order[t] : t);
+}
+
 // ---------------------------------------------------------------- element pass
 // ELVALS per element (src/fasolt/Elvals.f90:31-126): gather, SHAPE_12,
 // DSTRNS, DSTRSS, store the GP increments and the element record.
@@ -88,69 +112,69 @@ __global__ void __launch_bounds__(128) k_elem(MeshDev Mh, DevMat M, DevCtrl C, D
                                               const double *__restrict__ x,
                                               const double *__restrict__ dx, double *rec,
                                               double dt, int inc, int nit,
-                                              unsigned long long *errkey, const int *__restrict__ order)
+                                              unsigned long long *errkey, const int *__restrict__ order,
+                                              int *queue)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= Mh.nlmnt) return;
-    const int e = order ? order[t] : t;   // work-sorted element order, or the natural one
-    if (Mh.lt[e] < 9) return;   // tie element: no Gauss point
-    const int ne = Mh.nlmnt;
-    double xl[8][3], dxl[8][3];
+    for_each_item(Mh.nlmnt, order, queue, [&](int e) {
+        if (Mh.lt[e] < 9) return;   // tie element: no Gauss point
+        const int ne = Mh.nlmnt;
+        double xl[8][3], dxl[8][3];
 #pragma unroll
-    for (int a = 0; a < 8; ++a) {
-        const int n = Mh.ln[a * ne + e];
+        for (int a = 0; a < 8; ++a) {
+            const int n = Mh.ln[a * ne + e];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            xl[a][c] = x[3 * n + c];
-            dxl[a][c] = dx[3 * n + c];
+            for (int c = 0; c < 3; ++c) {
+                xl[a][c] = x[3 * n + c];
+                dxl[a][c] = dx[3 * n + c];
+            }
         }
-    }
-    double sfd[8][3];
-    const double w = shape12(xl, sfd);
-    if (w < 1.e-7) {
-        atomicMin(errkey, ((unsigned long long)e << 16) | 920ull);
-        return;
-    }
-    double del[6], r[3], defl;
-    int rc = dstrns(sfd, dxl, C.smalr, C.smale, del, r, defl);
-    if (rc) {
-        atomicMin(errkey, ((unsigned long long)e << 16) | (unsigned long long)rc);
-        return;
-    }
-    const int g = Mh.gpe[e];
-    const int ng = G.ngps;
-    double st[6], ds[6];
+        double sfd[8][3];
+        const double w = shape12(xl, sfd);
+        if (w < 1.e-7) {
+            atomicMin(errkey, ((unsigned long long)e << 16) | 920ull);
+            return;
+        }
+        double del[6], r[3], defl;
+        int rc = dstrns(sfd, dxl, C.smalr, C.smale, del, r, defl);
+        if (rc) {
+            atomicMin(errkey, ((unsigned long long)e << 16) | (unsigned long long)rc);
+            return;
+        }
+        const int g = Mh.gpe[e];
+        const int ng = G.ngps;
+        double st[6], ds[6];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        st[k] = G.st[k * ng + g];
-        ds[k] = G.ds[k * ng + g];
-    }
-    GpOut o;
-    rc = dstrss<NS>(M, C, G, g, Mh.le[e], del, r, st, ds, dt, inc, nit, o);
-    if (rc) {
-        atomicMin(errkey, ((unsigned long long)e << 16) | (unsigned long long)rc);
-        return;
-    }
-    G.dep[g] = o.deff;
+        for (int k = 0; k < 6; ++k) {
+            st[k] = G.st[k * ng + g];
+            ds[k] = G.ds[k * ng + g];
+        }
+        GpOut o;
+        rc = dstrss<NS>(M, C, G, g, Mh.le[e], del, r, st, ds, dt, inc, nit, o);
+        if (rc) {
+            atomicMin(errkey, ((unsigned long long)e << 16) | (unsigned long long)rc);
+            return;
+        }
+        G.dep[g] = o.deff;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        G.de[k * ng + g] = del[k];
-        G.ds[k * ng + g] = ds[k];
-    }
+        for (int k = 0; k < 6; ++k) {
+            G.de[k * ng + g] = del[k];
+            G.ds[k * ng + g] = ds[k];
+        }
 #pragma unroll
-    for (int k = 0; k < 3; ++k) G.dr[k * ng + g] = r[k];
-    double *R = rec + (size_t)e * REC;
+        for (int k = 0; k < 3; ++k) G.dr[k * ng + g] = r[k];
+        double *R = rec + (size_t)e * REC;
 #pragma unroll
-    for (int a = 0; a < 8; ++a)
+        for (int a = 0; a < 8; ++a)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) R[3 * a + c] = sfd[a][c];
+            for (int c = 0; c < 3; ++c) R[3 * a + c] = sfd[a][c];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) R[REC_S + k] = o.t[k];
-    R[REC_W] = w;
+        for (int k = 0; k < 6; ++k) R[REC_S + k] = o.t[k];
+        R[REC_W] = w;
 #pragma unroll
-    for (int i = 0; i < 6; ++i)
+        for (int i = 0; i < 6; ++i)
 #pragma unroll
-        for (int j = i; j < 6; ++j) R[REC_D + utri(i, j)] = o.chi[i][j];
+            for (int j = i; j < 6; ++j) R[REC_D + utri(i, j)] = o.chi[i][j];
+    });
 }
 
 // ELVALS per Gauss point of 20-node bricks (src/fasolt/Elvals.f90:82-126
@@ -167,88 +191,88 @@ __global__ void __launch_bounds__(128) k_elem22(MeshDev Mh, DevMat M, DevCtrl C,
                                                 const double *__restrict__ x,
                                                 const double *__restrict__ dx, double *rec,
                                                 double dt, int inc, int nit,
-                                                unsigned long long *errkey, const int *__restrict__ order)
+                                                unsigned long long *errkey, const int *__restrict__ order,
+                                                int *queue)
 {
     using L = RecLayout<20>;
-    const long long ti = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (ti >= 8LL * Mh.nlmnt) return;
-    const long long t = order ? order[ti] : ti;   // item e*8 + gq, work-sorted or natural
-    const int e = (int)(t >> 3), gq = (int)(t & 7);
-    if (Mh.lt[e] < 9) return;   // tie element: no Gauss point
-    const int ne = Mh.nlmnt;
-    const unsigned long long key = (unsigned long long)t << 16;
-    const double *dn = dn22 + gq * 60;
-    double jac[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    for (int i = 0; i < 20; ++i) {
-        const int n = Mh.ln[i * ne + e];
-        const double d0 = __ldg(dn + i), d1 = __ldg(dn + 20 + i), d2 = __ldg(dn + 40 + i);
+    for_each_item(8 * Mh.nlmnt, order, queue, [&](int t) {   // item e*8 + gq
+        const int e = (int)(t >> 3), gq = (int)(t & 7);
+        if (Mh.lt[e] < 9) return;   // tie element: no Gauss point
+        const int ne = Mh.nlmnt;
+        const unsigned long long key = (unsigned long long)t << 16;
+        const double *dn = dn22 + gq * 60;
+        double jac[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int i = 0; i < 20; ++i) {
+            const int n = Mh.ln[i * ne + e];
+            const double d0 = __ldg(dn + i), d1 = __ldg(dn + 20 + i), d2 = __ldg(dn + 40 + i);
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const double xk = x[3 * n + k];
-            jac[0][k] = jac[0][k] + d0 * xk;
-            jac[1][k] = jac[1][k] + d1 * xk;
-            jac[2][k] = jac[2][k] + d2 * xk;
+            for (int k = 0; k < 3; ++k) {
+                const double xk = x[3 * n + k];
+                jac[0][k] = jac[0][k] + d0 * xk;
+                jac[1][k] = jac[1][k] + d1 * xk;
+                jac[2][k] = jac[2][k] + d2 * xk;
+            }
         }
-    }
-    double inv[3][3];
-    const double w = 1.0 * invert3(jac, inv);
-    if (w < 1.e-7) {
-        atomicMin(errkey, key | 920ull);
-        return;
-    }
-    double *R = rec + (size_t)t * L::LEN;
-    double gr[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    for (int i = 0; i < 20; ++i) {
-        const int n = Mh.ln[i * ne + e];
-        const double d0 = __ldg(dn + i), d1 = __ldg(dn + 20 + i), d2 = __ldg(dn + 40 + i);
-        double sf[3];
+        double inv[3][3];
+        const double w = 1.0 * invert3(jac, inv);
+        if (w < 1.e-7) {
+            atomicMin(errkey, key | 920ull);
+            return;
+        }
+        double *R = rec + (size_t)t * L::LEN;
+        double gr[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int i = 0; i < 20; ++i) {
+            const int n = Mh.ln[i * ne + e];
+            const double d0 = __ldg(dn + i), d1 = __ldg(dn + 20 + i), d2 = __ldg(dn + 40 + i);
+            double sf[3];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            sf[k] = inv[k][0] * d0 + inv[k][1] * d1 + inv[k][2] * d2;
-            R[3 * i + k] = sf[k];
+            for (int k = 0; k < 3; ++k) {
+                sf[k] = inv[k][0] * d0 + inv[k][1] * d1 + inv[k][2] * d2;
+                R[3 * i + k] = sf[k];
+            }
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const double u = dx[3 * n + b];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) gr[a][b] = gr[a][b] + sf[a] * u;
+            }
+        }
+        double del[6], r[3], defl;
+        int rc = dstrns_grad(gr, C.smalr, C.smale, del, r, defl);
+        if (rc) {
+            atomicMin(errkey, key | (unsigned long long)rc);
+            return;
+        }
+        const int g = Mh.gpe[gq * ne + e];
+        const int ng = G.ngps;
+        double st[6], ds[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            st[k] = G.st[k * ng + g];
+            ds[k] = G.ds[k * ng + g];
+        }
+        GpOut o;
+        rc = dstrss<NS>(M, C, G, g, Mh.le[e], del, r, st, ds, dt, inc, nit, o);
+        if (rc) {
+            atomicMin(errkey, key | (unsigned long long)rc);
+            return;
+        }
+        G.dep[g] = o.deff;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            G.de[k * ng + g] = del[k];
+            G.ds[k * ng + g] = ds[k];
         }
 #pragma unroll
-        for (int b = 0; b < 3; ++b) {
-            const double u = dx[3 * n + b];
+        for (int k = 0; k < 3; ++k) G.dr[k * ng + g] = r[k];
 #pragma unroll
-            for (int a = 0; a < 3; ++a) gr[a][b] = gr[a][b] + sf[a] * u;
-        }
-    }
-    double del[6], r[3], defl;
-    int rc = dstrns_grad(gr, C.smalr, C.smale, del, r, defl);
-    if (rc) {
-        atomicMin(errkey, key | (unsigned long long)rc);
-        return;
-    }
-    const int g = Mh.gpe[gq * ne + e];
-    const int ng = G.ngps;
-    double st[6], ds[6];
+        for (int k = 0; k < 6; ++k) R[L::S + k] = o.t[k];
+        R[L::W] = w;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        st[k] = G.st[k * ng + g];
-        ds[k] = G.ds[k * ng + g];
-    }
-    GpOut o;
-    rc = dstrss<NS>(M, C, G, g, Mh.le[e], del, r, st, ds, dt, inc, nit, o);
-    if (rc) {
-        atomicMin(errkey, key | (unsigned long long)rc);
-        return;
-    }
-    G.dep[g] = o.deff;
+        for (int i = 0; i < 6; ++i)
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        G.de[k * ng + g] = del[k];
-        G.ds[k * ng + g] = ds[k];
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) G.dr[k * ng + g] = r[k];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) R[L::S + k] = o.t[k];
-    R[L::W] = w;
-#pragma unroll
-    for (int i = 0; i < 6; ++i)
-#pragma unroll
-        for (int j = i; j < 6; ++j) R[L::D + utri(i, j)] = o.chi[i][j];
+            for (int j = i; j < 6; ++j) R[L::D + utri(i, j)] = o.chi[i][j];
+    });
 }
 
 // Work-sorted launch order for the constitutive kernels: items (elements or
@@ -270,6 +294,11 @@ __global__ void k_work_hist(int n, const int *__restrict__ gp_of, const double *
     if (i >= n) return;
     atomicAdd(&hist[work_bin(gp_of ? gp_of[i] : i, ops)], 1);
 }
+// Bin offsets: heaviest bin first (FAS_WORK_DESC, the default), so the
+// tail of a pass holds the cheapest items, or lightest first.
+#ifndef FAS_WORK_DESC
+#define FAS_WORK_DESC 1
+#endif
 __global__ void __launch_bounds__(WORK_BINS) k_work_scan(int *hist)
 {
     __shared__ int v[WORK_BINS];
@@ -277,7 +306,8 @@ __global__ void __launch_bounds__(WORK_BINS) k_work_scan(int *hist)
     __syncthreads();
     if (threadIdx.x == 0) {
         int acc = 0;
-        for (int b = 0; b < WORK_BINS; ++b) {
+        for (int k = 0; k < WORK_BINS; ++k) {
+            const int b = FAS_WORK_DESC ? WORK_BINS - 1 - k : k;
             const int c = v[b];
             v[b] = acc;
             acc += c;
@@ -299,34 +329,34 @@ __global__ void k_work_scatter(int n, const int *__restrict__ gp_of, const doubl
 template <int NS>
 __global__ void __launch_bounds__(128) k_points(DevMat M, DevCtrl C, DevGp G, const int *gp_iel,
                                                 double *chi, double dt, int inc, int nit,
-                                                unsigned long long *errkey, const int *__restrict__ order)
+                                                unsigned long long *errkey, const int *__restrict__ order,
+                                                int *queue)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= G.ngps) return;
-    const int g = order ? order[t] : t;   // work-sorted point order, or the natural one
-    const int ng = G.ngps;
-    double de[6], r[3], st[6], ds[6];
+    for_each_item(G.ngps, order, queue, [&](int g) {
+        const int ng = G.ngps;
+        double de[6], r[3], st[6], ds[6];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        de[k] = G.de[k * ng + g];
-        st[k] = G.st[k * ng + g];
-        ds[k] = G.ds[k * ng + g];
-    }
+        for (int k = 0; k < 6; ++k) {
+            de[k] = G.de[k * ng + g];
+            st[k] = G.st[k * ng + g];
+            ds[k] = G.ds[k * ng + g];
+        }
 #pragma unroll
-    for (int k = 0; k < 3; ++k) r[k] = G.dr[k * ng + g];
-    GpOut o;
-    const int rc = dstrss<NS>(M, C, G, g, gp_iel[g], de, r, st, ds, dt, inc, nit, o);
-    if (rc) {
-        atomicMin(errkey, ((unsigned long long)g << 16) | (unsigned long long)rc);
-        return;
-    }
-    G.dep[g] = o.deff;
+        for (int k = 0; k < 3; ++k) r[k] = G.dr[k * ng + g];
+        GpOut o;
+        const int rc = dstrss<NS>(M, C, G, g, gp_iel[g], de, r, st, ds, dt, inc, nit, o);
+        if (rc) {
+            atomicMin(errkey, ((unsigned long long)g << 16) | (unsigned long long)rc);
+            return;
+        }
+        G.dep[g] = o.deff;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) G.ds[k * ng + g] = ds[k];
+        for (int k = 0; k < 6; ++k) G.ds[k * ng + g] = ds[k];
 #pragma unroll
-    for (int i = 0; i < 6; ++i)
+        for (int i = 0; i < 6; ++i)
 #pragma unroll
-        for (int j = 0; j < 6; ++j) chi[(i + 6 * j) * (size_t)ng + g] = o.chi[i][j];
+            for (int j = 0; j < 6; ++j) chi[(i + 6 * j) * (size_t)ng + g] = o.chi[i][j];
+    });
 }
 
 // ---------------------------------------------------------------- warp-cooperative pass
@@ -1103,7 +1133,7 @@ constexpr int TMA_LPR = FAS_TMA_LPR;         // lanes per row of 27-slot rows (a
 #define FAS_TMA_LPR81 16
 #endif
 #ifndef FAS_TMA_ROWS81
-#define FAS_TMA_ROWS81 8
+#define FAS_TMA_ROWS81 4
 #endif
 constexpr int TMA_LPR81 = FAS_TMA_LPR81;     // lanes per row of 81-slot rows
 constexpr int TMA_ROWS81 = FAS_TMA_ROWS81;   // rows per chunk of 81-slot rows
