@@ -233,6 +233,35 @@ def _state_arrays(p):
     return {n: getattr(p, n).copy() for n in ("x", "dx", "st", "sv", "ep", "ds", "cumslip")}
 
 
+AD_INC, AD_CHK = 4, 2
+
+
+def run_adjoint(g, prob, start, de, dr, dt):
+    """Time one replay and one replay-with-gradients over every GP (wall
+    clock around the synchronous calls, the history's upload included)."""
+    from cpfem_code_b200 import ReplayHistory, abi
+    hist = ReplayHistory(np.repeat(de[None], AD_INC, 0), np.repeat(dr[None], AD_INC, 0), np.full(AD_INC, dt),
+                         np.full(prob.ngps, 1.0 / prob.ngps), np.zeros(prob.ngps), q=(1.0, 0.0, 0.0),
+                         chk_every=AD_CHK)
+    g.upload(start)
+    try:
+        g.adjoint_forward(hist)   # warm-up (buffers)
+        t0 = time.perf_counter()
+        J, _ = g.adjoint_forward(hist)
+        tf = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        g.adjoint_grad(hist)
+        tg = time.perf_counter() - t0
+    except abi.FasError as e:
+        return {"error": str(e)}
+    n = prob.ngps * AD_INC
+    return {"history": f"{AD_INC} increments per GP, each the last timed increment's strain increment "
+                       f"and spin, from the state before the timed increments; checkpoints every {AD_CHK}",
+            "objective": "sum over GPs of (lattice strain along x)^2 / (2 ngps)", "J": J,
+            "forward_s": tf, "grad_s": tg, "gp_increments_per_s_forward": n / tf,
+            "gp_increments_per_s_grad": n / tg}
+
+
 def run_gpu(args):
     import torch
 
@@ -283,6 +312,7 @@ def run_gpu(args):
     value = work / t_max
     g.download()
     plain_end = _state_arrays(prob)
+    last_de, last_dr = prob.de.copy(), prob.dr.copy()   # the last timed increment's strain and spin
 
     # ---- e2e: the same increments through the ABI, state from pinned host memory
     nit_e, e2e_s, deterministic = 0, 0.0, None
@@ -302,6 +332,13 @@ def run_gpu(args):
         e2e_s = time.perf_counter() - t0
         deterministic = all(np.array_equal(v, getattr(host, k)) for k, v in plain_end.items())
     te, work_e = reduce_max_sum(dist, e2e_s, float(prob.ngps * nit_e), dev)
+
+    # ---- adjoint: every GP replays the last timed increment's strain
+    # increment and spin AD_INC times from the state at the start of the
+    # timed increments; the objective and its gradients (fas_gpu_adjoint_grad)
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = run_adjoint(g, prob, start, last_de, last_dr, float(prob.tiem[incs[-1] - 1]))
 
     # ---- tuned form: FP32 SOR sweeps with FP64 residual refinement
     tuned = None
@@ -396,6 +433,7 @@ def run_gpu(args):
                     "newton_iters": nit_e, "increments": [incs[0], incs[-1]],
                     "same_result_as_resident_run": deterministic},
             "tuned": tuned,
+            "adjoint": adjoint,
         }
         if ws == 1 and not args.no_cpu:
             # plastic state at the end of the timed increments: time the first
@@ -425,6 +463,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer (e2e) leg")
     ap.add_argument("--no-tuned", action="store_true", help="skip the tuned-form (FP32 SOR) leg")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (replay gradients) leg")
     ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, *OTHER_WORKLOADS],
                     help="the headline 64^3 workload (default) or a 20-node brick mesh")
     args = ap.parse_args()
