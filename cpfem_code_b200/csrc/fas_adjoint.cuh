@@ -170,16 +170,52 @@ template <int NS> struct AdjIn {
     Dual p[ADJ_NP];              // shifts of ampar(1), (2), (3), (5)
 };
 
+// Orientation values of one increment: CTMATRX's a and aug, ELASTC's S,
+// and the rotated slip direction and plane normal of every active system
+// (isa order).  Only the dual passes that perturb the Euler angles need
+// their derivatives; the others take these values.
+template <int NS> struct AdjOrient {
+    double a[3][3], aug[3], S[6][6], sdr[NS][3], spn[NS][3];
+};
+
+template <int NS>
+__device__ void adj_orient(const DevMat &M, int mc, int nsa, const int *isa, const double ph[3],
+                           AdjOrient<NS> &o)
+{
+    ctmatrx(ph[0], ph[1], ph[2], o.a, o.aug);
+    elastc(M.e + 9 * mc, ph[0], ph[1], ph[2], o.S);
+    const double *ab = M.ab + (size_t)mc * MAXSS * 3;
+    const double *an = M.an + (size_t)mc * MAXSS * 3;
+    for (int q = 0; q < nsa; ++q) {
+        const int i = isa[q];
+        for (int j = 0; j < 3; ++j) {
+            o.sdr[q][j] = o.a[0][j] * ab[3 * i] + o.a[1][j] * ab[3 * i + 1] + o.a[2][j] * ab[3 * i + 2];
+            o.spn[q][j] = o.a[0][j] * an[3 * i] + o.a[1][j] * an[3 * i + 1] + o.a[2][j] * an[3 * i + 2];
+        }
+    }
+}
+
 // Residuals R (6 strain rows, then the active systems in isa order) and
 // outputs Y (stress, slip resistances, Euler angles) of one increment.
+// With `oc` the orientation values come from it (their derivatives are
+// zero); without, they are formed from in.ph in dual arithmetic.
 template <int NS>
 __device__ void adj_eval(const DevMat &M, int mc, int ns, bool plastic, int nsa, const int *isa,
                          const double de[6], const double r[3], double dt, const AdjIn<NS> &in,
-                         Dual *R, Dual *Y)
+                         const AdjOrient<NS> *oc, Dual *R, Dual *Y)
 {
     Dual a[3][3], aug[3], S[6][6];
-    ctmatrx_d(in.ph, a, aug);
-    elastc_d(M.e + 9 * mc, a, S);
+    if (oc) {
+        for (int i = 0; i < 3; ++i) {
+            aug[i] = Dual(oc->aug[i]);
+            for (int j = 0; j < 3; ++j) a[i][j] = Dual(oc->a[i][j]);
+        }
+        for (int i = 0; i < 6; ++i)
+            for (int j = 0; j < 6; ++j) S[i][j] = Dual(oc->S[i][j]);
+    } else {
+        ctmatrx_d(in.ph, a, aug);
+        elastc_d(M.e + 9 * mc, a, S);
+    }
     if (!plastic) {
         // DSTRSS's elastic branch: new stress S^-1 de (Sig_eps.f90:305-313)
         double Sv[6][6], y[6];
@@ -234,8 +270,13 @@ __device__ void adj_eval(const DevMat &M, int mc, int ns, bool plastic, int nsa,
         const int i = isa[q];
         Dual sdr[3], spn[3];
         for (int j = 0; j < 3; ++j) {
-            sdr[j] = a[0][j] * ab[3 * i] + a[1][j] * ab[3 * i + 1] + a[2][j] * ab[3 * i + 2];
-            spn[j] = a[0][j] * an[3 * i] + a[1][j] * an[3 * i + 1] + a[2][j] * an[3 * i + 2];
+            if (oc) {
+                sdr[j] = Dual(oc->sdr[q][j]);
+                spn[j] = Dual(oc->spn[q][j]);
+            } else {
+                sdr[j] = a[0][j] * ab[3 * i] + a[1][j] * ab[3 * i + 1] + a[2][j] * ab[3 * i + 2];
+                spn[j] = a[0][j] * an[3 * i] + a[1][j] * an[3 * i + 1] + a[2][j] * an[3 * i + 2];
+            }
         }
         Dual b[6];
         b[0] = sdr[0] * spn[0];
@@ -339,11 +380,13 @@ __device__ int adj_step(const DevMat &M, int mc, int ns, bool plastic, const dou
     for (int k = 0; k < ADJ_NP; ++k) in.p[k] = Dual(0.0);
     Dual R[NX], Y[NX + 3];
     double A[NX * NX], lam[NX];
+    AdjOrient<NS> oc;
+    adj_orient<NS>(M, mc, nsa, isa, zph, oc);
     // x passes: columns of dR/dx, and (dY/dx)^T ybar
     for (int j = 0; j < nx; ++j) {
         Dual &xj = j < 6 ? in.s[j] : in.g[isa[j - 6]];
         xj.d = 1.0;
-        adj_eval<NS>(M, mc, ns, plastic, nsa, isa, de, r, dt, in, R, Y);
+        adj_eval<NS>(M, mc, ns, plastic, nsa, isa, de, r, dt, in, &oc, R, Y);
         xj.d = 0.0;
         double acc = 0.0;
         for (int i = 0; i < ny; ++i) acc += ybar[i] * Y[i].d;
@@ -357,7 +400,8 @@ __device__ int adj_step(const DevMat &M, int mc, int ns, bool plastic, const dou
     for (int j = 0; j < nz + ADJ_NP; ++j) {
         Dual &v = j < 6 ? in.st[j] : j < 6 + ns ? in.s0[j - 6] : j < nz ? in.ph[j - 6 - ns] : in.p[j - nz];
         v.d = 1.0;
-        adj_eval<NS>(M, mc, ns, plastic, nsa, isa, de, r, dt, in, R, Y);
+        const bool euler = j >= 6 + ns && j < nz;   // only these passes move the orientation
+        adj_eval<NS>(M, mc, ns, plastic, nsa, isa, de, r, dt, in, euler ? nullptr : &oc, R, Y);
         v.d = 0.0;
         double acc = 0.0;
         for (int i = 0; i < ny; ++i) acc += ybar[i] * Y[i].d;
