@@ -9,9 +9,61 @@ resistances; torch is the harness here, not the compute path.
 """
 from __future__ import annotations
 
+import itertools
+
+import numpy as np
 import torch
 
 from .solver import GpuSolver, ReplayHistory
+
+
+def bunge_matrix(euler: np.ndarray) -> np.ndarray:
+    """CTMATRX's a (src/fasolt/crys_math.f90:25-62) for [n, 3] Euler angles:
+    [n, 3, 3]; a crystal-frame vector v has sample-frame components a^T v
+    (as BTMATRX rotates the slip systems)."""
+    ph1, phi, ph2 = euler[:, 0], euler[:, 1], euler[:, 2]
+    c1, s1, c2, s2, c, s = np.cos(ph1), np.sin(ph1), np.cos(ph2), np.sin(ph2), np.cos(phi), np.sin(phi)
+    a = np.empty((euler.shape[0], 3, 3))
+    a[:, 0, 0] = c1 * c2 - s1 * s2 * c
+    a[:, 1, 0] = -c1 * s2 - s1 * c2 * c
+    a[:, 2, 0] = s1 * s
+    a[:, 0, 1] = s1 * c2 + c1 * s2 * c
+    a[:, 1, 1] = -s1 * s2 + c1 * c2 * c
+    a[:, 2, 1] = -c1 * s
+    a[:, 0, 2] = s2 * s
+    a[:, 1, 2] = c2 * s
+    a[:, 2, 2] = c
+    return a
+
+
+def cubic_family(hkl) -> np.ndarray:
+    """The distinct plane normals of a cubic {hkl} family (unit vectors,
+    one of each +/- pair)."""
+    out = []
+    for p in itertools.permutations(hkl):
+        for sg in itertools.product((1, -1), repeat=3):
+            v = np.array(p, float) * sg
+            v /= np.linalg.norm(v)
+            if not any(abs(abs(v @ u) - 1.0) < 1e-12 for u in out):
+                out.append(v)
+    return np.array(out)
+
+
+def bin_weights(euler: np.ndarray, normals: np.ndarray, q, tol_deg: float) -> np.ndarray:
+    """Weights of an orientation bin for the replay objective: 1/count for
+    the GPs that have a plane normal of the family (crystal frame,
+    `normals` [m, 3]) within tol_deg of the scattering direction q, 0 for
+    the others (as a diffraction measurement selects grains)."""
+    q = np.asarray(q, float) / np.linalg.norm(q)
+    n = normals / np.linalg.norm(normals, axis=1, keepdims=True)
+    a = bunge_matrix(np.asarray(euler, float))
+    sample = np.einsum("gij,mi->gmj", a, n)             # a^T n for every GP and normal
+    cosang = np.abs(sample @ q).max(axis=1)
+    inside = cosang >= np.cos(np.radians(tol_deg)) - 1e-15
+    w = np.zeros(len(cosang))
+    if inside.any():
+        w[inside] = 1.0 / inside.sum()
+    return w
 
 
 class LatticeStrainObjective(torch.autograd.Function):
