@@ -233,6 +233,20 @@ def _state_arrays(p):
     return {n: getattr(p, n).copy() for n in ("x", "dx", "st", "sv", "ep", "ds", "cumslip")}
 
 
+L2_BYTES = 126e6
+
+
+def l2_note(prob) -> str:
+    """Whether the SOR block matrix (FP64 values and column ids, the bytes
+    every sweep re-reads) exceeds the 126 MB L2."""
+    slots = 81 if int(prob.nd.max(initial=8)) == 20 else 27
+    rows = prob.nnod
+    mb = rows * ((9 * slots + 3) // 4 * 4 * 8 + (slots + 4) // 4 * 4 * 4) / 1e6
+    if mb * 1e6 > L2_BYTES:
+        return f"inputs larger than L2 ({mb:.0f} MB block matrix re-read every sweep)"
+    return f"block matrix ({mb:.0f} MB) fits in L2 and is not flushed: L2-resident rates"
+
+
 AD_INC, AD_CHK = 4, 2
 
 
@@ -399,7 +413,7 @@ def run_gpu(args):
             "data": "synthetic (seeded generator, fs3pre semantics)",
             "config": {"workload": WORKLOAD, "desc": DESC, "parallelism": f"replicas{ws}",
                        "increments": [incs[0], incs[-1]], "newton_iters": nit, "sor_sweeps": sweeps,
-                       "l2": "inputs larger than L2 (536 MB block matrix re-read every sweep)"},
+                       "l2": l2_note(prob)},
             "s_per_increment": t_max / args.steps,
             "wall_s": wall,
             "gpu_launches": int(prof["n_launches"]),
