@@ -37,10 +37,11 @@
 //
 // Reverse sweep.  Checkpoints hold the state at the start of every
 // segment of chk increments.  The reverse kernel takes the segments from
-// the last: it recomputes one from its checkpoint (the same code as the
-// forward sweep, so the same converged states), keeps each increment's
-// input state and converged system in a per-GP record buffer, and sweeps it
-// backwards.
+// the last.  The forward sweep has recorded the last segment: each
+// increment's input state and converged system, in a per-GP record buffer.
+// Every earlier segment is recomputed from its checkpoint (the forward
+// sweep's code, so the same converged states) into that buffer.  Each
+// segment is then swept backwards.
 #pragma once
 
 #include "fas_device.cuh"
@@ -523,22 +524,33 @@ __device__ __forceinline__ void replay_load(const ReplayDev &H, int n, int g, in
 // st0 the starting stress ([6][ngps]).  Writes the checkpoints
 // chk[(seg * zs + k) * ngps + g] (stress 6, Euler angles 3, slip
 // resistances), the objective share Jg and the final lattice strain eq.
+// With `rec` it also writes the last segment's records (the layout of
+// k_replay_adj), so the reverse sweep need not recompute that segment;
+// G.sv is left holding the final state.
 template <int NS>
 __global__ void __launch_bounds__(128) k_replay_fwd(DevMat M, DevCtrl C, DevGp G, const int *gp_iel,
-                                                    const double *st0, ReplayDev H, double *chk, double *Jg,
-                                                    double *eq, unsigned long long *errkey)
+                                                    const double *st0, ReplayDev H, double *chk, double *rec,
+                                                    int rs, double *Jg, double *eq, unsigned long long *errkey)
 {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     const int ng = G.ngps;
     if (g >= ng) return;
     const int iel = gp_iel[g], mc = (iel < 0 ? -iel : iel) - 1, ns = M.ns[mc];
+    const int nlast = (H.ninc - 1) / H.chk * H.chk;   // first increment of the last segment
     double st[6], de[6], r[3], xg[NS];
+    auto R = [&](int j, int k) -> double & { return rec[((size_t)j * rs + k) * ng + g]; };
     for (int k = 0; k < 6; ++k) st[k] = st0[k * ng + g];
     for (int n = 0; n < H.ninc; ++n) {
         if (n % H.chk == 0) {
             double *c = chk + (size_t)(n / H.chk) * H.zs * ng + g;
             for (int k = 0; k < 6; ++k) c[(size_t)k * ng] = st[k];
             for (int k = 0; k < 3 + ns; ++k) c[(size_t)(6 + k) * ng] = G.sv[k * ng + g];
+        }
+        const bool keep = rec && n >= nlast;
+        const int j = n - nlast;
+        if (keep) {
+            for (int k = 0; k < 6; ++k) R(j, k) = st[k];
+            for (int k = 0; k < 3 + ns; ++k) R(j, 6 + k) = G.sv[k * ng + g];
         }
         replay_load(H, n, g, ng, de, r);
         bool plastic = false;
@@ -547,6 +559,11 @@ __global__ void __launch_bounds__(128) k_replay_fwd(DevMat M, DevCtrl C, DevGp G
             atomicMin(errkey, ((unsigned long long)g << 16) | (unsigned long long)rc);
             return;
         }
+        if (keep) {
+            for (int k = 0; k < 6; ++k) R(j, H.zs + k) = st[k];
+            for (int i = 0; i < ns; ++i) R(j, H.zs + 6 + i) = xg[i];
+            R(j, H.zs + 6 + NS) = plastic ? 1.0 : 0.0;
+        }
     }
     const double ph[3] = {G.sv[g], G.sv[ng + g], G.sv[2 * ng + g]};
     double ybar[9 + NS], e;
@@ -554,7 +571,8 @@ __global__ void __launch_bounds__(128) k_replay_fwd(DevMat M, DevCtrl C, DevGp G
     eq[g] = e;
 }
 
-// Reverse sweep (above).  rec holds chk increments of records per GP:
+// Reverse sweep (above), after k_replay_fwd with records.  rec holds chk
+// increments of records per GP:
 // record j at rec[(j * rs + k) * ngps + g], rs = zs + 6 + NS + 1 rows: input
 // state (stress, Euler angles, slip resistances), converged stress,
 // signed slips, branch.  Writes the adjoints of the starting stress
@@ -575,11 +593,16 @@ __global__ void __launch_bounds__(128) k_replay_adj(DevMat M, DevCtrl C, DevGp G
     double st[6], de[6], r[3], xg[NS];
     auto R = [&](int j, int k) -> double & { return rec[((size_t)j * rs + k) * ng + g]; };
     for (int sg = nseg - 1; sg >= 0; --sg) {
-        const double *c = chk + (size_t)sg * H.zs * ng + g;
-        for (int k = 0; k < 6; ++k) st[k] = c[(size_t)k * ng];
-        for (int k = 0; k < 3 + ns; ++k) G.sv[k * ng + g] = c[(size_t)(6 + k) * ng];
         const int n0 = sg * H.chk, n1 = min(H.ninc, n0 + H.chk);
-        for (int n = n0; n < n1; ++n) {
+        if (sg == nseg - 1) {
+            // recorded by the forward sweep, which left the final state in G.sv
+            for (int k = 0; k < 6; ++k) st[k] = R(n1 - 1 - n0, H.zs + k);
+        } else {
+            const double *c = chk + (size_t)sg * H.zs * ng + g;
+            for (int k = 0; k < 6; ++k) st[k] = c[(size_t)k * ng];
+            for (int k = 0; k < 3 + ns; ++k) G.sv[k * ng + g] = c[(size_t)(6 + k) * ng];
+        }
+        for (int n = n0; n < n1 && sg < nseg - 1; ++n) {
             const int j = n - n0;
             for (int k = 0; k < 6; ++k) R(j, k) = st[k];
             for (int k = 0; k < 3 + ns; ++k) R(j, 6 + k) = G.sv[k * ng + g];

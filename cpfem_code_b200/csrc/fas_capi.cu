@@ -1436,12 +1436,14 @@ int replay_prepare(fas_handle *h, const fas_replay_desc *d, bool grad, ReplayDev
     return 0;
 }
 
+// The forward sweep; with rs > 0 it also records the last segment for
+// the reverse sweep.
 template <int NS>
-void launch_replay_fwd(fas_handle *h, const ReplayDev &H, const DevGp &G)
+void launch_replay_fwd(fas_handle *h, const ReplayDev &H, const DevGp &G, int rs)
 {
     k_replay_fwd<NS><<<nblocks(h->ngps, 128), 128, 0, h->stream>>>(h->M, h->C, G, h->gp_iel.p, h->st.p, H,
-                                                                  h->rp.chk.p, h->rp.jg.p, h->rp.eq.p,
-                                                                  h->ekey.p);
+                                                                  h->rp.chk.p, rs > 0 ? h->rp.rec.p : nullptr,
+                                                                  rs, h->rp.jg.p, h->rp.eq.p, h->ekey.p);
 }
 
 template <int NS>
@@ -1739,8 +1741,8 @@ int32_t fas_gpu_adjoint_forward(fas_handle *h, const fas_replay_desc *d, double 
     int rs = 0;
     int rc = replay_prepare(h, d, false, H, G, rs);
     if (rc) return rc;
-    if (h->ns_tmpl == 12) launch_replay_fwd<12>(h, H, G);
-    else launch_replay_fwd<32>(h, H, G);
+    if (h->ns_tmpl == 12) launch_replay_fwd<12>(h, H, G, 0);
+    else launch_replay_fwd<32>(h, H, G, 0);
     LAUNCHED(h);
     rc = replay_finish(h, J);
     if (rc) return rc;
@@ -1757,8 +1759,8 @@ int32_t fas_gpu_adjoint_grad(fas_handle *h, const fas_replay_desc *d, double *J,
     int rc = replay_prepare(h, d, true, H, G, rs);
     if (rc) return rc;
     const size_t ng = h->ngps;
-    if (h->ns_tmpl == 12) launch_replay_fwd<12>(h, H, G);
-    else launch_replay_fwd<32>(h, H, G);
+    if (h->ns_tmpl == 12) launch_replay_fwd<12>(h, H, G, rs);
+    else launch_replay_fwd<32>(h, H, G, rs);
     LAUNCHED(h);
     // the reverse sweep starts from the same twin state as the forward one
     CK(cudaMemcpyAsync(h->rp.twinsys.p, h->twinsys.p, ng * sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
