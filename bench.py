@@ -423,7 +423,7 @@ def run_gpu(args):
                 "sor_colour": prof_k["ms_sor_colour"], "total": prof_k["ms_total"]},
             "constitutive_gp_updates_per_s": prof_k["gp_updates"] / (prof_k["ms_constitutive"] / 1e3)
             if prof_k["ms_constitutive"] else None,
-            "roofline": {"kernel": "k_sor_colour", "bound": "hbm", "achieved": achieved,
+            "roofline": {"kernel": "k_sor_colour_tma", "bound": "hbm", "achieved": achieved,
                          "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
                          "peak_source": pk["source"],
                          # ncu dram__bytes_read.sum + dram__bytes_write.sum of two colour
