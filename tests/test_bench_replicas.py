@@ -44,3 +44,14 @@ def test_replica_max_time_sum_work():
 
 def test_single_rank_passthrough():
     assert bench.reduce_max_sum(None, 3.0, 7.0) == (3.0, 7.0)
+
+
+def test_l2_note_per_workload():
+    """The bench says whether the SOR matrix exceeds the 126 MB L2: the
+    64^3 cube (567 MB) and 32^3 20-node bricks stream from HBM, the sample
+    mesh does not."""
+    import bench
+    from cpfem_code_b200 import generator
+    assert bench.l2_note(generator.workload("cube64")).startswith("inputs larger than L2 (567 MB")
+    assert bench.l2_note(generator.workload("brick20_32")).startswith("inputs larger than L2")
+    assert "fits in L2" in bench.l2_note(generator.workload("brick20_10"))
