@@ -260,8 +260,9 @@ FAS_API int32_t fas_gpu_lattice_strain(fas_handle *h, void *strain, int32_t real
  *
  * Gradients come from the implicit function theorem at each increment's
  * converged CPSTRS system, swept backwards over the increments from
- * checkpoints taken every chk_every increments (a segment is recomputed
- * from its checkpoint before it is swept).  They are exact for the replay
+ * checkpoints taken every chk_every increments (the forward sweep keeps
+ * the last segment; each earlier one is recomputed from its checkpoint
+ * before it is swept).  They are exact for the replay
  * as converged: a tight toler makes them agree with finite differences of
  * fas_gpu_adjoint_forward.  Materials of at most 32 slip systems. */
 typedef struct fas_replay_desc {
