@@ -6,6 +6,6 @@ conditions and multicolour SOR of gabortimar/CPFEM_code's ``fasolt3``
 """
 from . import abi, generator  # noqa: F401
 from .problem import Control, Problem  # noqa: F401
-from .solver import GpuSolver, ReplayHistory, load_library, LIB_PATH  # noqa: F401
+from .solver import GpuSolver, NewtonStepper, ReplayHistory, load_library, LIB_PATH  # noqa: F401
 
-__all__ = ["abi", "generator", "Control", "Problem", "GpuSolver", "load_library", "LIB_PATH"]
+__all__ = ["abi", "generator", "Control", "Problem", "GpuSolver", "NewtonStepper", "load_library", "LIB_PATH"]

@@ -32,6 +32,8 @@ FAS_MODE_SOR_FP32 = 1
 FAS_MODE_SOR_NATURAL = 2
 FAS_MODE_SOR_GRID = 4
 FAS_MODE_CP_WARP = 8
+FAS_MODE_SOR_TILES = 16
+FAS_MODE_TANGENT_CONSISTENT = 32
 
 #: FAFERR codes the hot path raises, with the reference's meaning.
 FAFERR_TEXT = {
@@ -172,6 +174,8 @@ def declare(lib: C.CDLL, prefix: str) -> None:
         "suvals": (i32, [H, i32]),
         "facsls": (i32, [H, _i32p, C.POINTER(C.c_double)]),
         "nriter": (i32, [H, i32, C.POINTER(FasIterReport), i32, _i32p]),
+        "nr_step": (i32, [H, i32, i32, C.POINTER(FasIterReport), _i32p]),
+        "nr_finish": (i32, [H, i32]),
         "update_gptv": (i32, [H]),
         "reorient": (i32, [H, i32, C.POINTER(FasTwinEvent), i32, _i32p]),
         "increment": (i32, [H, i32, C.POINTER(FasIterReport), i32, _i32p,

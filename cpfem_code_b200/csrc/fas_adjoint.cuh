@@ -136,7 +136,7 @@ __device__ __forceinline__ void elastc_d(const double *e, const Dual a0[3][3], D
         for (int J = I + 1; J < 6; ++J) S[J][I] = S[I][J];
 }
 
-// TENS_ROT (src/fasolt/Sig_eps.f90:334-370) of a dual tensor by a fixed spin
+// TENS_ROT (src/fasolt/Sig_eps.f90:166-202) of a dual tensor by a fixed spin
 __device__ __forceinline__ void tens_rot_d(const double r[3], const Dual a[6], Dual b[6])
 {
     double rot[3][3];
@@ -218,7 +218,7 @@ __device__ void adj_eval(const DevMat &M, int mc, int ns, bool plastic, int nsa,
         elastc_d(M.e + 9 * mc, a, S);
     }
     if (!plastic) {
-        // DSTRSS's elastic branch: new stress S^-1 de (Sig_eps.f90:305-313)
+        // DSTRSS's elastic branch: new stress S^-1 de (Sig_eps.f90:137-145)
         double Sv[6][6], y[6];
         for (int i = 0; i < 6; ++i) {
             y[i] = de[i];

@@ -36,6 +36,7 @@ struct DevMat {
 struct DevCtrl {
     double toler, alpha, afactor, efix, smale, smalr;
     int maxit;
+    int tangent;                // 1: consistent tangent at the converged stress
     unsigned long long seed;
 };
 
@@ -51,7 +52,7 @@ struct DevGp {
 
 __device__ __forceinline__ double ld_ro(const double *p) { return __ldg(p); }
 
-// FJ2VOM, src/fasolt/Sig_eps.f90:385-409
+// FJ2VOM, src/fasolt/Sig_eps.f90:217-241
 __device__ __forceinline__ double fj2vom(bool stress, const double *x)
 {
     const double amult = stress ? 6.0 : 1.5;
@@ -207,7 +208,7 @@ __device__ __forceinline__ void elastc(const double *e, double ph1, double phi, 
         for (int J = I + 1; J < 6; ++J) S[J][I] = S[I][J];
 }
 
-// TENS_ROT, src/fasolt/Sig_eps.f90:334-370: R^T a R for the small spin r.
+// TENS_ROT, src/fasolt/Sig_eps.f90:166-202: R^T a R for the small spin r.
 __device__ __forceinline__ void tens_rot(const double r[3], const double a[6], double b[6])
 {
     double rot[3][3], old[3][3], tmp[3][3];
@@ -305,7 +306,7 @@ __device__ __forceinline__ double invert3(const double jac[3][3], double inv[3][
     return det;
 }
 
-// DSTRNS (src/fasolt/Sig_eps.f90:193-229) from the displacement gradient
+// DSTRNS (src/fasolt/Sig_eps.f90:25-61) from the displacement gradient
 // g[a][b] = sum_i sfd(a,i) dxl(b,i).  Returns 0, 905 or 906.
 __device__ __forceinline__ int dstrns_grad(const double g[3][3], double smalr, double smale, double del[6],
                                            double r[3], double &deff)
@@ -325,7 +326,7 @@ __device__ __forceinline__ int dstrns_grad(const double g[3][3], double smalr, d
     return 0;
 }
 
-// DSTRNS, src/fasolt/Sig_eps.f90:193-229.  Returns 0, 905 or 906.
+// DSTRNS, src/fasolt/Sig_eps.f90:25-61.  Returns 0, 905 or 906.
 __device__ __forceinline__ int dstrns(const double sfd[8][3], const double dxl[8][3],
                                       double smalr, double smale, double del[6], double r[3],
                                       double &deff)
@@ -588,7 +589,7 @@ struct GpOut {
 };
 
 // CPSTRS (src/fasolt/Cpstrs.f90:34-172) inside DSTRSS
-// (src/fasolt/Sig_eps.f90:252-319).  Reads sv/dsv of GP g, updates dsv,
+// (src/fasolt/Sig_eps.f90:84-151).  Reads sv/dsv of GP g, updates dsv,
 // srate and the twin flag, returns 0 or a FAFERR code.
 template <int NS>
 __device__ int dstrss(const DevMat &M, const DevCtrl &C, const DevGp &G, int g, int iel,
@@ -680,6 +681,39 @@ __device__ int dstrss(const DevMat &M, const DevCtrl &C, const DevGp &G, int g, 
         G.erepmd[g] = erepmd;
         double dp1, dph, dp2;
         echrot<NS>(w, a, aug, r, dp1, dph, dp2);
+        G.dsv[g] = dp1;
+        G.dsv[ng + g] = dph;
+        G.dsv[2 * ng + g] = dp2;
+        for (int i = 0; i < w.ns; ++i) G.dsv[(3 + i) * ng + g] = w.s1[i] - w.s0[i];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) o.t[i] = s[i];
+        o.deff = fj2vom(false, epl);
+        if (C.tangent) {
+            // the consistent tangent: (B X^-1 B^T + S)^-1 of the local
+            // system at the converged stress -- its slip stresses, and the
+            // slips and hardening that satisfy the flow rule there (SLPFTA
+            // from the last slips, same active set) -- instead of the
+            // Jacobian of the last iterate.  The outputs above are kept.
+            for (int i = 0; i < w.ns; ++i)
+                w.tau[i] = w.b[i][0] * s[0] + w.b[i][1] * s[1] + w.b[i][2] * s[2] +
+                           w.b[i][3] * s[3] + w.b[i][4] * s[4] + w.b[i][5] * s[5];
+            int ninner = 0;
+            rc = slpfta<NS>(M, w, C, dt, ninner);
+            if (rc) return rc;
+            const int n = w.nsa;
+            if (lu_factor_n(n, w.ah)) return 910;
+            for (int j = 0; j < 6; ++j) {
+                double wk[NS];
+                for (int k = 0; k < n; ++k) wk[k] = w.b[w.isa[k]][j];
+                lu_solve_n(n, w.ah, wk);
+                for (int i = 0; i < 6; ++i) {
+                    double sum = 0.0;
+                    for (int k = 0; k < n; ++k) sum = sum + w.b[w.isa[k]][i] * wk[k];
+                    djac[i][j] = sum + S[i][j];
+                }
+            }
+            if (lu_factor<6>(6, &djac[0][0])) return 910;
+        }
 #pragma unroll
         for (int i = 0; i < 6; ++i) {
             double e6[6] = {0, 0, 0, 0, 0, 0};
@@ -688,13 +722,6 @@ __device__ int dstrss(const DevMat &M, const DevCtrl &C, const DevGp &G, int g, 
 #pragma unroll
             for (int j = 0; j < 6; ++j) o.chi[j][i] = e6[j];
         }
-        G.dsv[g] = dp1;
-        G.dsv[ng + g] = dph;
-        G.dsv[2 * ng + g] = dp2;
-        for (int i = 0; i < w.ns; ++i) G.dsv[(3 + i) * ng + g] = w.s1[i] - w.s0[i];
-#pragma unroll
-        for (int i = 0; i < 6; ++i) o.t[i] = s[i];
-        o.deff = fj2vom(false, epl);
 #pragma unroll
         for (int i = 0; i < 6; ++i)
 #pragma unroll

@@ -234,7 +234,7 @@ __device__ __forceinline__ void symmetrise_rows(int lane, double row[6])
     for (int c = 0; c < 6; ++c) row[c] = (row[c] + col[c]) / 2.0;
 }
 
-// DSTRSS (Sig_eps.f90:252-319) with CPSTRS (Cpstrs.f90:34-172) for GP g,
+// DSTRSS (Sig_eps.f90:84-151) with CPSTRS (Cpstrs.f90:34-172) for GP g,
 // executed by one whole warp.  Every lane returns the same code.
 // NA bounds the number of active systems (and slip systems) of any material.
 template <int NA>

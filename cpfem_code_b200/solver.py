@@ -112,6 +112,18 @@ class _SolverBase:
             self.last_report = _report(rep, min(n.value, cap))
         return self.last_report
 
+    def nr_step(self, inc: int, nit: int):
+        """One pass of NRITER's loop body (src/fasolt/Stif_sol.f90:32-77);
+        returns (report line, whether NRITER would go on)."""
+        r = abi.FasIterReport()
+        more = C.c_int32(0)
+        self._call("nr_step", inc, nit, C.byref(r), C.byref(more))
+        return _report([r], 1)[0], bool(more.value)
+
+    def nr_finish(self, inc: int) -> None:
+        """NRITER's cumslip update after its loop (Stif_sol.f90:80-84)."""
+        self._call("nr_finish", inc)
+
     def update_gptv(self) -> None:
         self._call("update_gptv")
 
@@ -223,6 +235,39 @@ class ReplayHistory:
         return abi.FasReplay(self.ninc, self.chk_every, abi.ptr(self.de), abi.ptr(self.dr),
                              abi.ptr(self.dt), abi.ptr(self.w), abi.ptr(self.y),
                              (C.c_double * 3)(*self.q))
+
+
+class NewtonStepper:
+    """The driver loop of src/fasolt/Fasolt3.f90:38-46 advanced one global
+    Newton iteration at a time, on any solver with this module's methods
+    (the device solver, or the checker's).
+
+    A step is one pass of NRITER's loop body (Stif_sol.f90:32-77), preceded
+    by UPDATE_NODE when it opens an increment; when NRITER would stop, the
+    step also closes the increment: NRITER's cumslip tail, UPDATE_GPTV and
+    DoReorient.  Two solvers stepped from the same state take the same
+    sequence of Newton iterations, whatever increments they span."""
+
+    def __init__(self, solver, inc: int = 1):
+        self.s = solver
+        self.inc = inc
+        self.nit = 0
+        self.reports: list[dict] = []
+
+    def step(self) -> dict:
+        if self.nit == 0:
+            self.s.update_node()
+        self.nit += 1
+        r, more = self.s.nr_step(self.inc, self.nit)
+        r = dict(r, inc=self.inc, closes_increment=not more)
+        self.reports.append(r)
+        if not more:
+            self.s.nr_finish(self.inc)
+            self.s.update_gptv()
+            self.s.do_reorient(self.inc)
+            self.inc += 1
+            self.nit = 0
+        return r
 
 
 def _report(rep, n) -> list[dict]:

@@ -65,6 +65,20 @@ extern "C" {
 #define FAS_MODE_SOR_GRID     4u  /* always use the grid-wide SOR launches,
                                      also for meshes small enough for the
                                      one-CTA solve                          */
+#define FAS_MODE_TANGENT_CONSISTENT 32u  /* element tangent (B X^-1 B^T + S)^-1
+                                     of the local system re-evaluated at
+                                     the converged stress (the implicit-
+                                     function derivative of the converged
+                                     CPSTRS update, no counterpart in the
+                                     reference) instead of CPSTRS's chi of
+                                     the last iterate (Cpstrs.f90:154-162);
+                                     symmetrised like chi                  */
+#define FAS_MODE_SOR_TILES   16u  /* grid-wide SOR as one persistent launch
+                                     per solve: spatial tiles of rows, one
+                                     per SM, that start each colour once
+                                     their neighbour tiles have finished the
+                                     previous one (8-node bricks; other
+                                     meshes keep one launch per colour)     */
 
 /*
  * Mesh: the FAS_COM element and node tables.
@@ -191,6 +205,19 @@ FAS_API int32_t fas_gpu_facsls(fas_handle *h, int32_t *sweeps, double *error);
  * are written to `rep` (may be null); *n_rep receives the iteration count. */
 FAS_API int32_t fas_gpu_nriter(fas_handle *h, int32_t inc, fas_iter_report *rep,
                        int32_t cap, int32_t *n_rep);
+
+/* One pass of NRITER's loop body, src/fasolt/Stif_sol.f90:32-77: ELVALS,
+ * SUVALS, the residual norm, FACSLS, the damping factor and the correction
+ * of x and dx, for a driver that keeps its own Newton loop (ITEREP after
+ * every pass).  `nit` is the 1-based iteration number; *more receives the
+ * reference's loop condition (sdx >= toler and nit < maxit).  After the last
+ * pass call fas_gpu_nr_finish.  fas_gpu_nriter is this loop. */
+FAS_API int32_t fas_gpu_nr_step(fas_handle *h, int32_t inc, int32_t nit, fas_iter_report *rep,
+                        int32_t *more);
+
+/* NRITER's tail after its loop, src/fasolt/Stif_sol.f90:80-84: cumslip +=
+ * srate * tiem(inc) over nss(mat_code) of the last element evaluated. */
+FAS_API int32_t fas_gpu_nr_finish(fas_handle *h, int32_t inc);
 
 /* UPDATE_GPTV, src/fasolt/Fasolt3.f90:254-284. */
 FAS_API int32_t fas_gpu_update_gptv(fas_handle *h);
@@ -327,20 +354,24 @@ FAS_API int32_t fas_gpu_profile(fas_handle *h, int32_t enable, fas_profile *out)
  * (it instantiates a CUDA graph of its sweeps), which can then fail in
  * the middle of a run; this entry point never does.
  *
- * What it does: the same solve as fas_gpu_facsls -- same kernels, colour
- * order, sweep count and stopping test, same return codes (903, 904,
+ * What it does: the same solve as fas_gpu_facsls -- the same iterates
+ * (one launch per colour, the colour order, the reciprocal-diagonal
+ * quotients), sweep count and stopping test, same return codes (903, 904,
  * FAS_E_TIMEOUT) -- on the FP64 blocks, with the kernels' scratch (the
  * stopping-test control words and one pair of partial sums per colour
  * CTA) in a static device array of this library instead of buffers of the
- * handle.  It ignores FAS_MODE_SOR_FP32 and is not timed by
- * fas_gpu_profile.
+ * handle.  It ignores FAS_MODE_SOR_FP32 and FAS_MODE_SOR_TILES and is not
+ * timed by fas_gpu_profile.  It reads the stopping flag between chunks of
+ * sweeps, so it synchronises the handle's stream before it returns.
  *
  * Limits and rules:
- *  - the array holds FAS_NOALLOC_PARTIALS partial pairs (131,328 bytes per
+ *  - the array holds FAS_NOALLOC_PARTIALS partial pairs (262,400 bytes per
  *    device, held by every GPU that loads the library until the process
- *    exits); a handle whose layout needs more (colours x CTAs per colour;
- *    a structured brick mesh on a 148-SM B200 needs 8 x 592) gets
- *    FAS_E_RANGE;
+ *    exits); a handle whose layout needs more (colours x colour-kernel CTAs
+ *    per colour) gets FAS_E_RANGE.  On a 148-SM B200 the 64^3 8-node cube
+ *    needs 8 x 888 = 7,104 pairs and the 32^3 20-node brick mesh about
+ *    15 x 592 = 8,880; meshes of 27-slot rows with more than 18 colours,
+ *    or of 81-slot rows with more than 27, can exceed the array;
  *  - the first call on each device looks up the array's device address
  *    (cudaGetSymbolAddress, with the handle's device made current for the
  *    look-up); make that first call before any stream capture begins;
@@ -351,7 +382,7 @@ FAS_API int32_t fas_gpu_profile(fas_handle *h, int32_t enable, fas_profile *out)
  *  - there is one array per device and process, so calls that overlap in
  *    time on the same device (two host threads, two handles) race on it:
  *    the caller must serialise them. */
-#define FAS_NOALLOC_PARTIALS 8192
+#define FAS_NOALLOC_PARTIALS 16384
 FAS_API int32_t fas_gpu_facsls_noalloc(fas_handle *h, int32_t *sweeps, double *error);
 
 #ifdef __cplusplus

@@ -88,7 +88,7 @@ template <class R> struct Problem {
 };
 
 // ================================================================ crystal math
-// FJ2VOM, src/fasolt/Sig_eps.f90:385-409
+// FJ2VOM, src/fasolt/Sig_eps.f90:217-241
 template <class R> R fj2vom(bool stress, const R *x)
 {
     const R amult = stress ? R(6.0) : R(1.5);
@@ -194,7 +194,7 @@ template <class R> void elastc(const R e[9], R ph1, R phi, R ph2, R S[6][6])
         for (int js = is + 1; js < 6; ++js) S[js][is] = S[is][js];
 }
 
-// TENS_ROT, src/fasolt/Sig_eps.f90:334-370: R^T a R for small rotation r.
+// TENS_ROT, src/fasolt/Sig_eps.f90:166-202: R^T a R for small rotation r.
 template <class R> void tens_rot(const R r[3], const R a[6], R b[6])
 {
     R rot[3][3], old[3][3], tmp[3][3], nw[3][3];
@@ -655,21 +655,47 @@ int cpstrs(Problem<R> &P, int jgp, const Material<R> &m, const R S[6][6], const 
     P.cp_iters[jgp] = iter;
     R dp1, dph, dp2;
     echrot(w, a, aug, rl, dp1, dph, dp2);
+    dsv[0] = dp1;
+    dsv[1] = dph;
+    dsv[2] = dp2;
+    for (int i = 0; i < w.ns; ++i) dsv[i + 3] = w.s1[i] - w.s0[i];
+    P.ops_gp[jgp] = ops;
+    if (P.mode & FAS_MODE_TANGENT_CONSISTENT) {
+        // the consistent tangent: (B X^-1 B^T + S)^-1 of the local system at
+        // the converged stress -- its slip stresses, the slips and hardening
+        // that satisfy the flow rule there (SLPFTA from the last slips, same
+        // active set) -- instead of the Jacobian of the last iterate
+        for (int i = 0; i < w.ns; ++i) {
+            R acc = 0;
+            for (int k = 0; k < 6; ++k) acc = acc + w.b[i][k] * s[k];
+            w.tau[i] = acc;
+        }
+        int ninner = 0;
+        int rc = slpfta(P, w, dt, ninner);
+        if (rc) return rc;
+        const int n = w.nsa;
+        if (factor(n, w.ah, MAXSS)) return 910;
+        for (int j = 0; j < 6; ++j) {
+            for (int k = 0; k < n; ++k) w.wks[k] = w.b[w.isa[k]][j];
+            solver(n, w.ah, MAXSS, w.wks);
+            for (int i = 0; i < 6; ++i) {
+                R sum = 0;
+                for (int k = 0; k < n; ++k) sum = sum + w.b[w.isa[k]][i] * w.wks[k];
+                djac[i][j] = sum + S[i][j];
+            }
+        }
+        if (factor(6, &djac[0][0], 6)) return 910;
+    }
     for (int i = 0; i < 6; ++i) {
         R e[6] = {0, 0, 0, 0, 0, 0};
         e[i] = R(1.0);
         solver(6, &djac[0][0], 6, e);
         for (int j = 0; j < 6; ++j) chi[j][i] = e[j];
     }
-    dsv[0] = dp1;
-    dsv[1] = dph;
-    dsv[2] = dp2;
-    for (int i = 0; i < w.ns; ++i) dsv[i + 3] = w.s1[i] - w.s0[i];
-    P.ops_gp[jgp] = ops;
     return 0;
 }
 
-// DSTRSS, src/fasolt/Sig_eps.f90:252-319 (the `es` argument is unused there).
+// DSTRSS, src/fasolt/Sig_eps.f90:84-151 (the `es` argument is unused there).
 // ds in/out, t out (the new stress), chi out; deff out.
 template <class R>
 int dstrss(Problem<R> &P, int iel, int jgp, R &deff, const R de[6], const R st[6], R ds[6],
@@ -722,7 +748,7 @@ int dstrss(Problem<R> &P, int iel, int jgp, R &deff, const R de[6], const R st[6
     return 0;
 }
 
-// DSTRNS, src/fasolt/Sig_eps.f90:193-229.  sfd[i][a] = sfd(a+1,i+1),
+// DSTRNS, src/fasolt/Sig_eps.f90:25-61.  sfd[i][a] = sfd(a+1,i+1),
 // dxl[i][b] = dxl(b+1,i+1).  Returns 0, 905 or 906.
 template <class R>
 int dstrns(const Problem<R> &P, int npl, const R (*sfd)[3], const R (*dxl)[3], R del[6],
@@ -1202,6 +1228,8 @@ template <class R> int nr_step(Problem<R> &P, int inc, int nit, fas_iter_report 
     return 0;
 }
 
+template <class R> void nr_finish(Problem<R> &P, int inc);
+
 // NRITER, src/fasolt/Stif_sol.f90:10-88 (ITEREP lines go to `rep`).
 template <class R>
 int nriter(Problem<R> &P, int inc, fas_iter_report *rep, int cap, int *n_rep)
@@ -1217,14 +1245,20 @@ int nriter(Problem<R> &P, int inc, fas_iter_report *rep, int cap, int *n_rep)
         if (rep && nit <= cap) rep[nit - 1] = r;
     }
     if (n_rep) *n_rep = nit;
-    // cumslip over nss(mat_code) of the last material touched (Stif_sol.f90:80-84)
+    nr_finish(P, inc);
+    return 0;
+}
+
+// NRITER's tail after its loop: cumslip over nss(mat_code) of the last
+// material touched (Stif_sol.f90:80-84).
+template <class R> void nr_finish(Problem<R> &P, int inc)
+{
     const int nsc = P.mat[P.last_mat - 1].ns;
     const R tm = P.tiem[inc - 1];
     for (int g = 0; g < P.ngps; ++g)
         for (int k = 0; k < nsc; ++k)
             P.cumslip[(size_t)g * MAXSS + k] =
                 P.cumslip[(size_t)g * MAXSS + k] + (P.srate[(size_t)g * MAXSS + k] * tm);
-    return 0;
 }
 
 // UPDATE_GPTV, src/fasolt/Fasolt3.f90:254-284
@@ -1536,7 +1570,7 @@ template <class R> int constitutive(Problem<R> &P, int inc, int nit)
 
 // Replay of Gauss-point strain histories (the checker of the GPU library's
 // fas_gpu_adjoint_forward, which has no counterpart in the reference): per
-// increment DSTRSS (src/fasolt/Sig_eps.f90:252-319) with dsv = 0 and the
+// increment DSTRSS (src/fasolt/Sig_eps.f90:84-151) with dsv = 0 and the
 // elastic predictor S^-1 de as the stress guess, then the commit of
 // UPDATE_GPTV (src/fasolt/Fasolt3.f90:254-284).  Works on a copy of the
 // problem; J and the final lattice strains q^T e q (ELASEPS,
@@ -1699,6 +1733,15 @@ int32_t ora_nr_step(ora_problem *p, int32_t inc, int32_t nit, fas_iter_report *r
         int rc = nr_step(P, inc, nit, rep, &m);
         if (more) *more = m ? 1 : 0;
         return rc;
+    });
+}
+int32_t ora_nr_finish(ora_problem *p, int32_t inc)
+{
+    DISPATCH(p, {
+        if (!P.have_state || P.nlmnt == 0) return FAS_E_STATE;
+        if (inc < 1 || inc > P.ninc1) return FAS_E_ARG;
+        nr_finish(P, inc);
+        return 0;
     });
 }
 int32_t ora_update_gptv(ora_problem *p)

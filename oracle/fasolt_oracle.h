@@ -44,6 +44,8 @@ int32_t ora_nriter(ora_problem *p, int32_t inc, fas_iter_report *rep,
 /* One pass of NRITER's loop body; *more = 1 when NRITER would go on. */
 int32_t ora_nr_step(ora_problem *p, int32_t inc, int32_t nit, fas_iter_report *rep,
                     int32_t *more);
+/* NRITER's cumslip update after its loop. */
+int32_t ora_nr_finish(ora_problem *p, int32_t inc);
 int32_t ora_update_gptv(ora_problem *p);
 int32_t ora_reorient(ora_problem *p, int32_t inc, fas_twin_event *ev,
                      int32_t cap, int32_t *n_ev);

@@ -40,9 +40,6 @@ def _load() -> C.CDLL:
         lib.ora_facsls_limited.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_int32),
                                            C.POINTER(C.c_double)]
         lib.ora_facsls_limited.restype = C.c_int32
-        lib.ora_nr_step.argtypes = [C.c_void_p, C.c_int32, C.c_int32,
-                                    C.POINTER(abi.FasIterReport), C.POINTER(C.c_int32)]
-        lib.ora_nr_step.restype = C.c_int32
         for name, args, res in (
                 ("ora_spower", [C.c_double, C.c_double], C.c_double),
                 ("ora_fj2vom", [C.c_int32, C.POINTER(C.c_double)], C.c_double),
@@ -81,14 +78,6 @@ class OracleSolver(_SolverBase):
 
     def set_threads(self, n: int) -> None:
         self._lib.ora_set_threads(self._h, n)
-
-    def nr_step(self, inc: int, nit: int):
-        """One Newton iteration (NRITER's loop body); returns (report, more)."""
-        r = abi.FasIterReport()
-        more = C.c_int32(0)
-        abi.check(self._lib.ora_nr_step(self._h, inc, nit, C.byref(r), C.byref(more)), "ora_nr_step")
-        return dict(nit=r.nit, sor_sweeps=r.sor_sweeps, sdx=r.sdx, sfc=r.sfc, cp_err=r.cp_err,
-                    alp2=r.alp2, sor_error=r.sor_error), bool(more.value)
 
     def facsls_limited(self, max_sweeps: int):
         s, e = C.c_int32(0), C.c_double(0.0)

@@ -223,7 +223,7 @@ def _point_problem(n, toler=1e-3, iel=1, seed=4, h0=150.0):
 
 
 def test_elastic_only_point_is_hooke(oracle_lib):
-    """DSTRSS's elastic branch (Sig_eps.f90:298-313): t = S(phi)^-1 de."""
+    """DSTRSS's elastic branch (Sig_eps.f90:130-145): t = S(phi)^-1 de."""
     from oracle import OracleSolver
     p, mat = _point_problem(32, iel=-1)
     st0 = p.st.copy()
