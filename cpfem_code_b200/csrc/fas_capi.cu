@@ -13,6 +13,7 @@
 
 #include "../../include/fasolt_gpu.h"
 #include "fas_kernels.cuh"
+#include "fas_sor_tiles.cuh"
 #include "fas_adjoint.cuh"
 
 #include <algorithm>
@@ -141,6 +142,13 @@ struct fas_handle {
     DVec<int> work_order, work_hist;   // work-sorted constitutive launch order
     DVec<int> cp_queue;          // head of the constitutive pass's device queue
     DVec<int> gp_item;           // GP of item e*npg + g (20-node bricks; -1 for ties)
+    // tile layout of the persistent SOR solve (k_sor_tiles; 27-slot rows)
+    int ntiles = 0;
+    DVec<int> tseg, tadj_ptr, tadj, tsrc, tbcol, tprog;
+    DVec<double> tblk64, trdiag, tpart, sol_scr;
+    DVec<float> tblk32;
+    DVec<TileSync> tsync;
+    int tile_keep_rows = 0;      // rows per tile whose blocks stay in L2 across sweeps
     int refine_every = 16;       // FP32 sweeps per FP64 residual
     cudaGraphExec_t sor_graph = nullptr;   // GRAPH_SWEEPS plain sweeps
     cudaGraphExec_t sor32_graph = nullptr; // one refinement cycle of the FP32 form
@@ -324,6 +332,9 @@ int greedy_colouring(fas_handle *h, const std::vector<double> &xyz)
     return 0;
 }
 
+int build_tiles(fas_handle *h, const std::vector<double> &xyz, const std::vector<int> &bcol_host,
+                const std::vector<int> &nslot_host, const std::vector<int> &rowof_host);
+
 // Row permutation by colour, node block neighbourhoods and the per-slot
 // element-local index words; allocates the block matrix.
 int build_layout(fas_handle *h, const std::vector<double> &xyz)
@@ -449,6 +460,118 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
     CK(h->d_cstart.put(h->col_start.data(), h->ncol + 1, s));
     h->sor_small = nn <= (h->slots == SLOTS ? SOR_SMALL_ROWS : SOR_SMALL_ROWS81);
     CK(cudaStreamSynchronize(s));
+    return build_tiles(h, xyz, bcol, nslot, rowof);
+}
+
+// Recursive coordinate bisection of nodes[lo, hi) into nt tiles t0 ..
+// t0 + nt - 1 of (nearly) equal node counts: cut across the longest extent
+// of the bounding box, in proportion to the tiles on each side.
+void rcb_tiles(std::vector<int> &nodes, int lo, int hi, int t0, int nt, const std::vector<double> &xyz,
+               std::vector<int> &tile_of)
+{
+    if (nt <= 1 || hi - lo <= 1) {
+        for (int k = lo; k < hi; ++k) tile_of[nodes[k]] = t0;
+        return;
+    }
+    double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+    for (int k = lo; k < hi; ++k)
+        for (int c = 0; c < 3; ++c) {
+            mn[c] = std::min(mn[c], xyz[3 * (size_t)nodes[k] + c]);
+            mx[c] = std::max(mx[c], xyz[3 * (size_t)nodes[k] + c]);
+        }
+    int ax = 0;
+    for (int c = 1; c < 3; ++c)
+        if (mx[c] - mn[c] > mx[ax] - mn[ax]) ax = c;
+    const int ntl = nt / 2;
+    const int cut = lo + (int)((long long)(hi - lo) * ntl / nt);
+    std::nth_element(nodes.begin() + lo, nodes.begin() + cut, nodes.begin() + hi, [&](int a, int b) {
+        const double xa = xyz[3 * (size_t)a + ax], xb = xyz[3 * (size_t)b + ax];
+        return xa != xb ? xa < xb : a < b;
+    });
+    rcb_tiles(nodes, lo, cut, t0, ntl, xyz, tile_of);
+    rcb_tiles(nodes, cut, hi, t0 + ntl, nt - ntl, xyz, tile_of);
+}
+
+// Tile layout of the persistent SOR solve (k_sor_tiles): one spatial tile
+// of nodes per SM, rows ordered tile by tile and colour by colour inside a
+// tile, the column ids marked by colour order, and the tiles each tile
+// depends on.  27-slot rows only; other layouts keep the colour kernels.
+int build_tiles(fas_handle *h, const std::vector<double> &xyz, const std::vector<int> &bcol_host,
+                const std::vector<int> &nslot_host, const std::vector<int> &rowof_host)
+{
+    if (h->slots != SLOTS) return 0;
+    const int nn = h->nnod, ncol = h->ncol, crow = crow_of(SLOTS);
+    int occ = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sor_tiles<double>, 32 * tile_warps<double>(),
+                                                     tile_smem_bytes<double>()));
+    int occ32 = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ32, k_sor_tiles<float>, 32 * tile_warps<float>(),
+                                                     tile_smem_bytes<float>()));
+    if (occ < 1 || occ32 < 1) return 0;   // the colour kernels serve this device
+    const int nt = std::min(h->nsm, std::max(1, nn / 64));
+    std::vector<int> nodes(nn), tile_of(nn, 0);
+    for (int i = 0; i < nn; ++i) nodes[i] = i;
+    rcb_tiles(nodes, 0, nn, 0, nt, xyz, tile_of);
+    // rows: tile, then colour, then node id
+    std::vector<int> order(nn);
+    for (int i = 0; i < nn; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int b) {
+        if (tile_of[a] != tile_of[b]) return tile_of[a] < tile_of[b];
+        if (h->h_colour[a] != h->h_colour[b]) return h->h_colour[a] < h->h_colour[b];
+        return a < b;
+    });
+    std::vector<int> tseg((size_t)nt * (ncol + 1), 0), tsrc(nn), tbcol((size_t)crow * nn, 0);
+    {
+        std::vector<int> cnt((size_t)nt * ncol, 0);
+        for (int n = 0; n < nn; ++n) ++cnt[(size_t)tile_of[n] * ncol + h->h_colour[n]];
+        int r = 0;
+        for (int t = 0; t < nt; ++t) {
+            for (int c = 0; c < ncol; ++c) {
+                tseg[(size_t)t * (ncol + 1) + c] = r;
+                r += cnt[(size_t)t * ncol + c];
+            }
+            tseg[(size_t)t * (ncol + 1) + ncol] = r;
+        }
+    }
+    std::vector<std::vector<int>> adj(nt);
+    for (int r = 0; r < nn; ++r) {
+        const int n = order[r], p = rowof_host[n], t = tile_of[n];
+        tsrc[r] = p;
+        const int ns = nslot_host[p];
+        for (int sl = 0; sl < ns; ++sl) {
+            const int m = bcol_host[(size_t)p * crow + sl];
+            unsigned w = (unsigned)m;
+            if (h->h_colour[m] < h->h_colour[n]) w |= TILE_LOWER;
+            tbcol[(size_t)r * crow + sl] = (int)w;
+            if (tile_of[m] != t) adj[t].push_back(tile_of[m]);
+        }
+        tbcol[(size_t)r * crow + SLOTS] = ns;
+    }
+    std::vector<int> aptr(nt + 1, 0), alist;
+    for (int t = 0; t < nt; ++t) {
+        std::sort(adj[t].begin(), adj[t].end());
+        adj[t].erase(std::unique(adj[t].begin(), adj[t].end()), adj[t].end());
+        aptr[t + 1] = aptr[t] + (int)adj[t].size();
+        alist.insert(alist.end(), adj[t].begin(), adj[t].end());
+    }
+    cudaStream_t s = h->stream;
+    h->ntiles = nt;
+    CKA(h->tseg.alloc(tseg.size()));
+    CKA(h->tadj_ptr.alloc(aptr.size()));
+    CKA(h->tadj.alloc(std::max<size_t>(alist.size(), 1)));
+    CKA(h->tsrc.alloc(nn));
+    CKA(h->tbcol.alloc(tbcol.size()));
+    CKA(h->tprog.alloc(nt));
+    CKA(h->tpart.alloc((size_t)TILE_SLOTS_SYNC * nt * 2));
+    CKA(h->tsync.alloc(1));
+    CKA(h->trdiag.alloc((size_t)3 * nn));
+    CKA(h->sol_scr.alloc((size_t)3 * nn));
+    CK(h->tseg.put(tseg.data(), tseg.size(), s));
+    CK(h->tadj_ptr.put(aptr.data(), aptr.size(), s));
+    if (!alist.empty()) CK(h->tadj.put(alist.data(), alist.size(), s));
+    CK(h->tsrc.put(tsrc.data(), nn, s));
+    CK(h->tbcol.put(tbcol.data(), tbcol.size(), s));
+    CK(cudaStreamSynchronize(s));
     return 0;
 }
 
@@ -511,6 +634,10 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
                             cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem_bytes<double, SLOTS20>()));
     CK(cudaFuncSetAttribute(k_sor_colour_tma<float, SLOTS20, TMA_LPR81>,
                             cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem_bytes<float, SLOTS20>()));
+    CK(cudaFuncSetAttribute(k_sor_tiles<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            tile_smem_bytes<double>()));
+    CK(cudaFuncSetAttribute(k_sor_tiles<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            tile_smem_bytes<float>()));
     CK(cudaMallocHost((void **)&h->hc, sizeof(HostCtl)));
     CK(cudaEventCreate(&h->ev_t0));
     CK(cudaEventCreate(&h->ev_t1));
@@ -691,6 +818,7 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
     const int cb = Cd->real_bytes;
     h->C.toler = Cd->toler; h->C.alpha = Cd->alpha; h->C.afactor = Cd->afactor; h->C.efix = Cd->efix;
     h->C.smale = Cd->smale; h->C.smalr = Cd->smalr; h->C.maxit = Cd->maxit; h->C.seed = Cd->twin_seed;
+    h->C.tangent = (h->mode & FAS_MODE_TANGENT_CONSISTENT) ? 1 : 0;
     h->ninc1 = Cd->ninc1; h->nxs = Cd->nxs; h->nfs = Cd->nfs;
     if (h->nxs < 0 || h->nfs < 0 || (h->nxs > 0 && (!Cd->x_spec || Cd->ld_xs < h->nxs)) ||
         (h->nfs > 0 && (!Cd->f_spec || Cd->ld_xs < h->nfs)))
@@ -1147,6 +1275,107 @@ int ensure_fp32_graph(fas_handle *h, const BlockDev &B, double tolerl)
     return 0;
 }
 
+// One cooperative launch of the persistent tile solve: at most maxsw
+// sweeps from sol0, sweep counts reported from sweep_base on.
+template <typename T>
+int launch_tiles(fas_handle *h, const T *blk, const double *rhs, const double *base, const double *rdiag,
+                 double *sol0, int maxsw, int sweep_base, double tolerl)
+{
+    cudaStream_t s = h->stream;
+    CK(h->tprog.zero(s));
+    CK(h->tsync.zero(s));
+    TileArgs<T> a;
+    a.blk = blk;
+    a.bcol = h->tbcol.p;
+    a.tseg = h->tseg.p;
+    a.tadj_ptr = h->tadj_ptr.p;
+    a.tadj = h->tadj.p;
+    a.rhs = rhs;
+    a.base = base;
+    a.rdiag = rdiag;
+    a.sol0 = sol0;
+    a.sol1 = h->sol_scr.p;
+    a.progress = h->tprog.p;
+    a.part = h->tpart.p;
+    a.sync = h->tsync.p;
+    a.ctl = h->sorctl.p;
+    a.ntiles = h->ntiles;
+    a.ncol = h->ncol;
+    a.maxsw = maxsw;
+    a.sweep_base = sweep_base;
+    a.tolerl = tolerl;
+    a.keep_rows = h->tile_keep_rows;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(h->ntiles);
+    cfg.blockDim = dim3(32 * tile_warps<T>());
+    cfg.dynamicSmemBytes = tile_smem_bytes<T>();
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, k_sor_tiles<T>, a));
+    LAUNCHED(h);
+    return 0;
+}
+
+// FACSLS by the persistent tile kernel: the assembled rows are copied into
+// the tile layout, then one launch runs the FP64 solve to convergence; the
+// FP32 form runs refinement cycles of refine_every sweeps (one launch, the
+// fold and the FP64 residual each).  Leaves the verdict in h->hc->sor.
+int facsls_tiles(fas_handle *h, const BlockDev &B, double tolerl, bool fp32)
+{
+    cudaStream_t s = h->stream;
+    const int rows = h->nnod;
+    const size_t nd3 = 3 * (size_t)rows;
+    const unsigned pblk = (unsigned)std::min<long long>(nblocks(rows, 8), (long long)h->nsm * 8);
+    if (!fp32) {
+        if (!h->tblk64.p) CKA(h->tblk64.alloc((size_t)BROW * rows));
+        k_tile_pack<double><<<pblk, 256, 0, s>>>(B, h->tsrc.p, rows, h->tblk64.p, h->trdiag.p);
+        LAUNCHED(h);
+        Span sp(h, &h->P.ms_sor_colour);
+        const int rc = launch_tiles<double>(h, h->tblk64.p, h->rhs.p, nullptr, FAS_SOR_RCP ? h->trdiag.p : nullptr,
+                                            h->ddx.p, 1000, 0, tolerl);
+        sp.end();
+        keep(h, sp);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(&h->hc->sor, h->sorctl.p, sizeof(SorCtl), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        return 0;
+    }
+    if (!h->tblk32.p) CKA(h->tblk32.alloc((size_t)BROW * rows));
+    k_tile_pack<float><<<pblk, 256, 0, s>>>(B, h->tsrc.p, rows, h->tblk32.p, nullptr);
+    LAUNCHED(h);
+    // x (= ddx) starts at 0, so the first residual is rhs itself
+    CK(cudaMemcpyAsync(h->sor_r.p, h->rhs.p, nd3 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemsetAsync(h->sor_d.p, 0, nd3 * sizeof(double), s));
+    const int m = h->refine_every;
+    const unsigned rblk = (unsigned)std::min<long long>(nblocks(rows, 8), (long long)h->nsm * 8);
+    int done = 0, outer_per_chunk = 1;
+    while (done < 1000) {
+        for (int o = 0; o < outer_per_chunk && done < 1000; ++o) {
+            const int k = std::min(m, 1000 - done);
+            Span sp(h, &h->P.ms_sor_colour);
+            const int rc = launch_tiles<float>(h, h->tblk32.p, h->sor_r.p, h->ddx.p, nullptr, h->sor_d.p, k, done,
+                                               tolerl);
+            sp.end();
+            keep(h, sp);
+            if (rc) return rc;
+            k_fold<<<nblocks((long long)nd3, 256), 256, 0, s>>>((int)nd3, h->ddx.p, h->sor_d.p);
+            LAUNCHED(h);
+            k_residual<<<rblk, 256, 0, s>>>(B, h->rhs.p, h->ddx.p, h->sor_r.p, h->sorctl.p);
+            LAUNCHED(h);
+            done += k;
+        }
+        CK(cudaMemcpyAsync(&h->hc->sor, h->sorctl.p, sizeof(SorCtl), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (h->hc->sor.conv || h->hc->sor.fault) break;
+        outer_per_chunk = std::min(outer_per_chunk * 2, 4);
+    }
+    return 0;
+}
+
 // FACSLS: rhs <- ddx, ddx <- 0, multicolour SOR sweeps until the relative
 // change drops below toler^2 or 1000 sweeps (Stif_sol.f90:173-213).
 int facsls_impl(fas_handle *h, int *sweeps, double *error)
@@ -1165,7 +1394,8 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
     if (h->hc->ekey[1] != ~0ull) return 903;
     const double tolerl = h->C.toler * h->C.toler;
     const bool small = h->sor_small && !(h->mode & FAS_MODE_SOR_GRID);
-    if (!small && FAS_SOR_RCP) {
+    const bool tiles = !small && h->ntiles > 0 && (h->mode & FAS_MODE_SOR_TILES);
+    if (!small && !tiles && FAS_SOR_RCP) {
         k_rdiag<<<nblocks(h->nnod, 256), 256, 0, s>>>(B, h->rdiag.p);
         LAUNCHED(h);
     }
@@ -1180,7 +1410,12 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
     }
     int done = small ? 1000 : 0, chunk = 4;
     const bool fp32 = !small && (h->mode & FAS_MODE_SOR_FP32) && h->blk32.p && h->blk32_fresh;
-    if (fp32) {
+    if (tiles) {
+        const int rc = facsls_tiles(h, B, tolerl, fp32);
+        if (rc) return rc;
+        done = 1000;
+    }
+    if (fp32 && !tiles) {
         // x (= ddx) starts at 0, so the first residual is rhs itself
         CK(cudaMemcpyAsync(h->sor_r.p, h->rhs.p, nd3 * sizeof(double), cudaMemcpyDeviceToDevice, s));
         CK(cudaMemsetAsync(h->sor_d.p, 0, nd3 * sizeof(double), s));
@@ -1264,52 +1499,68 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
     return 0;
 }
 
-int nriter_impl(fas_handle *h, int inc, fas_iter_report *rep, int cap, int *n_rep)
+// One pass of NRITER's loop body (Stif_sol.f90:32-77): ELVALS + SUVALS,
+// the residual norm, FACSLS, the damping factor and the correction of x and
+// dx.  *more = the reference's loop condition for another pass.
+int nr_step_impl(fas_handle *h, int inc, int nit, fas_iter_report *r, bool *more)
 {
     cudaStream_t s = h->stream;
     const int ndof = 3 * h->nnod;
+    int rc = elvals_impl(h, inc, nit, true);
+    if (rc) return rc;
+    int sweeps = 0;
+    double serr = 0.0;
+    rc = facsls_impl(h, &sweeps, &serr);
+    if (rc) return rc;
+    k_nr_norms<<<h->nr_nblk, 256, 0, s>>>(h->nnod, h->ngps, h->ib.p, h->rhs.p, h->dx.p, h->ddx.p,
+                                          h->erepmd.p, h->part_nr.p, h->nr_nblk);
+    LAUNCHED(h);
+    k_final_sum<4><<<1, 1024, 0, s>>>(h->part_nr.p, h->nr_nblk, h->sums.p);
+    LAUNCHED(h);
+    CK(cudaMemcpyAsync(h->hc->sums, h->sums.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const double sfc = std::sqrt(h->hc->sums[0]);
+    const double errdx = std::sqrt(h->hc->sums[1]);
+    const double erddx = std::sqrt(h->hc->sums[2]);
+    const double sdx = errdx == 0.0 ? h->C.toler : erddx / errdx;
+    const double alp2 = 1.0 / (1.0 + h->C.alpha * sdx);
+    if (r) {
+        r->nit = nit;
+        r->sor_sweeps = sweeps;
+        r->sdx = sdx;
+        r->sfc = sfc;
+        r->cp_err = h->hc->sums[3] / (double)h->ngps;
+        r->alp2 = alp2;
+        r->sor_error = serr;
+    }
+    k_nr_update<<<nblocks(ndof, 256), 256, 0, s>>>(ndof, alp2, h->ddx.p, h->x.p, h->dx.p);
+    LAUNCHED(h);
+    if (more) *more = (sdx >= h->C.toler) && (nit < h->C.maxit);
+    return 0;
+}
+
+// NRITER's tail after the loop (Stif_sol.f90:80-84): cumslip += srate *
+// tiem(inc) over nss(mat_code) of the last element evaluated.
+int nr_finish_impl(fas_handle *h, int inc)
+{
+    const int nsc = h->M.ns[h->last_mat - 1];
+    k_cumslip<<<nblocks(h->ngps, 256), 256, 0, h->stream>>>(h->gp(), nsc, h->h_tiem[inc - 1]);
+    LAUNCHED(h);
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int nriter_impl(fas_handle *h, int inc, fas_iter_report *rep, int cap, int *n_rep)
+{
     int nit = 0;
     bool l_conv = true;
     while (l_conv) {
         ++nit;
         if (n_rep) *n_rep = nit;
-        int rc = elvals_impl(h, inc, nit, true);
+        const int rc = nr_step_impl(h, inc, nit, rep && nit <= cap ? &rep[nit - 1] : nullptr, &l_conv);
         if (rc) return rc;
-        int sweeps = 0;
-        double serr = 0.0;
-        rc = facsls_impl(h, &sweeps, &serr);
-        if (rc) return rc;
-        k_nr_norms<<<h->nr_nblk, 256, 0, s>>>(h->nnod, h->ngps, h->ib.p, h->rhs.p, h->dx.p, h->ddx.p,
-                                              h->erepmd.p, h->part_nr.p, h->nr_nblk);
-        LAUNCHED(h);
-        k_final_sum<4><<<1, 1024, 0, s>>>(h->part_nr.p, h->nr_nblk, h->sums.p);
-        LAUNCHED(h);
-        CK(cudaMemcpyAsync(h->hc->sums, h->sums.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        const double sfc = std::sqrt(h->hc->sums[0]);
-        const double errdx = std::sqrt(h->hc->sums[1]);
-        const double erddx = std::sqrt(h->hc->sums[2]);
-        const double sdx = errdx == 0.0 ? h->C.toler : erddx / errdx;
-        const double alp2 = 1.0 / (1.0 + h->C.alpha * sdx);
-        if (rep && nit <= cap) {
-            fas_iter_report &r = rep[nit - 1];
-            r.nit = nit;
-            r.sor_sweeps = sweeps;
-            r.sdx = sdx;
-            r.sfc = sfc;
-            r.cp_err = h->hc->sums[3] / (double)h->ngps;
-            r.alp2 = alp2;
-            r.sor_error = serr;
-        }
-        k_nr_update<<<nblocks(ndof, 256), 256, 0, s>>>(ndof, alp2, h->ddx.p, h->x.p, h->dx.p);
-        LAUNCHED(h);
-        l_conv = (sdx >= h->C.toler) && (nit < h->C.maxit);
     }
-    const int nsc = h->M.ns[h->last_mat - 1];
-    k_cumslip<<<nblocks(h->ngps, 256), 256, 0, s>>>(h->gp(), nsc, h->h_tiem[inc - 1]);
-    LAUNCHED(h);
-    CK(cudaStreamSynchronize(s));
-    return 0;
+    return nr_finish_impl(h, inc);
 }
 
 int reorient_impl(fas_handle *h, int inc, fas_twin_event *ev, int cap, int *n_ev)
@@ -1496,6 +1747,7 @@ int32_t fas_gpu_set_mode(fas_handle *h, uint32_t mode)
 {
     if (!h) return FAS_E_ARG;
     h->mode = mode;
+    h->C.tangent = (mode & FAS_MODE_TANGENT_CONSISTENT) ? 1 : 0;
     return 0;
 }
 
@@ -1555,6 +1807,25 @@ int32_t fas_gpu_nriter(fas_handle *h, int32_t inc, fas_iter_report *rep, int32_t
     const int rc = nriter_impl(h, inc, rep, cap, &n);
     if (n_rep) *n_rep = n;
     return rc;
+}
+
+int32_t fas_gpu_nr_step(fas_handle *h, int32_t inc, int32_t nit, fas_iter_report *rep, int32_t *more)
+{
+    if (!h || nit < 1) return FAS_E_ARG;
+    if (!h->have_state || h->point_mode) return FAS_E_STATE;
+    if (inc < 1 || inc > h->ninc1) return FAS_E_ARG;
+    bool m = false;
+    const int rc = nr_step_impl(h, inc, nit, rep, &m);
+    if (more) *more = m ? 1 : 0;
+    return rc;
+}
+
+int32_t fas_gpu_nr_finish(fas_handle *h, int32_t inc)
+{
+    if (!h) return FAS_E_ARG;
+    if (!h->have_state || h->point_mode) return FAS_E_STATE;
+    if (inc < 1 || inc > h->ninc1) return FAS_E_ARG;
+    return nr_finish_impl(h, inc);
 }
 
 int32_t fas_gpu_update_gptv(fas_handle *h)
@@ -1839,7 +2110,7 @@ int32_t fas_gpu_profile(fas_handle *h, int32_t enable, fas_profile *out)
 // (SorCtl) and the per-CTA reduction partials -- lives in this file-scope
 // array instead of in buffers of the handle: a 256-byte block for the
 // control words, then FAS_NOALLOC_PARTIALS pairs of doubles (the sums of
-// |dx|^2 and |x|^2 of every colour CTA).  131,328 bytes per device.
+// |dx|^2 and |x|^2 of every colour CTA).  262,400 bytes per device.
 static __device__ __align__(256) unsigned char fas_noalloc_scratch[256 + 2 * sizeof(double) * FAS_NOALLOC_PARTIALS];
 
 namespace {
@@ -1871,9 +2142,11 @@ int noalloc_scratch(int dev, unsigned char **out)
     return 0;
 }
 
-// The FP64 FACSLS of facsls_impl (same kernels, colour order, sweep
-// chunks and stopping test) on the static scratch; no CUDA graph, no
-// FP32-matrix sweeps, no profiling spans.
+// The FP64 FACSLS of facsls_impl (same colour kernels, colour order,
+// reciprocal-diagonal quotients, sweep chunks and stopping test) on the
+// static scratch; no CUDA graph, no FP32-matrix sweeps, no profiling
+// spans.  The reciprocal diagonal goes to the handle's own buffer, which
+// set-up allocated.
 int facsls_noalloc_impl(fas_handle *h, int *sweeps, double *error)
 {
     if (h->sor_nblk_tot > FAS_NOALLOC_PARTIALS) return FAS_E_RANGE;
@@ -1899,13 +2172,18 @@ int facsls_noalloc_impl(fas_handle *h, int *sweeps, double *error)
         launch_sor_small(h, B, ctl, tolerl);
         LAUNCHED(h);
     } else {
+        const double *rdiag = FAS_SOR_RCP ? h->rdiag.p : nullptr;
+        if (rdiag) {
+            k_rdiag<<<nblocks(h->nnod, 256), 256, 0, s>>>(B, h->rdiag.p);
+            LAUNCHED(h);
+        }
         int done = 0, chunk = 4;
         while (done < 1000) {
             const int k = std::min(chunk, 1000 - done);
             for (int it = 0; it < k; ++it) {
                 for (int c = 0; c < h->ncol; ++c) {
                     if (h->col_start[c + 1] <= h->col_start[c]) continue;
-                    launch_colour_kernel<double>(h, c, false, h->blk.p, h->rhs.p, h->ddx.p, nullptr, nullptr, ctl,
+                    launch_colour_kernel<double>(h, c, false, h->blk.p, h->rhs.p, h->ddx.p, nullptr, rdiag, ctl,
                                                  part);
                     LAUNCHED(h);
                 }
