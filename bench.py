@@ -75,6 +75,10 @@ SOR_TRAFFIC_PER_LAUNCH = 81.1e6
 CPU_STEPS = 2          # steps of the full-size checker run (cpu_baseline and oracle_error)
 INC_WARM, INC_TIMED = 5, 10   # increments leg: untimed increments, then timed ones
 POINTS = 1 << 20
+# the tuned form: FP32 sweeps with FP64 refinement, persistent tile solve,
+# consistent tangent (abi.FAS_MODE_SOR_FP32 | FAS_MODE_SOR_TILES |
+# FAS_MODE_TANGENT_CONSISTENT)
+TUNED_MODE = 1 | 16 | 32
 POINTS_CPU = 1 << 15   # points of the checker's bounded sample in the point workload
 
 
@@ -406,7 +410,8 @@ def run_increments(g, prob, start, ninc_warm: int, ninc_timed: int):
     g.download(s0)
     incs = list(range(ninc_warm + 1, ninc_warm + ninc_timed + 1))
     out, ends = {}, {}
-    for tag, mode in (("plain", abi.FAS_MODE_PLAIN), ("tuned", abi.FAS_MODE_SOR_FP32)):
+    for tag, mode in (("plain", abi.FAS_MODE_PLAIN), ("tuned", TUNED_MODE),
+                      ("plain_consistent_tangent", abi.FAS_MODE_TANGENT_CONSISTENT)):
         t = s0.copy()
         g.upload(t)
         g.set_mode(mode)
@@ -424,7 +429,9 @@ def run_increments(g, prob, start, ninc_warm: int, ninc_timed: int):
     g.set_mode(abi.FAS_MODE_PLAIN)
     e = stress_errors(ends["tuned"], ends["plain"])
     out["increments"] = [incs[0], incs[-1]]
-    out["tuned"]["mode"] = "FP32-matrix SOR sweeps, FP64 residual refinement every 16 sweeps"
+    out["tuned"]["mode"] = ("FP32-matrix SOR sweeps with FP64 residual refinement every 16 sweeps, "
+                            "persistent tile solve, consistent tangent")
+    out["plain_consistent_tangent"]["mode"] = "plain FP64 with the consistent tangent (Newton counts of both tangents)"
     out["speedup_tuned_vs_plain_s_per_increment"] = out["plain"]["s_per_increment"] / out["tuned"]["s_per_increment"]
     out["tuned_vs_plain_error"] = e
     return out, s0, ends["plain"]
@@ -547,7 +554,7 @@ def run_gpu(args):
                           f"({sum(r['sor_sweeps'] for r in reps_c)} SOR sweeps) by the C++ restatement, "
                           f"{secs:.1f} s"}
             errs = {}
-            for tag, mode in (("plain", abi.FAS_MODE_PLAIN), ("tuned", abi.FAS_MODE_SOR_FP32)):
+            for tag, mode in (("plain", abi.FAS_MODE_PLAIN), ("tuned", TUNED_MODE)):
                 q = prob.copy()
                 _, rg = timed_steps(g, start, CPU_STEPS, mode, level=0)
                 g.download(q)
@@ -579,7 +586,11 @@ def rooflines(g, start, prob) -> dict:
     from cpfem_code_b200 import abi
     pk = peaks()
     out = {}
-    for tag, mode in (("sor", abi.FAS_MODE_PLAIN), ("sor_fp32", abi.FAS_MODE_SOR_FP32)):
+    kernels = {"sor": "k_sor_colour_tma<double,27,4>", "sor_fp32": "k_sor_colour_tma<float,27,4>",
+               "sor_tiles": "k_sor_tiles<double>", "sor_fp32_tiles": "k_sor_tiles<float>"}
+    for tag, mode in (("sor", abi.FAS_MODE_PLAIN), ("sor_fp32", abi.FAS_MODE_SOR_FP32),
+                      ("sor_tiles", abi.FAS_MODE_SOR_TILES),
+                      ("sor_fp32_tiles", abi.FAS_MODE_SOR_FP32 | abi.FAS_MODE_SOR_TILES)):
         g.upload(start)
         g.set_mode(mode)
         g.update_node()
@@ -591,7 +602,7 @@ def rooflines(g, start, prob) -> dict:
         secs = p["ms_total"] / 1e3
         ach = p["sor_bytes"] / secs / 1e9
         nl = max(int(p["n_sor_colour"]), 1)
-        out[tag] = {"kernel": "k_sor_colour_tma<double,27,4>" if mode == 0 else "k_sor_colour_tma<float,27,4>",
+        out[tag] = {"kernel": kernels[tag],
                     "bound": "hbm", "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
                     "frac": ach / pk["hbm_gbs"], "peak_source": pk["source"],
                     "traffic": SOR_TRAFFIC_PER_LAUNCH if (mode == 0 and WORKLOAD == "cube64") else None,
@@ -699,6 +710,45 @@ def run_gpu_points(args, ws, rank, local, dist, dev):
     return 0
 
 
+def run_case(args) -> int:
+    """Small single-purpose runs for profiling (one GPU, a few launches):
+
+    * ``--case facsls``: UPDATE_NODE, ELVALS, SUVALS and one FACSLS solve of
+      the workload's first Newton iteration, in ``--mode``;
+    * ``--case adjoint``: the adjoint replay with gradients on ``--points``
+      independent FCC points (4 increments, checkpoints every 2);
+    * ``--case points``: ``--reps`` DSTRSS passes over ``--points`` points.
+    """
+    from cpfem_code_b200 import GpuSolver, ReplayHistory, generator
+    if args.case == "facsls":
+        p = make_problem(WORKLOAD)
+        g = GpuSolver(p, mode=args.mode)
+        g.update_node()
+        g.elvals(1, 1)
+        g.suvals(1)
+        sweeps, err = g.facsls()
+        print(f"{WORKLOAD}: FACSLS {sweeps} sweeps, error {err:.3e}", flush=True)
+    elif args.case == "adjoint":
+        n = args.points
+        p = generator.point_batch(n, seed=1)
+        rng = np.random.default_rng(2)
+        de = np.stack([p.de * (1.0 + 0.2 * rng.standard_normal(p.de.shape)) for _ in range(4)])
+        dr = 2e-4 * rng.standard_normal((4, n, 3))
+        h = ReplayHistory(de, dr, np.full(4, p.tiem[0]), np.ones(n), np.zeros(n), chk_every=2)
+        g = GpuSolver(p)
+        out = g.adjoint_grad(h)
+        print(f"adjoint: {n} points x 4 increments, J {out['J']:.4e}", flush=True)
+    else:
+        p = generator.point_batch(args.points, seed=1)
+        g = GpuSolver(p.copy(), mode=args.mode)
+        for _ in range(args.reps):
+            g.upload(p)
+            g.constitutive(1, 1)
+        print(f"points: {args.points} x {args.reps} DSTRSS passes", flush=True)
+    g.close()
+    return 0
+
+
 def main():
     global WORKLOAD, METRIC, DESC
     ap = argparse.ArgumentParser()
@@ -712,9 +762,16 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (replay gradients) leg")
     ap.add_argument("--workload", default=WORKLOAD, choices=list(WORKLOADS),
                     help="the headline 64^3 workload (default), another mesh, or the point batch")
+    ap.add_argument("--case", default=None, choices=["facsls", "adjoint", "points"],
+                    help="a small profiling run instead of the benchmark (see run_case)")
+    ap.add_argument("--mode", type=int, default=0, help="FAS_MODE_* mask of --case facsls / points")
+    ap.add_argument("--points", type=int, default=1 << 14, help="points of --case adjoint / points")
+    ap.add_argument("--reps", type=int, default=2, help="passes of --case points")
     args = ap.parse_args()
     WORKLOAD = args.workload
     METRIC, DESC = WORKLOADS[WORKLOAD]
+    if args.case:
+        return run_case(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_gpu(args)
