@@ -410,8 +410,12 @@ def run_increments(g, prob, start, ninc_warm: int, ninc_timed: int):
     g.download(s0)
     incs = list(range(ninc_warm + 1, ninc_warm + ninc_timed + 1))
     out, ends = {}, {}
-    for tag, mode in (("plain", abi.FAS_MODE_PLAIN), ("tuned", TUNED_MODE),
-                      ("plain_consistent_tangent", abi.FAS_MODE_TANGENT_CONSISTENT)):
+    legs = [("plain", abi.FAS_MODE_PLAIN), ("tuned", TUNED_MODE),
+            ("plain_consistent_tangent", abi.FAS_MODE_TANGENT_CONSISTENT)]
+    if WORKLOAD == "mixed32":
+        # the persistent phase-sorted queue for the constitutive passes
+        legs.append(("plain_cp_queue", abi.FAS_MODE_CP_QUEUE))
+    for tag, mode in legs:
         t = s0.copy()
         g.upload(t)
         g.set_mode(mode)
@@ -423,7 +427,12 @@ def run_increments(g, prob, start, ninc_warm: int, ninc_timed: int):
         prof = g.profile(0)
         g.download(t)
         ends[tag] = t
+        g.profile(2)                  # one more increment with per-phase events
+        g.upload(s0)
+        g.increment(incs[0])
+        ph = g.profile(0)
         out[tag] = {"s_per_increment": prof["ms_total"] / 1e3 / len(incs), "newton_iters": nit,
+                    "ms_constitutive_first_increment": ph["ms_constitutive"],
                     "sor_sweeps": int(prof["sor_sweeps"]),
                     "gp_updates_per_s": prob.ngps * nit / (prof["ms_total"] / 1e3)}
     g.set_mode(abi.FAS_MODE_PLAIN)
@@ -717,7 +726,10 @@ def run_case(args) -> int:
       the workload's first Newton iteration, in ``--mode``;
     * ``--case adjoint``: the adjoint replay with gradients on ``--points``
       independent FCC points (4 increments, checkpoints every 2);
-    * ``--case points``: ``--reps`` DSTRSS passes over ``--points`` points.
+    * ``--case points``: ``--reps`` DSTRSS passes over ``--points`` points;
+    * ``--case sweeps``: microseconds per sweep of the first FACSLS of n^3
+      cubes on every solve path (one CTA, colour kernels, tiles; FP64 and
+      FP32), one JSON line per size.
     """
     from cpfem_code_b200 import GpuSolver, ReplayHistory, generator
     if args.case == "facsls":
@@ -738,6 +750,34 @@ def run_case(args) -> int:
         g = GpuSolver(p)
         out = g.adjoint_grad(h)
         print(f"adjoint: {n} points x 4 increments, J {out['J']:.4e}", flush=True)
+    elif args.case == "sweeps":
+        # us per sweep of the first FACSLS of n^3 cubes on each solve path
+        from cpfem_code_b200 import abi
+        paths = {"one_cta": 0, "colour": abi.FAS_MODE_SOR_GRID,
+                 "tiles": abi.FAS_MODE_SOR_GRID | abi.FAS_MODE_SOR_TILES,
+                 "tiles_fp32": abi.FAS_MODE_SOR_GRID | abi.FAS_MODE_SOR_TILES | abi.FAS_MODE_SOR_FP32,
+                 "colour_fp32": abi.FAS_MODE_SOR_GRID | abi.FAS_MODE_SOR_FP32}
+        for n in (2, 4, 8, 12, 16, 20, 24, 32, 48):
+            p = generator.cube_config(n=n, ninc=1, grain=1, seed=n)
+            row = {"n": n, "nodes": p.nnod}
+            for tag, mode in paths.items():
+                if tag == "one_cta" and p.nnod > 8192:
+                    continue
+                g = GpuSolver(p.copy(), mode=mode)
+                g.update_node()
+                g.elvals(1, 1)
+                g.suvals(1)
+                start = g.download(p.copy())
+                g.facsls()                 # warm-up (graphs, buffers)
+                g.upload(start)
+                g.profile(1)
+                sw, _ = g.facsls()
+                pr = g.profile(0)
+                row[tag] = round(1e3 * pr["ms_total"] / max(sw, 1), 2)
+                row["sweeps"] = sw
+                g.close()
+            print(json.dumps(row), flush=True)
+        return 0
     else:
         p = generator.point_batch(args.points, seed=1)
         g = GpuSolver(p.copy(), mode=args.mode)
@@ -762,7 +802,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (replay gradients) leg")
     ap.add_argument("--workload", default=WORKLOAD, choices=list(WORKLOADS),
                     help="the headline 64^3 workload (default), another mesh, or the point batch")
-    ap.add_argument("--case", default=None, choices=["facsls", "adjoint", "points"],
+    ap.add_argument("--case", default=None, choices=["facsls", "adjoint", "points", "sweeps"],
                     help="a small profiling run instead of the benchmark (see run_case)")
     ap.add_argument("--mode", type=int, default=0, help="FAS_MODE_* mask of --case facsls / points")
     ap.add_argument("--points", type=int, default=1 << 14, help="points of --case adjoint / points")

@@ -499,7 +499,7 @@ void rcb_tiles(std::vector<int> &nodes, int lo, int hi, int t0, int nt, const st
 int build_tiles(fas_handle *h, const std::vector<double> &xyz, const std::vector<int> &bcol_host,
                 const std::vector<int> &nslot_host, const std::vector<int> &rowof_host)
 {
-    if (h->slots != SLOTS) return 0;
+    if (h->slots != SLOTS || h->ncol > TILE_MAXCOL) return 0;
     const int nn = h->nnod, ncol = h->ncol, crow = crow_of(SLOTS);
     int occ = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sor_tiles<double>, 32 * tile_warps<double>(),
@@ -551,6 +551,7 @@ int build_tiles(fas_handle *h, const std::vector<double> &xyz, const std::vector
     for (int t = 0; t < nt; ++t) {
         std::sort(adj[t].begin(), adj[t].end());
         adj[t].erase(std::unique(adj[t].begin(), adj[t].end()), adj[t].end());
+        if ((int)adj[t].size() > TILE_MAXADJ) return 0;   // the colour kernels serve this mesh
         aptr[t + 1] = aptr[t] + (int)adj[t].size();
         alist.insert(alist.end(), adj[t].begin(), adj[t].end());
     }
@@ -1021,13 +1022,14 @@ const int *work_order(fas_handle *h, int n, const int *gp_of)
 }
 
 // Grid of a constitutive pass over n items (for_each_item).  With the
-// queue: as many 128-thread CTAs as reside at once, at most one item per
-// thread, and the queue head zeroed; otherwise one thread per item.
+// queue (FAS_MODE_CP_QUEUE, or built in with FAS_CP_QUEUE=1): as many
+// 128-thread CTAs as reside at once, at most one item per thread, and the
+// queue head zeroed; otherwise one thread per item.
 template <typename K> unsigned cp_grid(fas_handle *h, K kern, long long n, int **queue)
 {
     *queue = nullptr;
     const unsigned full = nblocks(n, 128);
-    if (!FAS_CP_QUEUE) return full;
+    if (!FAS_CP_QUEUE && !(h->mode & FAS_MODE_CP_QUEUE)) return full;
     int occ = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 128, 0) != cudaSuccess || occ < 1) return full;
     if (!h->cp_queue.p && h->cp_queue.alloc(1) != cudaSuccess) return full;

@@ -69,6 +69,10 @@ static_assert(tile_smem_bytes<double>() <= 227 * 1024 && tile_smem_bytes<float>(
 
 constexpr unsigned TILE_LOWER = 0x80000000u;   // column-id bit: lower colour than the row
 constexpr int TILE_SLOTS_SYNC = 4;             // per-sweep slots of the stopping test
+// a tile's colour bounds and neighbour list live in shared memory (global
+// reads of them after every acquire would cost an L2 round trip each)
+constexpr int TILE_MAXCOL = 64;
+constexpr int TILE_MAXADJ = 128;
 
 // Per-sweep stopping-test state, zeroed before every launch.
 struct TileSync {
@@ -111,17 +115,16 @@ __device__ __forceinline__ void st_release(int *p, int v)
 // ends the kernel in well under a minute.
 constexpr int TILE_POLLS = 1 << 21;
 
-// Waits until every tile adjacent to `t` has finished `target` phases.
+// Waits until every tile of adj[0, nadj) has finished `target` phases.
 // One warp polls up to 32 neighbours at a time.  Returns false on a
 // timeout or when another tile raised the fault.
-__device__ __forceinline__ bool tile_wait_neighbours(const int *tadj_ptr, const int *tadj, const int *progress,
-                                                     int t, int target, TileSync *sync)
+__device__ __forceinline__ bool tile_wait_neighbours(const int *adj, int nadj, const int *progress, int target,
+                                                     TileSync *sync)
 {
     const int lane = threadIdx.x & 31;
-    const int a0 = tadj_ptr[t], a1 = tadj_ptr[t + 1];
-    for (int b = a0; b < a1; b += 32) {
+    for (int b = 0; b < nadj; b += 32) {
         const int k = b + lane;
-        const int nb = k < a1 ? tadj[k] : -1;
+        const int nb = k < nadj ? adj[k] : -1;
         int it = 0;
         while (true) {
             const bool ok = nb < 0 || ld_acquire(progress + nb) >= target;
@@ -203,6 +206,8 @@ __global__ void __launch_bounds__(32 * tile_warps<T>(), 1) k_sor_tiles(TileArgs<
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int s_flag[2];
     __shared__ double s_red[2][NW];
+    __shared__ int seg[TILE_MAXCOL + 1];   // first row of each colour of this tile
+    __shared__ int s_adj[TILE_MAXADJ];      // the tiles this tile waits for
 
     // a launch queued behind the one that converged does nothing
     if (((volatile const SorCtl *)a.ctl)->conv) return;
@@ -210,7 +215,10 @@ __global__ void __launch_bounds__(32 * tile_warps<T>(), 1) k_sor_tiles(TileArgs<
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int row = lane / LPR, q = lane % LPR;
     const int ncol = a.ncol;
-    const int *seg = a.tseg + (size_t)t * (ncol + 1);
+    const int a0 = a.tadj_ptr[t], nadj = a.tadj_ptr[t + 1] - a0;   // at most TILE_MAXADJ (set-up checks)
+    for (int k = threadIdx.x; k <= ncol; k += blockDim.x) seg[k] = a.tseg[(size_t)t * (ncol + 1) + k];
+    for (int k = threadIdx.x; k < nadj; k += blockDim.x) s_adj[k] = a.tadj[a0 + k];
+    __syncthreads();
     unsigned char *ring = smem + (size_t)w * TMA_STAGES * SB;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + (size_t)NW * TMA_STAGES * SB) + w * TMA_STAGES;
     const uint64_t stream_pol = l2_evict_first();
@@ -284,10 +292,10 @@ __global__ void __launch_bounds__(32 * tile_warps<T>(), 1) k_sor_tiles(TileArgs<
         double v0 = 0.0, v1 = 0.0;
         for (int c = 0; c < ncol && !fault; ++c) {
             if (w == 0) {
-                const bool ok = tile_wait_neighbours(a.tadj_ptr, a.tadj, a.progress, t, (j - 1) * ncol + c, a.sync);
+                const bool ok = tile_wait_neighbours(s_adj, nadj, a.progress, (j - 1) * ncol + c, a.sync);
+                __threadfence();
                 if (lane == 0) s_flag[1] = ok ? 1 : 0;
             }
-            __threadfence();
             __syncthreads();
             if (!s_flag[1]) {
                 fault = true;

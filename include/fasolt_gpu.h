@@ -73,6 +73,11 @@ extern "C" {
                                      reference) instead of CPSTRS's chi of
                                      the last iterate (Cpstrs.f90:154-162);
                                      symmetrised like chi                  */
+#define FAS_MODE_CP_QUEUE    64u  /* constitutive passes on a persistent grid
+                                     whose warps take the next 32 GPs of the
+                                     work-sorted (heaviest first) order from
+                                     a device queue, instead of one thread
+                                     per GP in that order                   */
 #define FAS_MODE_SOR_TILES   16u  /* grid-wide SOR as one persistent launch
                                      per solve: spatial tiles of rows, one
                                      per SM, that start each colour once

@@ -27,7 +27,7 @@ def pair(p, threads=4, mode=abi.FAS_MODE_PLAIN):
     return GpuSolver(pg, mode=mode), OracleSolver(po, 8, threads=threads), pg, po
 
 
-@pytest.mark.parametrize("mode", [abi.FAS_MODE_PLAIN, abi.FAS_MODE_CP_WARP])
+@pytest.mark.parametrize("mode", [abi.FAS_MODE_PLAIN, abi.FAS_MODE_CP_WARP, abi.FAS_MODE_CP_QUEUE])
 def test_constitutive_points(mode):
     """One thread per point (default) and one warp per point."""
     p = generator.point_batch(2048, seed=11)
@@ -224,7 +224,7 @@ def test_fp32_sor_refinement_error():
     assert per_point < 1e-4 and macro < 1e-5
 
 
-@pytest.mark.parametrize("mode", [abi.FAS_MODE_PLAIN, abi.FAS_MODE_CP_WARP])
+@pytest.mark.parametrize("mode", [abi.FAS_MODE_PLAIN, abi.FAS_MODE_CP_WARP, abi.FAS_MODE_CP_QUEUE])
 def test_mixed_fcc_hcp_increment(mode):
     """Mixed FCC (12 systems) / HCP (30 systems, with twins) grains: the
     32-system kernel instantiations against the checker, including twin
