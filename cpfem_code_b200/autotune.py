@@ -10,7 +10,11 @@ time it sets:
   by the FACSLS of 32^3 20-node bricks;
 * ``cp``: ``FAS_WORK_DESC``, ``FAS_CP_QUEUE`` (order and device queue of the
   constitutive pass), timed by the element pass of the mixed FCC/HCP 32^3
-  cube and the 2^20-point batch (geometric mean of the two ratios).
+  cube and the 2^20-point batch (geometric mean of the two ratios);
+* ``sor27f32``: ``FAS_TMA_ROWS32``, ``FAS_TMA_LPR32``, ``FAS_TMA_MINB32``
+  (rows per chunk, lanes per row and the CTAs per SM the register budget
+  must allow, of the tuned form's FP32-matrix colour kernel), timed by the
+  FP32 FACSLS of the 64^3 cube's first Newton iteration.
 
 The knobs act on different kernels, so library i carries candidate i of
 every knob (a knob with fewer candidates repeats its last one), and one
@@ -40,6 +44,8 @@ KNOBS = {
               for r, l, st in ((8, 4, 2), (16, 4, 2), (8, 8, 2), (8, 4, 3), (16, 8, 2))],
     "sor81": [dict(FAS_TMA_ROWS81=r, FAS_TMA_LPR81=l) for r, l in ((8, 16), (4, 16), (8, 8), (4, 32), (16, 8))],
     "cp": [dict(FAS_WORK_DESC=d, FAS_CP_QUEUE=q) for d, q in ((1, 1), (1, 0), (0, 1), (0, 0))],
+    "sor27f32": [dict(FAS_TMA_ROWS32=r, FAS_TMA_LPR32=l, FAS_TMA_MINB32=m)
+                 for r, l, m in ((8, 4, 1), (8, 8, 1), (16, 4, 1), (4, 8, 1), (8, 8, 12), (8, 4, 16))],
 }
 
 
@@ -78,11 +84,11 @@ def _median(xs):
     return xs[len(xs) // 2]
 
 
-def _solve_us(p, reps: int = 3) -> tuple[float, int]:
+def _solve_us(p, reps: int = 3, mode: int = 0) -> tuple[float, int]:
     """us per sweep of the FACSLS of the first Newton iteration (graphs and
-    programmatic launches as the increments run it)."""
+    programmatic launches as the increments run it), in `mode`."""
     from .solver import GpuSolver
-    g = GpuSolver(p.copy())
+    g = GpuSolver(p.copy(), mode=mode)
     try:
         g.update_node()
         g.elvals(1, 1)
@@ -135,8 +141,10 @@ def measure() -> dict:
         _load(lib_path(i))
         us27, sw27 = _solve_us(probs["cube64"])
         us81, sw81 = _solve_us(probs["brick20_32"])
+        us32, sw32 = _solve_us(probs["cube64"], mode=1)   # FAS_MODE_SOR_FP32
         out[str(i)] = dict(defines=defines_of(i), cube64_sweep_us=us27, cube64_sweeps=sw27,
                            brick20_32_sweep_us=us81, brick20_32_sweeps=sw81,
+                           cube64_fp32_sweep_us=us32, cube64_fp32_sweeps=sw32,
                            mixed32_cp_ms=_cp_ms(probs["mixed32"], False),
                            points_cp_ms=_cp_ms(probs["points"], True))
         print(json.dumps(out[str(i)]), flush=True)
@@ -155,12 +163,13 @@ def select(meas: dict | None = None, out: str = TUNED) -> dict:
     score = {
         "sor27": lambda r: r["cube64_sweep_us"],
         "sor81": lambda r: r["brick20_32_sweep_us"],
+        "sor27f32": lambda r: r["cube64_fp32_sweep_us"],
         "cp": lambda r: math.sqrt(r["mixed32_cp_ms"] / rows[0]["mixed32_cp_ms"]
                                   * r["points_cp_ms"] / rows[0]["points_cp_ms"]),
     }
     # sweep counts do not depend on a launch shape; a candidate that changed
     # them would be wrong, not fast
-    for key in ("cube64_sweeps", "brick20_32_sweeps"):
+    for key in ("cube64_sweeps", "brick20_32_sweeps", "cube64_fp32_sweeps"):
         assert len({r[key] for r in rows}) == 1, f"{key} differ between candidates"
     tuned = {"defines": {}, "measured": {}}
     for knob, cands in KNOBS.items():

@@ -218,11 +218,13 @@ struct fas_handle {
     }
 };
 
-// meshes with at most this many nodes run each SOR solve in one CTA: 8192
-// for 27-slot rows (1024 threads, a slot per lane); 512 for 81-slot rows,
-// whose three slots per lane on 256 threads make a row about 12x slower than
-// in the colour kernels, which cost about 64 us per sweep at that size
-constexpr int SOR_SMALL_ROWS = 8192;
+// meshes with at most this many nodes run each SOR solve in one CTA: 256
+// for 27-slot rows (1024 threads, a slot per lane; measured us per sweep,
+// one CTA against the colour kernels: 17 / 33 at 125 nodes, 74 / 27 at
+// 729, 439 / 26 at 4,913); 512 for 81-slot rows, whose three slots per lane
+// on 256 threads make a row about 12x slower than in the colour kernels,
+// which cost about 64 us per sweep at that size
+constexpr int SOR_SMALL_ROWS = 256;
 constexpr int SOR_SMALL_ROWS81 = 512;
 
 #define CK(expr)                                      \
@@ -446,9 +448,9 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
     int tot32 = 0;
     for (int c = 0; c < h->ncol; ++c) {
         h->sor_boff32[c] = tot32;
-        const int cps = h->slots == SLOTS ? tma_ctas_per_sm<SLOTS, TMA_LPR, float>()
+        const int cps = h->slots == SLOTS ? tma_ctas_per_sm<SLOTS, TMA_LPR32, float>()
                                           : tma_ctas_per_sm<SLOTS20, TMA_LPR81, float>();
-        const int rows = h->slots == SLOTS ? tma_rows<SLOTS>() : tma_rows<SLOTS20>();
+        const int rows = h->slots == SLOTS ? tma_rows<SLOTS, float>() : tma_rows<SLOTS20, float>();
         h->sor_nblk32[c] = (int)std::min<long long>(nblocks(h->col_start[c + 1] - h->col_start[c], rows),
                                                      (long long)h->nsm * cps);
         tot32 += h->sor_nblk32[c];
@@ -629,7 +631,7 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     CK(cudaFuncSetAttribute(k_sor_colour_tma<double, SLOTS, TMA_LPR>,
                             cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem_bytes<double, SLOTS>()));
-    CK(cudaFuncSetAttribute(k_sor_colour_tma<float, SLOTS, TMA_LPR>,
+    CK(cudaFuncSetAttribute(k_sor_colour_tma<float, SLOTS, TMA_LPR32>,
                             cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem_bytes<float, SLOTS>()));
     CK(cudaFuncSetAttribute(k_sor_colour_tma<double, SLOTS20, TMA_LPR81>,
                             cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem_bytes<double, SLOTS20>()));
@@ -1176,12 +1178,14 @@ void launch_colour_kernel(fas_handle *h, int c, bool pdl, const T *blk, const do
     const int boff = f32 ? h->sor_boff32[c] : h->sor_boff[c];
     const int ntot = f32 ? h->sor_nblk_tot32 : h->sor_nblk_tot;
     if (h->slots == SLOTS) {
-        auto k = k_sor_colour_tma<T, SLOTS, TMA_LPR>;
+        constexpr int LPR = sizeof(T) == 4 ? TMA_LPR32 : TMA_LPR;
+        auto k = k_sor_colour_tma<T, SLOTS, LPR>;
+        const unsigned nt = tma_threads<LPR, tma_rows<SLOTS, T>()>();
         if (pdl)
-            launch_pdl(k, nblk, TMA_THREADS, tma_smem_bytes<T, SLOTS>(), h->stream, blk, h->bcol.p, p0,
+            launch_pdl(k, nblk, nt, tma_smem_bytes<T, SLOTS>(), h->stream, blk, h->bcol.p, p0,
                        p1, rhs, sol, base, rdiag, ctl, part, boff, ntot);
         else
-            k<<<nblk, TMA_THREADS, tma_smem_bytes<T, SLOTS>(), h->stream>>>(
+            k<<<nblk, nt, tma_smem_bytes<T, SLOTS>(), h->stream>>>(
                 blk, h->bcol.p, p0, p1, rhs, sol, base, rdiag, ctl, part, boff, ntot);
     } else {
         auto k = k_sor_colour_tma<T, SLOTS20, TMA_LPR81>;

@@ -1137,6 +1137,21 @@ constexpr int TMA_LPR = FAS_TMA_LPR;         // lanes per row of 27-slot rows (a
 #endif
 constexpr int TMA_LPR81 = FAS_TMA_LPR81;     // lanes per row of 81-slot rows
 constexpr int TMA_ROWS81 = FAS_TMA_ROWS81;   // rows per chunk of 81-slot rows
+// The FP32-matrix sweeps of the tuned form have their own shape: their rings
+// are half as large, so the same shared memory holds twice the rows in
+// flight, and the shape that hides the consumer's latency differs.
+#ifndef FAS_TMA_ROWS32
+#define FAS_TMA_ROWS32 8
+#endif
+#ifndef FAS_TMA_LPR32
+#define FAS_TMA_LPR32 4
+#endif
+#ifndef FAS_TMA_MINB32
+#define FAS_TMA_MINB32 1
+#endif
+constexpr int TMA_ROWS32 = FAS_TMA_ROWS32;   // rows per chunk of FP32 27-slot rows
+constexpr int TMA_LPR32 = FAS_TMA_LPR32;     // lanes per row of FP32 27-slot rows
+constexpr int TMA_MINB32 = FAS_TMA_MINB32;   // CTAs per SM the FP32 kernel's registers must allow
 constexpr int TMA_STAGES = FAS_TMA_STAGES;   // chunks in flight per CTA
 constexpr int TMA_PD = FAS_TMA_PD;           // chunks whose gathers run ahead of the computed one
 static_assert(TMA_PD >= 1 && TMA_PD < TMA_STAGES, "gathers run ahead within the ring");
@@ -1145,11 +1160,21 @@ constexpr int TMA_THREADS = tma_threads<TMA_LPR>();
 static_assert(TMA_LPR >= 1 && TMA_LPR <= 32 && (TMA_LPR & (TMA_LPR - 1)) == 0, "lanes per row");
 static_assert(TMA_THREADS % 32 == 0 && tma_threads<TMA_LPR81, TMA_ROWS81>() % 32 == 0, "whole warps per CTA");
 
-// rows per chunk of the S-slot layout
-template <int S> __host__ __device__ constexpr int tma_rows() { return S == SLOTS ? TMA_ROWS : TMA_ROWS81; }
+// rows per chunk of the S-slot layout in value type T
+template <int S, typename T = double> __host__ __device__ constexpr int tma_rows()
+{
+    return S == SLOTS ? (sizeof(T) == 4 ? TMA_ROWS32 : TMA_ROWS) : TMA_ROWS81;
+}
+// minimum CTAs per SM the kernel's register budget must allow (1: no bound)
+template <int S, typename T> __host__ __device__ constexpr int tma_minb()
+{
+    return S == SLOTS && sizeof(T) == 4 ? TMA_MINB32 : 1;
+}
+static_assert(tma_threads<TMA_LPR32, TMA_ROWS32>() % 32 == 0 && (TMA_LPR32 & (TMA_LPR32 - 1)) == 0,
+              "whole warps per CTA");
 template <typename T, int S = SLOTS> __host__ __device__ constexpr int tma_stage_bytes()
 {
-    return tma_rows<S>() * brow_of(S) * (int)sizeof(T) + tma_rows<S>() * crow_of(S) * 4;
+    return tma_rows<S, T>() * brow_of(S) * (int)sizeof(T) + tma_rows<S, T>() * crow_of(S) * 4;
 }
 // the ring, its mbarriers and a 512-byte guard: lanes whose slots lie past
 // the row (q + LPR j >= S) skip their reads, and the guard keeps even a
@@ -1163,9 +1188,9 @@ template <typename T, int S = SLOTS> __host__ __device__ constexpr int tma_smem_
 // to fill them.
 template <int S, int LPR, typename T = double> __host__ __device__ constexpr int tma_ctas_per_sm()
 {
-    return (228 * 1024) / (tma_smem_bytes<T, S>() + 1024) < 32 / (tma_threads<LPR, tma_rows<S>()>() / 32)
+    return (228 * 1024) / (tma_smem_bytes<T, S>() + 1024) < 32 / (tma_threads<LPR, tma_rows<S, T>()>() / 32)
                ? (228 * 1024) / (tma_smem_bytes<T, S>() + 1024)
-               : 32 / (tma_threads<LPR, tma_rows<S>()>() / 32);
+               : 32 / (tma_threads<LPR, tma_rows<S, T>()>() / 32);
 }
 constexpr int TMA_CTAS_PER_SM = tma_ctas_per_sm<SLOTS, TMA_LPR>();
 static_assert(TMA_CTAS_PER_SM >= 1 && tma_ctas_per_sm<SLOTS20, TMA_LPR81>() >= 1,
@@ -1218,14 +1243,14 @@ __device__ __forceinline__ void sor_gather(const int *stage_cols, int r0, int nr
 // the first lane updates x, y and z in turn (omega = 1.2), stores them and
 // adds |x_new - x_old|^2 to v0 and |x_new + base|^2 to v1.  With `rcp` the
 // quotients come from the gathered reciprocal diagonal.
-template <typename T, int S, int LPR>
+template <typename T, int S, int LPR, int ROWS>
 __device__ __forceinline__ void sor_update(const unsigned char *stage, int nrow, int row, int q,
                                            const SorOps<(S + LPR - 1) / LPR> &g, bool rcp,
                                            const double *__restrict__ base, double *sol, double &v0,
                                            double &v1)
 {
     constexpr int SPL = (S + LPR - 1) / LPR, BR = brow_of(S), CR = crow_of(S);
-    constexpr int VB = tma_rows<S>() * BR * (int)sizeof(T);
+    constexpr int VB = ROWS * BR * (int)sizeof(T);
     const bool live = row < nrow;
     const T *vals = reinterpret_cast<const T *>(stage) + (live ? row : 0) * BR;
     const int *cols = reinterpret_cast<const int *>(stage + VB) + (live ? row : 0) * CR;
@@ -1309,7 +1334,7 @@ __device__ __forceinline__ void sor_update(const unsigned char *stage, int nrow,
 // wait is bounded; on a timeout the CTA waits (bounded) for its own copies
 // still in flight, raises ctl->fault and leaves.
 template <typename T, int S, int LPR>
-__global__ void __launch_bounds__(tma_rows<S>() * LPR) k_sor_colour_tma(const T *__restrict__ blk,
+__global__ void __launch_bounds__(tma_rows<S, T>() * LPR, tma_minb<S, T>()) k_sor_colour_tma(const T *__restrict__ blk,
                                                                 const int *__restrict__ bcol, int p0, int p1,
                                                                 const double *__restrict__ rhs, double *sol,
                                                                 const double *__restrict__ base,
@@ -1321,7 +1346,7 @@ __global__ void __launch_bounds__(tma_rows<S>() * LPR) k_sor_colour_tma(const T 
     constexpr int BR = brow_of(S), CR = crow_of(S);
     static_assert((BR * sizeof(T)) % 16 == 0 && (CR * 4) % 16 == 0, "bulk copies move 16-byte multiples");
     constexpr int SPL = (S + LPR - 1) / LPR;   // slots per lane
-    constexpr int ROWS = tma_rows<S>();
+    constexpr int ROWS = tma_rows<S, T>();
     constexpr int VB = ROWS * BR * (int)sizeof(T);
     constexpr int SB = tma_stage_bytes<T, S>();
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TMA_STAGES * SB);
@@ -1404,7 +1429,7 @@ __global__ void __launch_bounds__(tma_rows<S>() * LPR) k_sor_colour_tma(const T 
         }
         const int st = k % TMA_STAGES;
         const int nrow = min(ROWS, p1 - (p0 + (int)(blockIdx.x + k * gridDim.x) * ROWS));
-        sor_update<T, S, LPR>(smem + st * SB, nrow, row, q, g[0], rdiag != nullptr, base, sol, v0, v1);
+        sor_update<T, S, LPR, ROWS>(smem + st * SB, nrow, row, q, g[0], rdiag != nullptr, base, sol, v0, v1);
         __syncthreads();   // every row of this stage is done
         if (threadIdx.x == 0 && k + TMA_STAGES < myn) {
             fence_proxy_async();

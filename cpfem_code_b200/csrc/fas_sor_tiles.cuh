@@ -22,7 +22,7 @@
 // Rows are ordered tile by tile, and inside a tile colour by colour:
 // tseg[t * (ncol + 1) + c] is the first row of colour c of tile t (the
 // entry c = ncol the end of the tile).  The rows of one colour of one tile
-// are cut into chunks of TMA_ROWS; warp w of the CTA serves chunks w, w +
+// are cut into chunks of TILE_ROWS; warp w of the CTA serves chunks w, w +
 // nwarps, ... of every phase.
 //
 // Stopping test without a global barrier.  Sweep j writes its iterate into
@@ -60,9 +60,17 @@ template <typename T> __host__ __device__ constexpr int tile_warps()
 {
     return sizeof(T) == 8 ? FAS_TILE_WARPS64 : FAS_TILE_WARPS32;
 }
+// chunk shape and ring depth of the tile kernel (fixed, independent of
+// the colour kernels' tuned shapes): 8 rows x 4 lanes = one warp per chunk
+constexpr int TILE_ROWS = 8, TILE_LPR = 4, TILE_STAGES = 2;
+// a ring stage: TILE_ROWS rows of 27 slots (values and column ids)
+template <typename T> __host__ __device__ constexpr int tile_stage_bytes()
+{
+    return TILE_ROWS * brow_of(SLOTS) * (int)sizeof(T) + TILE_ROWS * crow_of(SLOTS) * 4;
+}
 template <typename T> __host__ __device__ constexpr int tile_smem_bytes()
 {
-    return tile_warps<T>() * (TMA_STAGES * tma_stage_bytes<T, SLOTS>() + TMA_STAGES * 8) + 512;
+    return tile_warps<T>() * (TILE_STAGES * tile_stage_bytes<T>() + TILE_STAGES * 8) + 512;
 }
 static_assert(tile_smem_bytes<double>() <= 227 * 1024 && tile_smem_bytes<float>() <= 227 * 1024,
               "the tile CTA's rings must fit in shared memory");
@@ -195,11 +203,11 @@ struct TileCursor {
 template <typename T>
 __global__ void __launch_bounds__(32 * tile_warps<T>(), 1) k_sor_tiles(TileArgs<T> a)
 {
-    constexpr int S = SLOTS, LPR = TMA_LPR, ROWS = TMA_ROWS;
+    constexpr int S = SLOTS, LPR = TILE_LPR, ROWS = TILE_ROWS;
     constexpr int BR = brow_of(S), CR = crow_of(S);
     constexpr int SPL = (S + LPR - 1) / LPR;
     constexpr int VB = ROWS * BR * (int)sizeof(T);
-    constexpr int SB = tma_stage_bytes<T, S>();
+    constexpr int SB = tile_stage_bytes<T>();
     constexpr int NW = tile_warps<T>();
     static_assert(ROWS * LPR == 32, "one warp serves one chunk");
     static_assert((BR * sizeof(T)) % 16 == 0 && (CR * 4) % 16 == 0, "bulk copies move 16-byte multiples");
@@ -219,8 +227,8 @@ __global__ void __launch_bounds__(32 * tile_warps<T>(), 1) k_sor_tiles(TileArgs<
     for (int k = threadIdx.x; k <= ncol; k += blockDim.x) seg[k] = a.tseg[(size_t)t * (ncol + 1) + k];
     for (int k = threadIdx.x; k < nadj; k += blockDim.x) s_adj[k] = a.tadj[a0 + k];
     __syncthreads();
-    unsigned char *ring = smem + (size_t)w * TMA_STAGES * SB;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + (size_t)NW * TMA_STAGES * SB) + w * TMA_STAGES;
+    unsigned char *ring = smem + (size_t)w * TILE_STAGES * SB;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + (size_t)NW * TILE_STAGES * SB) + w * TILE_STAGES;
     const uint64_t stream_pol = l2_evict_first();
     const uint64_t keep_pol = l2_evict_last();
     const int tile_row0 = seg[0];
@@ -244,23 +252,23 @@ __global__ void __launch_bounds__(32 * tile_warps<T>(), 1) k_sor_tiles(TileArgs<
     auto issue = [&](const TileCursor &u, int k) {
         const int r0 = seg[u.c] + u.i * ROWS;
         const int nr = min(ROWS, seg[u.c + 1] - r0);
-        unsigned char *st = ring + (k % TMA_STAGES) * SB;
+        unsigned char *st = ring + (k % TILE_STAGES) * SB;
         const unsigned bv = (unsigned)(nr * BR * sizeof(T)), bc = (unsigned)(nr * CR * 4);
         const uint64_t pol = r0 - tile_row0 < a.keep_rows ? keep_pol : stream_pol;
-        mbar_expect_tx(&bars[k % TMA_STAGES], bv + bc);
-        bulk_g2s(st, a.blk + (size_t)r0 * BR, bv, &bars[k % TMA_STAGES], pol);
-        bulk_g2s(st + VB, a.bcol + (size_t)r0 * CR, bc, &bars[k % TMA_STAGES], pol);
+        mbar_expect_tx(&bars[k % TILE_STAGES], bv + bc);
+        bulk_g2s(st, a.blk + (size_t)r0 * BR, bv, &bars[k % TILE_STAGES], pol);
+        bulk_g2s(st + VB, a.bcol + (size_t)r0 * CR, bc, &bars[k % TILE_STAGES], pol);
     };
 
     TileCursor ic{1, 0, w};   // next chunk to issue (every lane keeps the same cursor)
     settle(ic);
     int issued = 0, taken = 0;
     if (lane == 0) {
-        for (int st = 0; st < TMA_STAGES; ++st) mbar_init(&bars[st], 1);
+        for (int st = 0; st < TILE_STAGES; ++st) mbar_init(&bars[st], 1);
         mbar_fence_init();
     }
     __syncwarp();
-    for (int st = 0; st < TMA_STAGES && ic.j <= a.maxsw; ++st) {
+    for (int st = 0; st < TILE_STAGES && ic.j <= a.maxsw; ++st) {
         if (lane == 0) issue(ic, issued);
         ++issued;
         advance(ic);
@@ -308,34 +316,34 @@ __global__ void __launch_bounds__(32 * tile_warps<T>(), 1) k_sor_tiles(TileArgs<
                 // the chunk of this phase taken now (taken-th of the warp's
                 // sequence): wait for its copy, gather, then compute
                 if (!have) {
-                    const unsigned par = (unsigned)((taken / TMA_STAGES) & 1);
-                    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bars[taken % TMA_STAGES], par))) {
+                    const unsigned par = (unsigned)((taken / TILE_STAGES) & 1);
+                    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bars[taken % TILE_STAGES], par))) {
                         fault = true;
                         break;
                     }
                     const int r0 = seg[c] + i * ROWS;
-                    tile_gather<S, LPR>(reinterpret_cast<const int *>(ring + (taken % TMA_STAGES) * SB + VB), r0,
+                    tile_gather<S, LPR>(reinterpret_cast<const int *>(ring + (taken % TILE_STAGES) * SB + VB), r0,
                                         min(ROWS, seg[c + 1] - r0), row, q, sol_new, sol_old, a.rhs, a.rdiag,
                                         keep_pol, gcur);
                 }
                 // gathers of the warp's next chunk of this phase run ahead
                 const int i2 = i + NW;
                 have = false;
-                if (i2 < nc && TMA_STAGES > 1) {
+                if (i2 < nc && TILE_STAGES > 1) {
                     const int k2 = taken + 1;
-                    const unsigned par = (unsigned)((k2 / TMA_STAGES) & 1);
-                    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bars[k2 % TMA_STAGES], par))) {
+                    const unsigned par = (unsigned)((k2 / TILE_STAGES) & 1);
+                    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bars[k2 % TILE_STAGES], par))) {
                         fault = true;
                         break;
                     }
                     const int r2 = seg[c] + i2 * ROWS;
-                    tile_gather<S, LPR>(reinterpret_cast<const int *>(ring + (k2 % TMA_STAGES) * SB + VB), r2,
+                    tile_gather<S, LPR>(reinterpret_cast<const int *>(ring + (k2 % TILE_STAGES) * SB + VB), r2,
                                         min(ROWS, seg[c + 1] - r2), row, q, sol_new, sol_old, a.rhs, a.rdiag,
                                         keep_pol, gnxt);
                     have = true;
                 }
                 const int r0 = seg[c] + i * ROWS;
-                sor_update<T, S, LPR>(ring + (taken % TMA_STAGES) * SB, min(ROWS, seg[c + 1] - r0), row, q, gcur,
+                sor_update<T, S, LPR, ROWS>(ring + (taken % TILE_STAGES) * SB, min(ROWS, seg[c + 1] - r0), row, q, gcur,
                                       a.rdiag != nullptr, a.base, sol_new, v0, v1);
                 __syncwarp();
                 // the stage is free: refill it with the warp's next chunk
@@ -438,7 +446,7 @@ __global__ void __launch_bounds__(32 * tile_warps<T>(), 1) k_sor_tiles(TileArgs<
     // copies issued and not taken may still write the ring
     if (lane == 0)
         for (int k = taken; k < issued; ++k)
-            mbar_wait_bounded(&bars[k % TMA_STAGES], (unsigned)((k / TMA_STAGES) & 1));
+            mbar_wait_bounded(&bars[k % TILE_STAGES], (unsigned)((k / TILE_STAGES) & 1));
     if (fault) {
         if (threadIdx.x == 0) {
             atomicExch(&a.sync->fault, 1);
