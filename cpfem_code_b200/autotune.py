@@ -45,7 +45,7 @@ KNOBS = {
     "sor81": [dict(FAS_TMA_ROWS81=r, FAS_TMA_LPR81=l) for r, l in ((8, 16), (4, 16), (8, 8), (4, 32), (16, 8))],
     "cp": [dict(FAS_WORK_DESC=d, FAS_CP_QUEUE=q) for d, q in ((1, 1), (1, 0), (0, 1), (0, 0))],
     "sor27f32": [dict(FAS_TMA_ROWS32=r, FAS_TMA_LPR32=l, FAS_TMA_MINB32=m)
-                 for r, l, m in ((8, 4, 1), (8, 8, 1), (16, 4, 1), (4, 8, 1), (8, 8, 12), (8, 4, 16))],
+                 for r, l, m in ((16, 4, 1), (8, 4, 1), (32, 4, 1), (16, 8, 1), (24, 4, 1), (16, 4, 6))],
 }
 
 

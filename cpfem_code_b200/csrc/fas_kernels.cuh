@@ -1141,7 +1141,7 @@ constexpr int TMA_ROWS81 = FAS_TMA_ROWS81;   // rows per chunk of 81-slot rows
 // are half as large, so the same shared memory holds twice the rows in
 // flight, and the shape that hides the consumer's latency differs.
 #ifndef FAS_TMA_ROWS32
-#define FAS_TMA_ROWS32 8
+#define FAS_TMA_ROWS32 16
 #endif
 #ifndef FAS_TMA_LPR32
 #define FAS_TMA_LPR32 4
