@@ -64,6 +64,11 @@ WORKLOADS = {
     "brick20_10": ("GP updates/s, 10^3 20-node bricks (DSTRSS evaluations per second of whole Newton iterations)",
                    "10^3 FCC Al 20-node eight-GP bricks (the reference sample's mesh: 8,000 GPs), "
                    "one grain per element, uniaxial tension 1e-3 per increment"),
+    "diff16": ("GP-increments/s of the adjoint gradient, 16^3 FCC cube, 20 increments (replay and reverse sweep)",
+               "16^3 FCC Al one-point bricks (4,096 GPs), one grain per element, 20 increments to 2 % tension; "
+               "lattice-strain objective over 8 {hkl} orientation bins along the load axis; gradients with "
+               "respect to h0, tau_sat, the rate exponent, the initial CRSS and all Euler angles; "
+               "checkpoints every 5 increments"),
     "points": ("GP updates/s, 2^20 independent FCC points (DSTRSS evaluations per second)",
                "2^20 FCC Al material points, uniform-SO(3) orientations, Gaussian strain increments of "
                "Frobenius norm 1e-3, CRSS uniform in [tau0, 2 tau0], elastic-predictor start"),
@@ -72,6 +77,8 @@ METRIC, DESC = WORKLOADS[WORKLOAD]
 # DRAM bytes (read + write) per FP64 colour launch at 64^3, measured with ncu
 # on two launches of the profiling case and scaled per row to the mean colour
 SOR_TRAFFIC_PER_LAUNCH = 81.1e6
+# the same for the FP32-matrix colour kernel (profiles/k_sor_colour_tma_fp32_cube64.md)
+SOR32_TRAFFIC_PER_LAUNCH = 47.3e6
 CPU_STEPS = 2          # steps of the full-size checker run (cpu_baseline and oracle_error)
 INC_WARM, INC_TIMED = 5, 10   # increments leg: untimed increments, then timed ones
 POINTS = 1 << 20
@@ -291,6 +298,14 @@ def run_reference(args):
             dist.destroy_process_group()
         return 0
     threads = os.cpu_count() or 1
+    if WORKLOAD == "diff16":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no adjoint, and its forward "
+                          "replay needs the history of a 16^3 FE run that the host cores take about 13 minutes "
+                          "to compute"}), flush=True)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
     prob = make_problem(WORKLOAD)
     if WORKLOAD == "points":
         dts = []
@@ -457,6 +472,8 @@ def run_gpu(args):
     dev = torch.device("cuda", local)
     if WORKLOAD == "points":
         return run_gpu_points(args, ws, rank, local, dist, dev)
+    if WORKLOAD == "diff16":
+        return run_gpu_diff16(args, ws, rank, local, dist, dev)
     from cpfem_code_b200 import GpuSolver, NewtonStepper, abi
 
     prob = make_problem(WORKLOAD, INC_WARM + INC_TIMED + 2)
@@ -616,7 +633,9 @@ def rooflines(g, start, prob) -> dict:
         out[tag] = {"kernel": kernels[tag],
                     "bound": "hbm", "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
                     "frac": ach / pk["hbm_gbs"], "peak_source": pk["source"],
-                    "traffic": SOR_TRAFFIC_PER_LAUNCH if (mode == 0 and WORKLOAD == "cube64") else None,
+                    "traffic": (SOR_TRAFFIC_PER_LAUNCH if tag == "sor" else
+                                SOR32_TRAFFIC_PER_LAUNCH if tag == "sor_fp32" else None)
+                    if WORKLOAD == "cube64" else None,
                     "bytes_per_launch": p["sor_bytes"] / nl, "launch_ms": p["ms_total"] / nl,
                     "launches": nl, "sweeps": int(p["sor_sweeps"]),
                     "timed": "one FACSLS solve of Newton iteration 1 of increment 1 (CUDA graph, programmatic "
@@ -640,6 +659,121 @@ def rooflines(g, start, prob) -> dict:
                                "gp_updates_per_s": p["gp_updates"] / (p["ms_constitutive"] / 1e3),
                                "timed": "per-launch events of the constitutive pass of Newton iteration 3"}
     return out
+
+
+DIFF_INC, DIFF_CHK = 20, 5
+DIFF_BINS = ((1, 1, 1), (2, 0, 0), (2, 2, 0), (3, 1, 1), (3, 3, 1), (4, 2, 0), (4, 2, 2), (5, 3, 1))
+
+
+def diff16_history(g, prob):
+    """The 16^3 run's strain history: every increment on the device (the
+    plain path), each GP's converged strain increment and spin recorded
+    before UPDATE_GPTV commits it."""
+    from cpfem_code_b200 import ReplayHistory, calibration
+    start = prob.copy()
+    de, dr = [], []
+    for inc in range(1, DIFF_INC + 1):
+        g.update_node()
+        g.nriter(inc)
+        q = g.download(prob.copy())
+        de.append(q.de.copy())
+        dr.append(q.dr.copy())
+        g.update_gptv()
+        g.do_reorient(inc)
+    euler = start.sv[:, :3]
+    w = np.zeros(prob.ngps)
+    for hkl in DIFF_BINS:
+        w += calibration.bin_weights(euler, calibration.cubic_family(hkl), (1.0, 0.0, 0.0), 5.0)
+    hist = ReplayHistory(np.stack(de), np.stack(dr), prob.tiem[:DIFF_INC], w / len(DIFF_BINS),
+                         np.zeros(prob.ngps), q=(1.0, 0.0, 0.0), chk_every=DIFF_CHK)
+    return start, hist
+
+
+def run_gpu_diff16(args, ws, rank, local, dist, dev):
+    """Configuration 3: adjoint gradients of a lattice-strain objective over
+    the 16^3 cube's 20 increments.  A step is one gradient evaluation
+    (fas_gpu_adjoint_grad: the replay of every GP's recorded history with
+    checkpoints every 5 increments, then the reverse sweep)."""
+    import torch
+
+    from cpfem_code_b200 import GpuSolver, generator
+    prob = generator.workload("cube16")
+    g = GpuSolver(prob)
+    start, hist = diff16_history(g, prob)
+    g.upload(start)
+    for _ in range(args.warmup):
+        g.adjoint_grad(hist)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    g.profile(1)
+    for _ in range(args.steps):
+        out = g.adjoint_grad(hist)
+    prof = g.profile(0)
+    clk = clocks.stop()
+    work = float(prob.ngps * DIFF_INC * args.steps)
+    t_max, work = reduce_max_sum(dist, prof["ms_total"] / 1e3, work, dev)
+    # e2e: the history uploaded from host memory every step (the call copies it)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        g.upload(start)
+        g.adjoint_grad(hist)
+    torch.cuda.synchronize()
+    te, work_e = reduce_max_sum(dist, time.perf_counter() - t0, float(prob.ngps * DIFF_INC * args.steps), dev)
+    line = None
+    if rank == 0:
+        # central differences (relative step 1e-6) of J in h0 (ampar(2)) and
+        # in a uniform shift of every initial CRSS, against the gradients
+        fd = {}
+        h0 = float(prob.ampar[0, 0, 1])
+        for name, setter, gval in (
+                ("h0", lambda p, d: p.ampar[:, :, 1].__iadd__(d), out["ampar"][0, 1]),
+                ("crss", lambda p, d: p.sv[:, 3:15].__iadd__(d), out["sv"][:, 3:15].sum())):
+            step = 1e-6 * (h0 if name == "h0" else float(start.sv[:, 3:15].mean()))
+            J = []
+            for sgn in (1.0, -1.0):
+                p = start.copy()
+                setter(p, sgn * step)
+                gg = GpuSolver(p)
+                J.append(gg.adjoint_forward(hist)[0])
+                gg.close()
+            d = (J[0] - J[1]) / (2 * step)
+            fd[name] = {"adjoint": float(gval), "central_difference": d,
+                        "rel_diff": abs(float(gval) - d) / max(abs(d), 1e-300)}
+        line = {
+            "metric": METRIC, "value": work / t_max, "unit": "GP-increments/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator, fs3pre semantics); history recorded from the 16^3 FE run",
+            "config": {"workload": WORKLOAD, "desc": DESC, "gps": prob.ngps, "increments": DIFF_INC,
+                       "checkpoint_every": DIFF_CHK, "bins": [list(b) for b in DIFF_BINS],
+                       "step": "one fas_gpu_adjoint_grad call (forward replay with checkpoints + reverse sweep)"},
+            "parallelism": f"replicas{ws}", "gpu_launches": int(prof["n_launches"]),
+            "J": out["J"], "finite_difference_check": fd,
+            "roofline": None,
+            "roofline_note": "the reverse kernel is bound by local-memory spills (profiles/k_replay_adj_points16k.md)",
+            "clocks": clk,
+            "e2e": {"value": work_e / te, "unit": "GP-increments/s",
+                    "h2d_bytes_per_step": int(hist.de.nbytes + hist.dr.nbytes + hist.w.nbytes + hist.y.nbytes),
+                    "d2h_bytes_per_step": int(prob.ngps * (6 + 63) * 8 + 10 * 8 * prob.nmatl)},
+        }
+        if ws == 1 and not args.no_cpu:
+            from oracle import OracleSolver
+            o = OracleSolver(start.copy(), 8, threads=os.cpu_count() or 1)
+            t0 = time.perf_counter()
+            o.adjoint_forward(hist)
+            dt = time.perf_counter() - t0
+            o.close()
+            line["cpu_baseline"] = {"value": prob.ngps * DIFF_INC / dt, "unit": "GP-increments/s",
+                                    "cores": os.cpu_count() or 1, "kind": "port",
+                                    "sample": "the checker's forward replay of the same history (no reverse sweep: "
+                                              f"the checker has none), {dt:.2f} s"}
+        print(json.dumps(line), flush=True)
+    g.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
 
 
 def run_gpu_points(args, ws, rank, local, dist, dev):

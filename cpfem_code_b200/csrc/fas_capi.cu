@@ -134,14 +134,17 @@ struct fas_handle {
     std::vector<double> col_bytes, col_bytes32;   // algorithmic bytes per colour launch
     DVec<int> perm, rowof, nslot, bcol;
     DVec<unsigned long long> bloc;
-    DVec<double> dn22;           // SHAPE_22's local-derivative table
+    DVec<double> dnq;            // the quadratic element's local-derivative table (SHAPE_21/22/23)
+    double wfac = 1.0;           // its GP weight factor
+    int ltype = 12;              // element type of the mesh's elements
+    int maxadj = 1;              // most elements on one node
     DVec<double> blk;
     DVec<float> blk32;           // FP32 copy for FAS_MODE_SOR_FP32
     DVec<double> sor_d, sor_r;   // correction and residual of the refinement
     DVec<double> rdiag;          // reciprocals of the diagonal entries, row order
     DVec<int> work_order, work_hist;   // work-sorted constitutive launch order
     DVec<int> cp_queue;          // head of the constitutive pass's device queue
-    DVec<int> gp_item;           // GP of item e*npg + g (20-node bricks; -1 for ties)
+    DVec<int> gp_item;           // GP of item e*npg + g (quadratic elements; -1 for ties)
     // tile layout of the persistent SOR solve (k_sor_tiles; 27-slot rows)
     int ntiles = 0;
     DVec<int> tseg, tadj_ptr, tadj, tsrc, tbcol, tprog;
@@ -212,7 +215,8 @@ struct fas_handle {
     {
         BlockDev b;
         b.R = nnod; b.slots = slots; b.brow = brow_of(slots); b.crow = crow_of(slots);
-        b.perm = perm.p; b.nslot = nslot.p; b.bcol = bcol.p; b.bloc = bloc.p; b.blk = blk.p;
+        b.perm = perm.p; b.nslot = nslot.p; b.bcol = bcol.p; b.bloc = bloc.p; b.nbw = (maxadj + 7) / 8;
+        b.blk = blk.p;
         b.blk32 = (mode & FAS_MODE_SOR_FP32) ? blk32.p : nullptr;
         return b;
     }
@@ -378,7 +382,8 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
     h->slots = maxs <= SLOTS ? SLOTS : SLOTS20;
     const int crow = crow_of(h->slots), brow = brow_of(h->slots);
     std::vector<int> nslot(nn), bcol((size_t)crow * nn, 0);
-    std::vector<unsigned long long> bloc((size_t)crow * nn, ~0ull);
+    const int nbw = (h->maxadj + 7) / 8;   // local-index words per slot
+    std::vector<unsigned long long> bloc((size_t)crow * nn * nbw, ~0ull);
     for (int p = 0; p < nn; ++p) {
         const int n = perm[p];
         const int cnt = (int)nbs[p].size();
@@ -386,16 +391,16 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
         bcol[(size_t)p * crow + h->slots] = cnt;   // the pad slot carries the slot count
         for (int s = 0; s < cnt; ++s) {
             bcol[(size_t)p * crow + s] = nbs[p][s];
-            unsigned long long word = ~0ull;
+            unsigned long long *words = &bloc[((size_t)p * crow + s) * nbw];
             int k = 0;
             for (int q = h->ne_ptr[n]; q < h->ne_ptr[n + 1]; ++q, ++k) {
                 const int e = h->ne_list[q];
                 unsigned long long b = 0xFF;
                 for (int a = 0; a < NN; ++a)
                     if (h->h_ln[(size_t)e * NN + a] == nbs[p][s]) { b = (unsigned long long)a; break; }
-                word = (word & ~(0xFFull << (8 * k))) | (b << (8 * k));
+                unsigned long long &word = words[k >> 3];
+                word = (word & ~(0xFFull << (8 * (k & 7)))) | (b << (8 * (k & 7)));
             }
-            bloc[(size_t)p * crow + s] = word;
         }
     }
     // algorithmic bytes of one colour launch: blocks and column ids of the
@@ -410,15 +415,15 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
     // algorithmic bytes of one assembly launch: each GP record read once
     // (3 nn + 28 used doubles), each block written once, the slot tables
     // and node adjacency read once, fc and ddx written
-    double ab = (double)h->nlmnt * h->npg * (3.0 * NN + 28.0) * 8.0 + (double)nn * (48.0 + 8.0 + 12.0 * MAXADJ);
-    for (int p = 0; p < nn; ++p) ab += nslot[p] * (72.0 + 4.0 + 8.0);
+    double ab = (double)h->nlmnt * h->npg * (3.0 * NN + 28.0) * 8.0 + (double)nn * (48.0 + 8.0 + 12.0 * h->maxadj);
+    for (int p = 0; p < nn; ++p) ab += nslot[p] * (72.0 + 4.0 + 8.0 * nbw);
     h->asm_bytes = ab;
     cudaStream_t s = h->stream;
     CKA(h->perm.alloc(nn));
     CKA(h->rowof.alloc(nn));
     CKA(h->nslot.alloc(nn));
     CKA(h->bcol.alloc((size_t)crow * nn));
-    CKA(h->bloc.alloc((size_t)crow * nn));
+    CKA(h->bloc.alloc(bloc.size()));
     CKA(h->blk.alloc((size_t)brow * nn));
     CK(h->perm.put(perm.data(), nn, s));
     CK(h->rowof.put(rowof.data(), nn, s));
@@ -619,6 +624,79 @@ std::vector<double> shape22_table()
     return t;
 }
 
+// SHAPE_21's local-derivative table (src/fasolt/Shapef.f90:104-189):
+// 10-node tetrahedron, corners 1, 3, 5, 10 with volume coordinates L1..L4,
+// mid-edge nodes 2 (1,3), 4 (3,5), 6 (1,5), 7 (1,10), 8 (3,10), 9 (5,10); GP
+// g at L_g = (5 + 3 sqrt5)/20, the others (5 - sqrt5)/20.  The reference's
+// local directions are L4, L2, L1 with L3 dependent: t[(g*3 + j)*10 + i] =
+// dN_i/dL_p(j) - dN_i/dL3, rounded to 6 decimals -- the reference's table.
+std::vector<double> shape21_table()
+{
+    static const int corner[10] = {0, -1, 1, -1, 2, -1, -1, -1, -1, 3};
+    static const int mid[10][2] = {{-1, -1}, {0, 1}, {-1, -1}, {1, 2}, {-1, -1},
+                                   {0, 2},   {0, 3}, {1, 3},   {2, 3}, {-1, -1}};
+    static const int dir[3] = {3, 1, 0};
+    const double r5 = std::sqrt(5.0), a = (5.0 + 3.0 * r5) / 20.0, b = (5.0 - r5) / 20.0;
+    std::vector<double> t(120);
+    for (int g = 0; g < 4; ++g) {
+        double L[4] = {b, b, b, b};
+        L[g] = a;
+        auto dNdL = [&](int i, int p) {
+            if (corner[i] >= 0) return corner[i] == p ? 4.0 * L[p] - 1.0 : 0.0;
+            const int u = mid[i][0], v = mid[i][1];
+            return p == u ? 4.0 * L[v] : (p == v ? 4.0 * L[u] : 0.0);
+        };
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 10; ++i)
+                t[(g * 3 + j) * 10 + i] = std::round((dNdL(i, dir[j]) - dNdL(i, 2)) * 1e6) / 1e6;
+    }
+    return t;
+}
+
+// SHAPE_23's local-derivative table (src/fasolt/Shapef.f90:360-485):
+// 15-node wedge, base corners 1, 3, 5 and top corners 10, 12, 14 with area
+// coordinates L1..L3 at zeta -1 / +1, base mid-edges 2, 4, 6, top 11, 13,
+// 15, vertical 7, 8, 9.  GPs 1-3 at L_(g) = 2/3 (others 1/6), zeta =
+// -1/sqrt3, GPs 4-6 above them.  Local directions L1, L2 (L3 dependent)
+// and zeta; the serendipity wedge functions' derivatives rounded to 6
+// decimals (60 of the reference's 270 tabulated entries differ from these
+// by one unit in the sixth decimal).  t[(g*3 + j)*15 + i].
+std::vector<double> shape23_table()
+{
+    static const int kind[15] = {0, 1, 0, 1, 0, 1, 2, 2, 2, 0, 1, 0, 1, 0, 1};
+    static const int la[15] = {0, 0, 1, 1, 2, 2, 0, 1, 2, 0, 0, 1, 1, 2, 2};
+    static const int lb[15] = {-1, 1, -1, 2, -1, 0, -1, -1, -1, -1, 1, -1, 2, -1, 0};
+    static const int side[15] = {-1, -1, -1, -1, -1, -1, 0, 0, 0, 1, 1, 1, 1, 1, 1};
+    std::vector<double> t(270);
+    for (int g = 0; g < 6; ++g) {
+        double L[3] = {1.0 / 6.0, 1.0 / 6.0, 1.0 / 6.0};
+        L[g % 3] = 2.0 / 3.0;
+        const double z = (g < 3 ? -1.0 : 1.0) / std::sqrt(3.0);
+        auto dNdL = [&](int i, int p) {
+            const double sd = side[i];
+            if (kind[i] == 0)
+                return la[i] == p ? 0.5 * (4.0 * L[p] - 1.0) * (1.0 + sd * z) - 0.5 * (1.0 - z * z) : 0.0;
+            if (kind[i] == 1) {
+                const double f = 2.0 * (1.0 + sd * z);
+                return p == la[i] ? f * L[lb[i]] : (p == lb[i] ? f * L[la[i]] : 0.0);
+            }
+            return la[i] == p ? 1.0 - z * z : 0.0;
+        };
+        auto dNdz = [&](int i) {
+            const double sd = side[i], La = L[la[i]];
+            if (kind[i] == 0) return 0.5 * La * (2.0 * La - 1.0) * sd + La * z;
+            if (kind[i] == 1) return 2.0 * La * L[lb[i]] * sd;
+            return -2.0 * z * La;
+        };
+        for (int i = 0; i < 15; ++i) {
+            t[(g * 3 + 0) * 15 + i] = std::round((dNdL(i, 0) - dNdL(i, 2)) * 1e6) / 1e6;
+            t[(g * 3 + 1) * 15 + i] = std::round((dNdL(i, 1) - dNdL(i, 2)) * 1e6) / 1e6;
+            t[(g * 3 + 2) * 15 + i] = std::round(dNdz(i) * 1e6) / 1e6;
+        }
+    }
+    return t;
+}
+
 int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, const fas_ctrl_desc *Cd)
 {
     int ndev = 0;
@@ -655,14 +733,17 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
     if (!h->point_mode) {
         if (!Md->le || !Md->lt || !Md->nd || !Md->np || !Md->ln || !Md->lg || !Md->ib) return FAS_E_ARG;
         const int ne = h->nlmnt;
-        // one brick family per mesh -- 8-node one-GP bricks (lt 12) or
-        // 20-node eight-GP bricks (lt 22) -- plus 2-node tie elements (lt 1-6)
+        // one element family per mesh -- 8-node one-GP bricks (lt 12),
+        // 10-node four-GP tetrahedra (lt 21), 20-node eight-GP bricks (lt
+        // 22) or 15-node six-GP wedges (lt 23) -- plus 2-node tie elements
+        // (lt 1-6)
         int lt0 = 0;
         for (int e = 0; e < ne && !lt0; ++e)
             if (Md->lt[e] >= 9) lt0 = Md->lt[e];
-        if (lt0 != 12 && lt0 != 22) return FAS_E_ELTYPE;
-        h->nn = lt0 == 12 ? 8 : 20;
-        h->npg = lt0 == 12 ? 1 : 8;
+        if (lt0 != 12 && lt0 != 21 && lt0 != 22 && lt0 != 23) return FAS_E_ELTYPE;
+        h->ltype = lt0;
+        h->nn = lt0 == 12 ? 8 : (lt0 == 21 ? 10 : (lt0 == 22 ? 20 : 15));
+        h->npg = lt0 == 12 ? 1 : (lt0 == 21 ? 4 : (lt0 == 22 ? 8 : 6));
         const int NN = h->nn, NG = h->npg;
         if (Md->ld_ln < NN || Md->ld_lg < NG || h->nnod < 1) return FAS_E_ARG;
         h->h_ln.assign((size_t)ne * NN, -1);
@@ -707,10 +788,13 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
         h->ne_ptr.assign(h->nnod + 1, 0);
         for (int e = 0; e < ne; ++e)
             for (int a = 0; a < NN && h->h_ln[(size_t)e * NN + a] >= 0; ++a) h->ne_ptr[h->h_ln[(size_t)e * NN + a] + 1]++;
+        h->maxadj = 1;
         for (int n = 0; n < h->nnod; ++n) {
             if (h->ne_ptr[n + 1] > MAXADJ) return FAS_E_RANGE;
+            h->maxadj = std::max(h->maxadj, h->ne_ptr[n + 1]);
             h->ne_ptr[n + 1] += h->ne_ptr[n];
         }
+        const int maxadj = h->maxadj;
         h->ne_list.resize(h->ne_ptr[h->nnod]);
         h->ne_locl.resize(h->ne_ptr[h->nnod]);
         std::vector<int> fill(h->ne_ptr.begin(), h->ne_ptr.end() - 1);
@@ -721,8 +805,8 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
                 h->ne_locl[fill[n]] = a;
                 fill[n]++;
             }
-        std::vector<int> lnT((size_t)NN * ne), gpeT((size_t)NG * ne), nee((size_t)MAXADJ * h->nnod, -1),
-            nel((size_t)MAXADJ * h->nnod, 0), nec(h->nnod);
+        std::vector<int> lnT((size_t)NN * ne), gpeT((size_t)NG * ne), nee((size_t)maxadj * h->nnod, -1),
+            nel((size_t)maxadj * h->nnod, 0), nec(h->nnod);
         for (int e = 0; e < ne; ++e) {
             for (int a = 0; a < NN; ++a) lnT[(size_t)a * ne + e] = h->h_ln[(size_t)e * NN + a];
             for (int q = 0; q < NG; ++q) gpeT[(size_t)q * ne + e] = h->h_gpe[(size_t)e * NG + q];
@@ -734,10 +818,11 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
                 nel[(size_t)k * h->nnod + n] = h->ne_locl[h->ne_ptr[n] + k];
             }
         }
-        if (NN == 20) {
-            const std::vector<double> t = shape22_table();
-            CKA(h->dn22.alloc(t.size()));
-            CK(h->dn22.put(t.data(), t.size(), s));
+        if (NN != 8) {
+            const std::vector<double> t = NN == 20 ? shape22_table() : (NN == 10 ? shape21_table() : shape23_table());
+            h->wfac = NN == 20 ? 1.0 : (NN == 10 ? -0.0416667 : 0.16666667);
+            CKA(h->dnq.alloc(t.size()));
+            CK(h->dnq.put(t.data(), t.size(), s));
             CKA(h->gp_item.alloc(h->h_gpe.size()));
             CK(h->gp_item.put(h->h_gpe.data(), h->h_gpe.size(), s));
         }
@@ -1043,13 +1128,21 @@ template <typename K> unsigned cp_grid(fas_handle *h, K kern, long long n, int *
 template <int NS> int launch_elem(fas_handle *h, int inc, int nit)
 {
     Span sp(h, &h->P.ms_constitutive);
-    if (h->nn == 20) {   // 20-node bricks: one thread per (element, GP)
-        const int *order = work_order(h, 8 * h->nlmnt, h->gp_item.p);
-        int *queue = nullptr;
-        const unsigned grid = cp_grid(h, k_elem22<NS>, 8LL * h->nlmnt, &queue);
-        k_elem22<NS><<<grid, 128, 0, h->stream>>>(
-            h->mesh(), h->M, h->C, h->gp(), h->dn22.p, h->x.p, h->dx.p, h->rec.p, h->h_tiem[inc - 1], inc, nit,
-            h->ekey.p, order, queue);
+    if (h->nn != 8) {   // quadratic elements: one thread per (element, GP)
+        auto go = [&](auto kern) {
+            const long long nit_items = (long long)h->npg * h->nlmnt;
+            const int *order = work_order(h, (int)nit_items, h->gp_item.p);
+            int *queue = nullptr;
+            const unsigned grid = cp_grid(h, kern, nit_items, &queue);
+            kern<<<grid, 128, 0, h->stream>>>(h->mesh(), h->M, h->C, h->gp(), h->dnq.p, h->wfac, h->x.p, h->dx.p,
+                                              h->rec.p, h->h_tiem[inc - 1], inc, nit, h->ekey.p, order, queue);
+        };
+        if (h->nn == 20)
+            go(k_elemq<NS, 20, 8>);
+        else if (h->nn == 10)
+            go(k_elemq<NS, 10, 4>);
+        else
+            go(k_elemq<NS, 15, 6>);
     }
     else if (!(h->mode & FAS_MODE_CP_WARP)) {
         const int *order = work_order(h, h->nlmnt, h->gpe.p);
@@ -1104,7 +1197,10 @@ int elvals_impl(fas_handle *h, int inc, int nit, bool bc)
     {
         Span sp(h, &h->P.ms_assembly);
         const long long nthr = (long long)h->slots * h->nnod;   // thread (row, slot), row-major
-        auto kern = h->nn == 20 ? k_assemble<20, 8> : k_assemble<8, 1>;
+        auto kern = h->nn == 20   ? k_assemble<20, 8>
+                    : h->nn == 10 ? k_assemble<10, 4>
+                    : h->nn == 15 ? k_assemble<15, 6>
+                                  : k_assemble<8, 1>;
         kern<<<nblocks(nthr, 256), 256, 0, s>>>(
             h->mesh(), h->block(), h->rec.p, h->x.p, h->dx.p, h->fc.p, h->ddx.p,
             h->xspec.p + (size_t)(inc - 1) * std::max(h->nxs, 1) * 15,

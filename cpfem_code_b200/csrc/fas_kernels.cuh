@@ -4,19 +4,20 @@
 //   * nodal vectors x, dx, fc, ddx, rhs: reference DOF order 3*node+comp;
 //   * Gauss-point state: structure of arrays field[k * ngps + g];
 //   * Gauss-point record rec[item * RecLayout<NN>::LEN + .] (item = element
-//     for 8-node bricks, element*8 + GP for 20-node bricks): sfd (3 NN),
+//     for 8-node bricks, element*NPG + GP for the quadratic elements):
+//     sfd (3 NN),
 //     stress (6), weight, tangent upper triangle (21) -- written once per
 //     Newton iteration by the element kernel, read by the row-gather
 //     assembly;
 //   * stiffness: block-ELL of 3x3 node blocks, rows permuted so each SOR
-//     colour is a contiguous row range.  A row of S slots (27 for 8-node,
-//     81 for 20-node bricks) holds brow_of(S) values, component-major:
+//     colour is a contiguous row range.  A row of S slots (27 for 8-node
+//     bricks, 81 for the quadratic elements) holds brow_of(S) values, component-major:
 //     blk[row*brow + (r*3+c)*S + slot], padded so FP64 and FP32 rows are
 //     16-byte multiples as bulk copies need (244 and 732 values).  Slot 0 is
 //     the diagonal block; bcol[row*crow + slot] is the column node and
 //     bcol[row*crow + S] the row's slot count (crow = 28 or 84).
 //
-// Kernels: the element pass (k_elem, k_elem22, the opt-in warp variants),
+// Kernels: the element pass (k_elem, k_elemq, the opt-in warp variants),
 // the work-sorted launch order of the constitutive kernels (k_work_*), the
 // row-gather assembly with fused SUVALS (k_assemble), the SOR colour phase
 // streamed by the bulk-copy engine (k_sor_colour_tma, launched with
@@ -39,7 +40,7 @@ constexpr int REC = RecLayout<8>::LEN;   // 56 doubles per 8-node element record
 constexpr int REC_S = RecLayout<8>::S, REC_W = RecLayout<8>::W, REC_D = RecLayout<8>::D;
 constexpr int SLOTS = 27;        // node blocks per row of an 8-node brick mesh
 constexpr int SLOTS20 = 81;      // node blocks per row of a 20-node brick mesh
-constexpr int MAXADJ = 8;        // elements per node
+constexpr int MAXADJ = 64;       // elements per node the tables allow (bytes of a local-index word)
 
 // block matrix addressing: a row of S slots holds 9 S values padded to a
 // multiple of 4 (so FP64 and FP32 rows are both 16-byte multiples, as bulk
@@ -61,8 +62,8 @@ struct MeshDev {
     const int *le;       // [nlmnt]
     const int *lt;       // [nlmnt] element type: the family's (12 or 22), or 1-6 for a tie
     const int *ib;       // [nnod]
-    const int *ne_elem;  // [MAXADJ][nnod] adjacent elements, ascending
-    const int *ne_loc;   // [MAXADJ][nnod] local index of the node in it
+    const int *ne_elem;  // [maxadj][nnod] adjacent elements, ascending
+    const int *ne_loc;   // [maxadj][nnod] local index of the node in it
     const int *ne_cnt;   // [nnod]
 };
 
@@ -72,8 +73,9 @@ struct BlockDev {
     const int *perm;     // row -> node
     const int *nslot;    // [R]
     const int *bcol;     // [R][crow] column node of each slot; [slots] = nslot
-    const unsigned long long *bloc;   // [R][crow] byte k: local index of the column node
+    const unsigned long long *bloc;   // [R][crow][nbw] byte k: local index of the column node
                                       // in the k-th adjacent element of the row node (0xFF: absent)
+    int nbw;             // words of bloc per slot: ceil(elements per node / 8)
     double *blk;         // [R][brow]: value (r, c) of slot s at (r*3+c)*slots + s
     float *blk32;        // FP32 copy of blk (tuned mode), or null
     __host__ __device__ size_t si(int p, int s) const { return (size_t)p * crow + s; }
@@ -177,34 +179,37 @@ __global__ void __launch_bounds__(128) k_elem(MeshDev Mh, DevMat M, DevCtrl C, D
     });
 }
 
-// ELVALS per Gauss point of 20-node bricks (src/fasolt/Elvals.f90:82-126
-// with SHAPE_22, src/fasolt/Shapef.f90:210-342): one thread per (element,
-// GP).  dn22[(g*3 + j)*20 + i] = dndn(j+1, i+1, g+1) is the reference's
-// tabulated local-derivative table.  The element's 20 nodes are streamed
+// ELVALS per Gauss point of the quadratic elements (src/fasolt/Elvals.f90:
+// 82-126): 10-node tetrahedra with SHAPE_21 (NN 10, NPG 4,
+// src/fasolt/Shapef.f90:104-189), 20-node bricks with SHAPE_22 (20, 8,
+// :210-342) and 15-node wedges with SHAPE_23 (15, 6, :360-485); one thread
+// per (element, GP).  dnt[(g*3 + j)*NN + i] = dndn(j+1, i+1, g+1) is the
+// element type's tabulated local-derivative table and wfac its GP weight
+// factor (-0.0416667, 1, 0.16666667).  The element's nodes are streamed
 // twice -- the Jacobian, then sfd (written straight to the GP record) and
-// the displacement gradient -- so no 20-node array is held in registers.
+// the displacement gradient -- so no node array is held in registers.
 // Errors are keyed by (element, GP) so the first one in the reference's
 // loop order wins.
-template <int NS>
-__global__ void __launch_bounds__(128) k_elem22(MeshDev Mh, DevMat M, DevCtrl C, DevGp G,
-                                                const double *__restrict__ dn22,
-                                                const double *__restrict__ x,
-                                                const double *__restrict__ dx, double *rec,
-                                                double dt, int inc, int nit,
-                                                unsigned long long *errkey, const int *__restrict__ order,
-                                                int *queue)
+template <int NS, int NN, int NPG>
+__global__ void __launch_bounds__(128) k_elemq(MeshDev Mh, DevMat M, DevCtrl C, DevGp G,
+                                               const double *__restrict__ dnt, double wfac,
+                                               const double *__restrict__ x,
+                                               const double *__restrict__ dx, double *rec,
+                                               double dt, int inc, int nit,
+                                               unsigned long long *errkey, const int *__restrict__ order,
+                                               int *queue)
 {
-    using L = RecLayout<20>;
-    for_each_item(8 * Mh.nlmnt, order, queue, [&](int t) {   // item e*8 + gq
-        const int e = (int)(t >> 3), gq = (int)(t & 7);
+    using L = RecLayout<NN>;
+    for_each_item(NPG * Mh.nlmnt, order, queue, [&](int t) {   // item e*NPG + gq
+        const int e = t / NPG, gq = t - e * NPG;
         if (Mh.lt[e] < 9) return;   // tie element: no Gauss point
         const int ne = Mh.nlmnt;
         const unsigned long long key = (unsigned long long)t << 16;
-        const double *dn = dn22 + gq * 60;
+        const double *dn = dnt + gq * 3 * NN;
         double jac[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-        for (int i = 0; i < 20; ++i) {
+        for (int i = 0; i < NN; ++i) {
             const int n = Mh.ln[i * ne + e];
-            const double d0 = __ldg(dn + i), d1 = __ldg(dn + 20 + i), d2 = __ldg(dn + 40 + i);
+            const double d0 = __ldg(dn + i), d1 = __ldg(dn + NN + i), d2 = __ldg(dn + 2 * NN + i);
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 const double xk = x[3 * n + k];
@@ -214,16 +219,16 @@ __global__ void __launch_bounds__(128) k_elem22(MeshDev Mh, DevMat M, DevCtrl C,
             }
         }
         double inv[3][3];
-        const double w = 1.0 * invert3(jac, inv);
+        const double w = wfac * invert3(jac, inv);
         if (w < 1.e-7) {
             atomicMin(errkey, key | 920ull);
             return;
         }
         double *R = rec + (size_t)t * L::LEN;
         double gr[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-        for (int i = 0; i < 20; ++i) {
+        for (int i = 0; i < NN; ++i) {
             const int n = Mh.ln[i * ne + e];
-            const double d0 = __ldg(dn + i), d1 = __ldg(dn + 20 + i), d2 = __ldg(dn + 40 + i);
+            const double d0 = __ldg(dn + i), d1 = __ldg(dn + NN + i), d2 = __ldg(dn + 2 * NN + i);
             double sf[3];
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
@@ -612,12 +617,12 @@ __global__ void __launch_bounds__(256) k_assemble(MeshDev Mh, BlockDev B,
     if (p >= B.R) return;
     if (s >= B.nslot[p]) return;
     const int n = B.perm[p];
-    const unsigned long long bl = B.bloc[B.si(p, s)];
+    const unsigned long long *bl = B.bloc + B.si(p, s) * B.nbw;
     const int cnt = Mh.ne_cnt[n];
     double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     double f[3] = {0, 0, 0};
     for (int k = 0; k < cnt; ++k) {
-        const int b = (int)((bl >> (8 * k)) & 0xFFull);
+        const int b = (int)((bl[k >> 3] >> (8 * (k & 7))) & 0xFFull);
         if (b == 0xFF) continue;
         const int e = Mh.ne_elem[k * Mh.nnod + n];
         const int a = Mh.ne_loc[k * Mh.nnod + n];

@@ -18,6 +18,7 @@ same tables directly, for 8-node one-Gauss-point bricks (``lt = 12``) and
 """
 from __future__ import annotations
 
+import itertools
 import math
 
 import numpy as np
@@ -35,6 +36,54 @@ BRICK20_HALF = np.array([(0, 0, 0), (1, 0, 0), (2, 0, 0), (2, 1, 0), (2, 2, 0), 
                          (0, 1, 0), (0, 0, 1), (2, 0, 1), (2, 2, 1), (0, 2, 1), (0, 0, 2), (1, 0, 2),
                          (2, 0, 2), (2, 1, 2), (2, 2, 2), (1, 2, 2), (0, 2, 2), (0, 1, 2)], dtype=np.int64)
 
+
+
+def _tet10_templates():
+    """The 6 tetrahedra of a brick split along its main diagonal (Kuhn's
+    triangulation), as 10-node elements in half edges: corners 1, 3, 5, 10
+    with 1, 3, 5 anticlockwise seen from 10 (SHAPE_21's convention,
+    src/fasolt/Shapef.f90:91-100), mid-edge nodes 2 (1,3), 4 (3,5), 6 (1,5),
+    7 (1,10), 8 (3,10), 9 (5,10)."""
+    out = []
+    for perm in itertools.permutations(range(3)):
+        v = [np.zeros(3, np.int64)]
+        for k in perm[:2]:
+            w = v[-1].copy()
+            w[k] += 2
+            v.append(w)
+        v.append(np.array([2, 2, 2], np.int64))
+        c1, c3, c5, c10 = v
+        if np.dot(np.cross(c3 - c1, c5 - c1), c10 - c1) < 0:
+            c3, c5 = c5, c3
+        m = lambda a, b: (a + b) // 2
+        out.append(np.array([c1, m(c1, c3), c3, m(c3, c5), c5, m(c1, c5), m(c1, c10), m(c3, c10), m(c5, c10), c10]))
+    return out
+
+
+def _wedge15_templates():
+    """The 2 wedges of a brick split along the diagonal plane of its x-y
+    faces, as 15-node elements in half edges: base corners 1, 3, 5
+    anticlockwise seen from the top, top corners 10, 12, 14 above them,
+    mid-edge nodes as SHAPE_23 numbers them (src/fasolt/Shapef.f90:348-356)."""
+    out = []
+    for tri in (((0, 0), (2, 0), (2, 2)), ((0, 0), (2, 2), (0, 2))):
+        b = [np.array([x, y, 0], np.int64) for x, y in tri]
+        t = [c + np.array([0, 0, 2]) for c in b]
+        m = lambda a, c: (a + c) // 2
+        out.append(np.array([b[0], m(b[0], b[1]), b[1], m(b[1], b[2]), b[2], m(b[2], b[0]),
+                             m(b[0], t[0]), m(b[1], t[1]), m(b[2], t[2]),
+                             t[0], m(t[0], t[1]), t[1], m(t[1], t[2]), t[2], m(t[2], t[0])]))
+    return out
+
+
+# element family: (element type lt, Gauss points, lattice step in the
+# templates, node templates per brick of the lattice)
+FAMILIES = {
+    8: (12, 1, 1, [BRICK8]),
+    10: (21, 4, 2, _tet10_templates()),
+    15: (23, 6, 2, _wedge15_templates()),
+    20: (22, 8, 2, [BRICK20_HALF]),
+}
 
 # ----------------------------------------------------------------- materials
 def cubic_compliance(c11: float, c12: float, c44: float) -> np.ndarray:
@@ -327,22 +376,21 @@ def structured_cube(n=(8, 8, 8), lengths=(1.0, 1.0, 1.0), xfree: int = 3,
     each grain draws its material from `fractions` (fs3p-matl.f90:33-57
     draws per element; here per grain so grains stay single-phase)."""
     nx, ny, nz = (int(v) for v in n)
-    if nodes not in (8, 20):
-        raise ValueError("nodes must be 8 or 20")
+    if nodes not in FAMILIES:
+        raise ValueError("nodes must be 8, 10, 15 or 20")
     materials = materials or [fcc_aluminium()]
-    nel = nx * ny * nz
+    ltype, npg, h, tmpl = FAMILIES[nodes]
+    nsub = len(tmpl)                         # elements per brick of the lattice
+    nel = nx * ny * nz * nsub
     dxl = np.array([lengths[0] / nx, lengths[1] / ny, lengths[2] / nz])
     iz, iy, ix = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
-    ix, iy, iz = ix.ravel(), iy.ravel(), iz.ravel()          # element order: x fastest
-    # node positions on the lattice of half (20 nodes) or whole edges (8 nodes)
-    if nodes == 8:
-        off, h = BRICK8, 1
-    else:
-        off, h = BRICK20_HALF, 2
-    npg = 1 if nodes == 8 else 8
-    gx = h * ix[:, None] + off[None, :, 0]
-    gy = h * iy[:, None] + off[None, :, 1]
-    gz = h * iz[:, None] + off[None, :, 2]
+    # element order: x fastest, the sub-elements of one brick together
+    ix, iy, iz = (np.repeat(a.ravel(), nsub) for a in (ix, iy, iz))
+    # node positions on the lattice of half (quadratic) or whole edges (8 nodes)
+    off_e = np.tile(np.stack(tmpl), (nx * ny * nz, 1, 1))    # [nel, nodes, 3]
+    gx = h * ix[:, None] + off_e[:, :, 0]
+    gy = h * iy[:, None] + off_e[:, :, 1]
+    gz = h * iz[:, None] + off_e[:, :, 2]
     key = (gx + (h * nx + 1) * (gy + (h * ny + 1) * gz)).ravel()
     uniq, first, inv = np.unique(key, return_index=True, return_inverse=True)
     order = np.argsort(first, kind="stable")
@@ -354,7 +402,7 @@ def structured_cube(n=(8, 8, 8), lengths=(1.0, 1.0, 1.0), xfree: int = 3,
     fo = first[order]
     fe, fa = fo // nodes, fo % nodes
     x0 = np.stack([dxl[0] * ix[fe], dxl[1] * iy[fe], dxl[2] * iz[fe]], axis=1)
-    xyz = x0 + dxl[None, :] * (off[fa] / float(h))
+    xyz = x0 + dxl[None, :] * (off_e[fe, fa] / float(h))
     x = np.ascontiguousarray(xyz.reshape(-1))
     tolerance = 0.5 * float(dxl.min()) / h   # SETSWTOL: 0.5 * shortest intra-element distance
     ib = setbounds(x, tolerance, xfree)
@@ -379,7 +427,7 @@ def structured_cube(n=(8, 8, 8), lengths=(1.0, 1.0, 1.0), xfree: int = 3,
     tiem, x_spec = setkinc(lengths, xfree, eps_inc, ninc)
     nsv = 3 + int(nss.max())
     ngps = npg * nel
-    lt = np.full(nel, 12 if nodes == 8 else 22, np.int32)
+    lt = np.full(nel, ltype, np.int32)
     nd = np.full(nel, nodes, np.int32)
     npa = np.full(nel, npg, np.int32)
     lg = np.arange(1, ngps + 1, dtype=np.int32).reshape(nel, npg)

@@ -45,7 +45,7 @@ extern "C" {
 #define FAS_E_ARG          (-1)  /* null / inconsistent argument            */
 #define FAS_E_NODEVICE     (-2)  /* no sm_100 (B200) device visible          */
 #define FAS_E_CUDA         (-3)  /* a CUDA runtime call failed               */
-#define FAS_E_ELTYPE       (-4)  /* element type not implemented: lt other than 12 or 22, or both in one mesh */
+#define FAS_E_ELTYPE       (-4)  /* element type not implemented: lt other than 12, 21, 22 or 23 (ties 1-6 aside), or two of them in one mesh */
 #define FAS_E_NOMEM        (-5)  /* device allocation failed                 */
 #define FAS_E_RANGE        (-6)  /* size beyond a documented maximum         */
 #define FAS_E_STATE        (-7)  /* call out of order (e.g. no state yet)    */

@@ -322,6 +322,131 @@ inline const Shape22Table &shape22_table()
     return t;
 }
 
+// SHAPE_21, src/fasolt/Shapef.f90:104-189: 10-node tetrahedron, 4 Gauss
+// points.  Corner nodes 1, 3, 5, 10 carry volume coordinates L1..L4;
+// mid-edge nodes 2 (1,3), 4 (3,5), 6 (1,5), 7 (1,10), 8 (3,10), 9 (5,10).
+// GP g has L_g = (5 + 3 sqrt5)/20 and the other three (5 - sqrt5)/20.  The
+// reference's three local directions are L4, L2 and L1 with L3 dependent:
+// dndn(k) = dN/dL_p(k) - dN/dL3 for p = (4, 2, 1), its derivatives of
+// L(2L-1) (corners) and 4 L_i L_j (mid-edges) rounded to 6 decimals as the
+// reference tabulates them -- which reproduces every entry of that table.
+// weight = -0.0416667 det(J).
+struct Shape21Table {
+    double dn[4][3][10];   // dn[g][j][i] = dndn(j+1, i+1, g+1)
+};
+inline const Shape21Table &shape21_table()
+{
+    static const Shape21Table t = [] {
+        static const int corner[10] = {0, -1, 1, -1, 2, -1, -1, -1, -1, 3};   // node -> L index
+        static const int mid[10][2] = {{-1, -1}, {0, 1}, {-1, -1}, {1, 2}, {-1, -1},
+                                       {0, 2},   {0, 3}, {1, 3},   {2, 3}, {-1, -1}};
+        static const int dir[3] = {3, 1, 0};
+        const double r5 = std::sqrt(5.0), a = (5.0 + 3.0 * r5) / 20.0, b = (5.0 - r5) / 20.0;
+        Shape21Table t{};
+        for (int g = 0; g < 4; ++g) {
+            double L[4] = {b, b, b, b};
+            L[g] = a;
+            auto dNdL = [&](int i, int p) {
+                if (corner[i] >= 0) return corner[i] == p ? 4.0 * L[p] - 1.0 : 0.0;
+                const int u = mid[i][0], v = mid[i][1];
+                return p == u ? 4.0 * L[v] : (p == v ? 4.0 * L[u] : 0.0);
+            };
+            for (int j = 0; j < 3; ++j)
+                for (int i = 0; i < 10; ++i)
+                    t.dn[g][j][i] = std::round((dNdL(i, dir[j]) - dNdL(i, 2)) * 1e6) / 1e6;
+        }
+        return t;
+    }();
+    return t;
+}
+
+// SHAPE_23, src/fasolt/Shapef.f90:360-485: 15-node pentahedron (wedge), 6
+// Gauss points.  Base corners 1, 3, 5 and top corners 10, 12, 14 carry area
+// coordinates L1..L3 at zeta = -1 / +1; mid-edge nodes 2 (1,3), 4 (3,5),
+// 6 (5,1) on the base, 11, 13, 15 on the top, 7, 8, 9 on the vertical
+// edges.  GP g < 3 sits at L_(g) = 2/3, the others 1/6, zeta = -1/sqrt3;
+// GPs 4-6 above them at +1/sqrt3.  Local directions L1 and L2 (L3
+// dependent) and zeta; the serendipity wedge functions' derivatives rounded
+// to 6 decimals.  This reproduces 210 of the reference's 270 tabulated
+// entries; the other 60 differ from it by one unit in the sixth decimal
+// (rounding of the reference's own tabulation).  weight = det(J) / 6.
+struct Shape23Table {
+    double dn[6][3][15];
+};
+inline const Shape23Table &shape23_table()
+{
+    static const Shape23Table t = [] {
+        // node -> (kind, a, b, side): kind 0 corner (L a), 1 mid-edge (L a,
+        // L b), 2 vertical mid-edge (L a); side -1 base, +1 top
+        static const int kind[15] = {0, 1, 0, 1, 0, 1, 2, 2, 2, 0, 1, 0, 1, 0, 1};
+        static const int la[15] = {0, 0, 1, 1, 2, 2, 0, 1, 2, 0, 0, 1, 1, 2, 2};
+        static const int lb[15] = {-1, 1, -1, 2, -1, 0, -1, -1, -1, -1, 1, -1, 2, -1, 0};
+        static const int side[15] = {-1, -1, -1, -1, -1, -1, 0, 0, 0, 1, 1, 1, 1, 1, 1};
+        Shape23Table t{};
+        for (int g = 0; g < 6; ++g) {
+            double L[3] = {1.0 / 6.0, 1.0 / 6.0, 1.0 / 6.0};
+            L[g % 3] = 2.0 / 3.0;
+            const double z = (g < 3 ? -1.0 : 1.0) / std::sqrt(3.0);
+            auto dNdL = [&](int i, int p) {   // at fixed zeta
+                const double s = side[i];
+                if (kind[i] == 0)
+                    return la[i] == p ? 0.5 * (4.0 * L[p] - 1.0) * (1.0 + s * z) - 0.5 * (1.0 - z * z) : 0.0;
+                if (kind[i] == 1) {
+                    const double f = 2.0 * (1.0 + s * z);
+                    return p == la[i] ? f * L[lb[i]] : (p == lb[i] ? f * L[la[i]] : 0.0);
+                }
+                return la[i] == p ? 1.0 - z * z : 0.0;
+            };
+            auto dNdz = [&](int i) {
+                const double s = side[i], La = L[la[i]];
+                if (kind[i] == 0) return 0.5 * La * (2.0 * La - 1.0) * s + La * z;
+                if (kind[i] == 1) return 2.0 * La * L[lb[i]] * s;
+                return -2.0 * z * La;
+            };
+            for (int i = 0; i < 15; ++i) {
+                t.dn[g][0][i] = std::round((dNdL(i, 0) - dNdL(i, 2)) * 1e6) / 1e6;
+                t.dn[g][1][i] = std::round((dNdL(i, 1) - dNdL(i, 2)) * 1e6) / 1e6;
+                t.dn[g][2][i] = std::round(dNdz(i) * 1e6) / 1e6;
+            }
+        }
+        return t;
+    }();
+    return t;
+}
+
+// The Jacobian, its inverse and the global derivatives of an NN-node
+// element from tabulated local derivatives dn[j][i] (j local direction);
+// returns det(J).  The steps of SHAPE_21/22/23 after their tables.
+template <class R, int NN> R shape_tab(const double dn_t[3][NN], const R xn[20][3], R dndx[20][3])
+{
+    R dn[3][NN];
+    for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < NN; ++i) dn[j][i] = (R)dn_t[j][i];
+    R jac[3][3];
+    for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 3; ++j) {
+            R s = 0;
+            for (int i = 0; i < NN; ++i) s = s + dn[j][i] * xn[i][k];
+            jac[j][k] = s;
+        }
+    R w = invert3(jac);
+    for (int i = 0; i < NN; ++i)
+        for (int k = 0; k < 3; ++k) {
+            R s = 0;
+            for (int j = 0; j < 3; ++j) s = s + jac[k][j] * dn[j][i];
+            dndx[i][k] = s;
+        }
+    return w;
+}
+template <class R> R shape21(int g, const R xn[20][3], R dndx[20][3])
+{
+    return R(-0.0416667) * shape_tab<R, 10>(shape21_table().dn[g], xn, dndx);
+}
+template <class R> R shape23(int g, const R xn[20][3], R dndx[20][3])
+{
+    return R(0.16666667) * shape_tab<R, 15>(shape23_table().dn[g], xn, dndx);
+}
+
 // xn[i][k] = xnode(k+1,i+1); dndx[i][k] = dndx(k+1,i+1); g is 0-based.
 template <class R> R shape22(int g, const R xn[20][3], R dndx[20][3])
 {
@@ -991,8 +1116,10 @@ template <class R> int elvals(Problem<R> &P, int inc, int nit)
             const int ng = P.np[e];
             for (int ig = 0; ig < ng; ++ig) {
                 R sfd[20][3];
-                R weight = itp == 12 ? shape12(reinterpret_cast<const R(*)[3]>(xl), reinterpret_cast<R(*)[3]>(sfd))
-                                     : shape22(ig, xl, sfd);
+                R weight = itp == 12   ? shape12(reinterpret_cast<const R(*)[3]>(xl), reinterpret_cast<R(*)[3]>(sfd))
+                           : itp == 21 ? shape21(ig, xl, sfd)
+                           : itp == 23 ? shape23(ig, xl, sfd)
+                                       : shape22(ig, xl, sfd);
                 if (weight < R(1.e-7)) { rc_buf[e - e0] = 920; break; }
                 const int j = P.lg[(size_t)e * 8 + ig];
                 R del[6], r[3], defl;
@@ -1376,9 +1503,12 @@ int create(Problem<R> &P, const fas_mesh_desc *M, const fas_matl_desc *T, const 
         P.ln.assign((size_t)P.nlmnt * P.ldn, 0);
         P.lg.assign((size_t)P.nlmnt * 8, 0);
         for (int e = 0; e < P.nlmnt; ++e) {
-            if (!(P.lt[e] == 12 || P.lt[e] == 22 || P.lt[e] < 9)) return FAS_E_ELTYPE;
+            if (!(P.lt[e] == 12 || P.lt[e] == 21 || P.lt[e] == 22 || P.lt[e] == 23 || P.lt[e] < 9))
+                return FAS_E_ELTYPE;
             if (P.lt[e] == 12 && (P.nd[e] != 8 || P.np[e] != 1)) return FAS_E_ARG;
+            if (P.lt[e] == 21 && (P.nd[e] != 10 || P.np[e] != 4 || M->ld_lg < 4)) return FAS_E_ARG;
             if (P.lt[e] == 22 && (P.nd[e] != 20 || P.np[e] != 8 || M->ld_lg < 8)) return FAS_E_ARG;
+            if (P.lt[e] == 23 && (P.nd[e] != 15 || P.np[e] != 6 || M->ld_lg < 6)) return FAS_E_ARG;
             for (int i = 0; i < P.nd[e]; ++i) {
                 int id = M->ln[(size_t)e * M->ld_ln + i];
                 if (id < 1 || id > P.nnod) return FAS_E_ARG;
@@ -1917,6 +2047,39 @@ double ora_shape22(int g, const double *x320, double *d320)
     for (int i = 0; i < 20; ++i)
         for (int k = 0; k < 3; ++k) d320[k + 3 * i] = dn[i][k];
     return w;
+}
+// SHAPE_21 / SHAPE_22 / SHAPE_23 of element type lt for GP g (0-based):
+// x[3*i + k] node coordinates, d[3*i + k] global derivatives; returns the
+// GP weight (0 for an unknown type or GP).
+double ora_shape_elem(int lt, int g, const double *x, double *d)
+{
+    const int nn = lt == 21 ? 10 : (lt == 22 ? 20 : (lt == 23 ? 15 : 0));
+    const int ng = lt == 21 ? 4 : (lt == 22 ? 8 : (lt == 23 ? 6 : 0));
+    if (!nn || g < 0 || g >= ng) return 0.0;
+    double xn[20][3] = {}, dn[20][3] = {};
+    for (int i = 0; i < nn; ++i)
+        for (int k = 0; k < 3; ++k) xn[i][k] = x[k + 3 * i];
+    const double w = lt == 21 ? shape21<double>(g, xn, dn) : (lt == 22 ? shape22<double>(g, xn, dn)
+                                                                         : shape23<double>(g, xn, dn));
+    for (int i = 0; i < nn; ++i)
+        for (int k = 0; k < 3; ++k) d[k + 3 * i] = dn[i][k];
+    return w;
+}
+// The local-derivative tables of SHAPE_21 ([4][3][10]) and SHAPE_23
+// ([6][3][15]), dn[(g*3 + j)*nn + i].
+void ora_shape21_table(double *dn)
+{
+    const Shape21Table &t = shape21_table();
+    for (int g = 0; g < 4; ++g)
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 10; ++i) dn[(g * 3 + j) * 10 + i] = t.dn[g][j][i];
+}
+void ora_shape23_table(double *dn)
+{
+    const Shape23Table &t = shape23_table();
+    for (int g = 0; g < 6; ++g)
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 15; ++i) dn[(g * 3 + j) * 15 + i] = t.dn[g][j][i];
 }
 void ora_shape22_table(double *dn)
 {

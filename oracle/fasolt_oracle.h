@@ -83,6 +83,10 @@ double  ora_shape12(const double *xnode_3x8_colmajor, double *dndx_3x8_colmajor)
 double  ora_shape22(int g, const double *xnode_3x20_colmajor, double *dndx_3x20_colmajor);
 void    ora_shape22_table(double *dn_8x3x20);
 
+/* SHAPE_21/22/23 of type lt at GP g (tests) and the SHAPE_21/23 tables. */
+double ora_shape_elem(int lt, int g, const double *x, double *d);
+void ora_shape21_table(double *dn);
+void ora_shape23_table(double *dn);
 #ifdef __cplusplus
 }
 #endif

@@ -49,7 +49,10 @@ def _load() -> C.CDLL:
                 ("ora_tens_rot", [C.POINTER(C.c_double)] * 3, None),
                 ("ora_shape12", [C.POINTER(C.c_double)] * 2, C.c_double),
                 ("ora_shape22", [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_double),
-                ("ora_shape22_table", [C.POINTER(C.c_double)], None)):
+                ("ora_shape22_table", [C.POINTER(C.c_double)], None),
+                ("ora_shape_elem", [C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_double),
+                ("ora_shape21_table", [C.POINTER(C.c_double)], None),
+                ("ora_shape23_table", [C.POINTER(C.c_double)], None)):
             f = getattr(lib, name)
             f.argtypes, f.restype = args, res
         _lib = lib
