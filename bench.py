@@ -276,10 +276,10 @@ def cpu_steps(prob, steps: int, threads: int):
 
 
 def cpu_points(prob, threads: int):
-    """The checker's DSTRSS pass over the first POINTS_CPU points."""
-    from cpfem_code_b200 import generator
+    """The checker's DSTRSS pass over the first POINTS_CPU points of `prob`
+    (the inputs before the pass)."""
     from oracle import OracleSolver
-    p = generator.point_batch(POINTS_CPU, seed=1)
+    p = prob.first_points(POINTS_CPU)
     o = OracleSolver(p, 8, threads=threads)
     t0 = time.perf_counter()
     o.constitutive(1, 1)
@@ -428,7 +428,8 @@ def run_increments(g, prob, start, ninc_warm: int, ninc_timed: int):
     incs = list(range(ninc_warm + 1, ninc_warm + ninc_timed + 1))
     out, ends = {}, {}
     legs = [("plain", abi.FAS_MODE_PLAIN), ("tuned", TUNED_MODE),
-            ("plain_consistent_tangent", abi.FAS_MODE_TANGENT_CONSISTENT)]
+            ("plain_consistent_tangent", abi.FAS_MODE_TANGENT_CONSISTENT),
+            ("plain_graph", abi.FAS_MODE_GRAPH), ("tuned_graph", TUNED_MODE | abi.FAS_MODE_GRAPH)]
     if WORKLOAD == "mixed32":
         # the persistent phase-sorted queue for the constitutive passes
         legs.append(("plain_cp_queue", abi.FAS_MODE_CP_QUEUE))
@@ -460,6 +461,14 @@ def run_increments(g, prob, start, ninc_warm: int, ninc_timed: int):
     out["speedup_tuned_vs_plain_s_per_increment"] = out["plain"]["s_per_increment"] / out["tuned"]["s_per_increment"]
     out["tuned_vs_plain_error"] = e
     out["consistent_tangent_vs_plain_error"] = stress_errors(ends["plain_consistent_tangent"], ends["plain"])
+    out["plain_graph"]["mode"] = "plain FP64, each increment's NRITER as one CUDA graph (conditional while nodes)"
+    out["plain_graph"]["same_result_as_plain"] = all(
+        np.array_equal(getattr(ends["plain_graph"], k), getattr(ends["plain"], k)) for k in _state_arrays(s0))
+    out["speedup_graph_vs_plain_s_per_increment"] = (out["plain"]["s_per_increment"]
+                                                     / out["plain_graph"]["s_per_increment"])
+    out["tuned_graph"]["mode"] = "the tuned form with each increment's NRITER as one CUDA graph"
+    out["tuned_graph"]["same_result_as_tuned"] = all(
+        np.array_equal(getattr(ends["tuned_graph"], k), getattr(ends["tuned"], k)) for k in _state_arrays(s0))
     return out, s0, ends["plain"]
 
 
@@ -839,7 +848,7 @@ def run_gpu_points(args, ws, rank, local, dist, dev):
                     "h2d_bytes_per_step": moved_bytes(prob, 12), "d2h_bytes_per_step": moved_bytes(prob, 12)},
         }
         if ws == 1 and not args.no_cpu:
-            secs, pc = cpu_points(prob, os.cpu_count() or 1)
+            secs, pc = cpu_points(start, os.cpu_count() or 1)
             line["cpu_baseline"] = {"value": POINTS_CPU / secs, "unit": "GP-updates/s",
                                     "cores": os.cpu_count() or 1, "kind": "port",
                                     "sample": f"one DSTRSS pass over the first {POINTS_CPU} points"}

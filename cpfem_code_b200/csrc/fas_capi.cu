@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <new>
 #include <vector>
@@ -85,6 +86,7 @@ struct HostCtl {                 // pinned mirror of the small device results
     int flags[4];                // 0 bad_bc, 1 tflag, 2 overflow, 3 nev
     SorCtl sor;
     double sums[8];
+    NrDev nr;                    // a graph-launched NRITER's outcome
 };
 
 }  // namespace
@@ -152,6 +154,14 @@ struct fas_handle {
     DVec<float> tblk32;
     DVec<TileSync> tsync;
     int tile_keep_rows = 0;      // rows per tile whose blocks stay in L2 across sweeps
+    // NRITER of an increment as one CUDA graph (FAS_MODE_GRAPH): loop state,
+    // report lines, the instantiated graph of each increment, and the two
+    // side streams its nested loop bodies are captured on
+    DVec<NrDev> nrdev;
+    DVec<fas_iter_report> nrrep;
+    std::map<int, cudaGraphExec_t> inc_graphs;
+    cudaStream_t cap2 = nullptr, cap3 = nullptr;
+    int64_t g_body_launches = 0, g_pass_launches = 0;   // per Newton iteration, per sweep pass
     int refine_every = 16;       // FP32 sweeps per FP64 residual
     cudaGraphExec_t sor_graph = nullptr;   // GRAPH_SWEEPS plain sweeps
     cudaGraphExec_t sor32_graph = nullptr; // one refinement cycle of the FP32 form
@@ -185,6 +195,9 @@ struct fas_handle {
     {
         if (sor_graph) cudaGraphExecDestroy(sor_graph);
         if (sor32_graph) cudaGraphExecDestroy(sor32_graph);
+        for (auto &g : inc_graphs) cudaGraphExecDestroy(g.second);
+        if (cap2) cudaStreamDestroy(cap2);
+        if (cap3) cudaStreamDestroy(cap3);
         for (auto e : ev_pool) cudaEventDestroy(e);
         if (ev_t0) cudaEventDestroy(ev_t0);
         if (ev_t1) cudaEventDestroy(ev_t1);
@@ -1652,8 +1665,274 @@ int nr_finish_impl(fas_handle *h, int inc)
     return 0;
 }
 
+// ---------------------------------------------------------------- graphed NRITER
+// Creates a condition in the graph that the stream `s` is capturing into.
+int make_condition(cudaStream_t s, unsigned default_value, bool assign_default, cudaGraphConditionalHandle *hc)
+{
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, nullptr, nullptr));
+    if (st != cudaStreamCaptureStatusActive || !g) return FAS_E_STATE;
+    CK(cudaGraphConditionalHandleCreate(hc, g, default_value, assign_default ? cudaGraphCondAssignDefault : 0));
+    return 0;
+}
+
+// Adds a conditional node (a while loop or an if) on condition `hc` at the
+// current end of the capture on `s`, and returns its body graph.
+int add_conditional(cudaStream_t s, cudaGraphConditionalHandle hc, cudaGraphConditionalNodeType type,
+                    cudaGraph_t *body)
+{
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    CK(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &ndeps));
+    if (st != cudaStreamCaptureStatusActive || !g) return FAS_E_STATE;
+    cudaGraphNodeParams prm = {};
+    prm.type = cudaGraphNodeTypeConditional;
+    prm.conditional.handle = hc;
+    prm.conditional.type = type;
+    prm.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps, ndeps, &prm));
+    CK(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    *body = prm.conditional.phGraph_out[0];
+    return 0;
+}
+
+// Captures what `issue` launches on h->stream into `body`, on the side
+// stream `side` (h->stream points at it meanwhile).
+template <typename F> int capture_into(fas_handle *h, cudaStream_t &side, cudaGraph_t body, F issue)
+{
+    std::swap(h->stream, side);
+    int rc = 0;
+    cudaError_t e = cudaStreamBeginCaptureToGraph(h->stream, body, nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        rc = issue();
+        cudaGraph_t done = nullptr;
+        const cudaError_t e2 = cudaStreamEndCapture(h->stream, &done);
+        if (e2 != cudaSuccess) e = e2;
+    }
+    std::swap(h->stream, side);
+    if (rc) return rc;
+    return e == cudaSuccess ? 0 : FAS_E_CUDA;
+}
+
+// One Newton iteration (nr_step_impl) with no host read: ELVALS + SUVALS,
+// FACSLS's prologue, the sweeps in a conditional node that runs only when
+// nothing failed so far (a while loop of GRAPH_SWEEPS sweeps per pass, or
+// the one-CTA solve under an if), the norms, the decision and the
+// correction.  Issued on h->stream while it captures the body of the
+// increment graph's Newton loop `hnr`.
+int capture_nr_body(fas_handle *h, int inc, cudaGraphConditionalHandle hnr)
+{
+    const size_t nd3 = 3 * (size_t)h->nnod;
+    const int ndof = (int)nd3;
+    const int64_t l0 = h->launches;
+    CK(cudaMemsetAsync(h->ekey.p, 0xFF, sizeof(unsigned long long), h->stream));
+    CK(cudaMemsetAsync(h->flags.p, 0, sizeof(int), h->stream));
+    int rc;
+    switch (h->ns_tmpl) {
+    case 12: rc = launch_elem<12>(h, inc, 0); break;
+    case 32: rc = launch_elem<32>(h, inc, 0); break;
+    default: {
+        const uint32_t m = h->mode;
+        h->mode &= ~FAS_MODE_CP_WARP;
+        rc = launch_elem<60>(h, inc, 0);
+        h->mode = m;
+    } break;
+    }
+    if (rc) return rc;
+    cudaStream_t s = h->stream;
+    {
+        const long long nthr = (long long)h->slots * h->nnod;
+        auto kern = h->nn == 20   ? k_assemble<20, 8>
+                    : h->nn == 10 ? k_assemble<10, 4>
+                    : h->nn == 15 ? k_assemble<15, 6>
+                                  : k_assemble<8, 1>;
+        kern<<<nblocks(nthr, 256), 256, 0, s>>>(
+            h->mesh(), h->block(), h->rec.p, h->x.p, h->dx.p, h->fc.p, h->ddx.p,
+            h->xspec.p + (size_t)(inc - 1) * std::max(h->nxs, 1) * 15,
+            h->fspec.p + (size_t)(inc - 1) * std::max(h->nfs, 1) * 3, h->nxs, h->nfs, h->C.efix, 1, h->flags.p);
+        LAUNCHED(h);
+    }
+    CK(cudaMemcpyAsync(h->rhs.p, h->ddx.p, nd3 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemsetAsync(h->ddx.p, 0, nd3 * sizeof(double), s));
+    CK(cudaMemsetAsync(h->ekey.p + 1, 0xFF, sizeof(unsigned long long), s));
+    CK(cudaMemsetAsync(h->sorctl.p, 0, sizeof(SorCtl), s));
+    const BlockDev B = h->block();
+    k_diag_check<<<nblocks(h->nnod, 256), 256, 0, s>>>(B, h->ekey.p + 1);
+    LAUNCHED(h);
+    const double tolerl = h->C.toler * h->C.toler;
+    const bool small = h->sor_small && !(h->mode & FAS_MODE_SOR_GRID);
+    if (!small && FAS_SOR_RCP) {
+        k_rdiag<<<nblocks(h->nnod, 256), 256, 0, s>>>(B, h->rdiag.p);
+        LAUNCHED(h);
+    }
+    // the FP32 solve (facsls_impl): cycles of refine_every sweeps on the
+    // FP32 copy, each closed by the fold and the FP64 residual
+    const bool fp32 = !small && (h->mode & FAS_MODE_SOR_FP32) && h->blk32.p;
+    const int m = h->refine_every, full = (1000 / m) * m, rest = 1000 - full;
+    if (fp32) {
+        CK(cudaMemcpyAsync(h->sor_r.p, h->rhs.p, nd3 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemsetAsync(h->sor_d.p, 0, nd3 * sizeof(double), s));
+    }
+    cudaGraphConditionalHandle hsor, hlast = 0;
+    if (int r = make_condition(s, 0, false, &hsor)) return r;
+    if (fp32)
+        if (int r = make_condition(s, 0, false, &hlast)) return r;
+    k_graph_sor_begin<<<1, 32, 0, s>>>(h->ekey.p, h->flags.p, hsor, hlast, fp32 ? 1 : 0);
+    LAUNCHED(h);
+    int ncolours = 0;
+    for (int c = 0; c < h->ncol; ++c) ncolours += h->col_start[c + 1] > h->col_start[c];
+    cudaGraph_t sbody = nullptr;
+    if (int r = add_conditional(s, hsor, small ? cudaGraphCondTypeIf : cudaGraphCondTypeWhile, &sbody)) return r;
+    rc = capture_into(h, h->cap3, sbody, [&]() -> int {
+        if (small) {
+            launch_sor_small(h, B, h->sorctl.p, tolerl);
+            LAUNCHED(h);
+            return 0;
+        }
+        if (fp32) {
+            launch_fp32_cycle(h, B, tolerl, m);
+            k_sor_cycle_cond<<<1, 32, 0, h->stream>>>(h->sorctl.p, full, rest, hsor, hlast);
+            h->g_pass_launches = (int64_t)m * (ncolours + 1) + 3;
+        } else {
+            for (int it = 0; it < GRAPH_SWEEPS; ++it) {
+                for (int c = 0; c < h->ncol; ++c) launch_colour(h, c, false);
+                launch_pdl(k_sor_check_cond, 1, 1024, 0, h->stream, h->part_sor.p, h->sor_nblk_tot,
+                           h->sorctl.p, tolerl, 1000, hsor);
+            }
+            h->g_pass_launches = (int64_t)GRAPH_SWEEPS * (ncolours + 1);
+        }
+        CK(cudaGetLastError());
+        return 0;
+    });
+    if (rc) return rc;
+    if (fp32 && rest > 0) {   // the shorter last cycle
+        cudaGraph_t lbody = nullptr;
+        if (int r = add_conditional(s, hlast, cudaGraphCondTypeIf, &lbody)) return r;
+        rc = capture_into(h, h->cap3, lbody, [&]() -> int {
+            launch_fp32_cycle(h, B, tolerl, rest);
+            CK(cudaGetLastError());
+            return 0;
+        });
+        if (rc) return rc;
+    }
+    k_nr_norms<<<h->nr_nblk, 256, 0, s>>>(h->nnod, h->ngps, h->ib.p, h->rhs.p, h->dx.p, h->ddx.p, h->erepmd.p,
+                                          h->part_nr.p, h->nr_nblk);
+    LAUNCHED(h);
+    k_final_sum<4><<<1, 1024, 0, s>>>(h->part_nr.p, h->nr_nblk, h->sums.p);
+    LAUNCHED(h);
+    k_nr_decide<<<1, 32, 0, s>>>(h->sums.p, h->ngps, h->ekey.p, h->flags.p, h->sorctl.p, h->C.toler, h->C.alpha,
+                                 h->C.maxit, tolerl, h->nrdev.p, h->nrrep.p, (int)h->nrrep.n, hnr);
+    LAUNCHED(h);
+    k_nr_update_dev<<<nblocks(ndof, 256), 256, 0, s>>>(ndof, h->nrdev.p, h->ddx.p, h->x.p, h->dx.p);
+    LAUNCHED(h);
+    h->g_body_launches = h->launches - l0;
+    return 0;
+}
+
+// The graph of NRITER for increment `inc`, built on first use and kept:
+// the loop state zeroed, a while node whose body is one Newton iteration,
+// and the cumslip tail.
+int ensure_inc_graph(fas_handle *h, int inc, cudaGraphExec_t *out)
+{
+    auto it = h->inc_graphs.find(inc);
+    if (it != h->inc_graphs.end()) {
+        *out = it->second;
+        return 0;
+    }
+    if (!h->cap2) CK(cudaStreamCreateWithFlags(&h->cap2, cudaStreamNonBlocking));
+    if (!h->cap3) CK(cudaStreamCreateWithFlags(&h->cap3, cudaStreamNonBlocking));
+    if (!h->nrdev.p) CKA(h->nrdev.alloc(1));
+    if (!h->nrrep.p) CKA(h->nrrep.alloc((size_t)std::max(h->C.maxit, 1)));
+    if (!h->cp_queue.p) CKA(h->cp_queue.alloc(1));
+    if (int rc = ensure_fp32(h)) return rc;
+    // the work-order buffers are sized outside the capture
+    if (h->nn != 8)
+        work_order(h, h->npg * h->nlmnt, h->gp_item.p);
+    else if (!(h->mode & FAS_MODE_CP_WARP))
+        work_order(h, h->nlmnt, h->gpe.p);
+    CK(cudaStreamSynchronize(h->stream));
+    const fas_profile P0 = h->P;
+    const int64_t L0 = h->launches;
+    const DevCtrl C0 = h->C;
+    h->C.nit_dev = &h->nrdev.p->nit;
+    cudaStream_t s = h->stream;
+    cudaGraph_t g = nullptr;
+    int rc = 0;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    if (cudaMemsetAsync(h->nrdev.p, 0, sizeof(NrDev), s) != cudaSuccess) rc = FAS_E_CUDA;
+    cudaGraphConditionalHandle hnr;
+    cudaGraph_t body = nullptr;
+    if (!rc) rc = make_condition(s, 1, true, &hnr);
+    if (!rc) rc = add_conditional(s, hnr, cudaGraphCondTypeWhile, &body);
+    if (!rc) rc = capture_into(h, h->cap2, body, [&]() { return capture_nr_body(h, inc, hnr); });
+    if (!rc) {
+        const int nsc = h->M.ns[h->last_mat - 1];
+        k_cumslip_dev<<<nblocks(h->ngps, 256), 256, 0, s>>>(h->gp(), nsc, h->h_tiem[inc - 1], h->nrdev.p);
+    }
+    const cudaError_t e = cudaStreamEndCapture(s, &g);
+    h->C = C0;
+    h->P = P0;
+    h->launches = L0;
+    if (rc || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return rc ? rc : FAS_E_CUDA;
+    }
+    cudaGraphExec_t ge = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    CK(ei);
+    h->inc_graphs[inc] = ge;
+    *out = ge;
+    return 0;
+}
+
+// NRITER of increment `inc` as one graph launch and one host read: the
+// report lines, the iteration count and the first error come back together.
+int nriter_graph_impl(fas_handle *h, int inc, fas_iter_report *rep, int cap, int *n_rep)
+{
+    cudaGraphExec_t ge;
+    if (int rc = ensure_inc_graph(h, inc, &ge)) return rc;
+    cudaStream_t s = h->stream;
+    CK(cudaGraphLaunch(ge, s));
+    CK(cudaMemcpyAsync(&h->hc->nr, h->nrdev.p, sizeof(NrDev), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const NrDev nr = h->hc->nr;
+    const int n = std::min(nr.nit - (nr.status ? 1 : 0), (int)h->nrrep.n);
+    std::vector<fas_iter_report> r(std::max(n, 1));
+    if (n > 0) CK(cudaMemcpy(r.data(), h->nrrep.p, n * sizeof(fas_iter_report), cudaMemcpyDeviceToHost));
+    if (n_rep) *n_rep = nr.nit;
+    if (rep)
+        for (int k = 0; k < std::min(n, cap); ++k) rep[k] = r[k];
+    // the counters of the iterations the graph ran
+    const bool small = h->sor_small && !(h->mode & FAS_MODE_SOR_GRID);
+    const bool fp32 = !small && (h->mode & FAS_MODE_SOR_FP32) && h->blk32.p;
+    const int per_pass = fp32 ? h->refine_every : GRAPH_SWEEPS;
+    double bytes = 0.0;
+    for (double b : fp32 ? h->col_bytes32 : h->col_bytes) bytes += b;
+    h->launches += 1 + (int64_t)nr.nit * h->g_body_launches;   // cumslip, and every iteration's body
+    for (int k = 0; k < n; ++k) {
+        const int sw = r[k].sor_sweeps;
+        h->P.n_constitutive++;
+        h->P.gp_updates += h->ngps;
+        h->P.n_assembly++;
+        h->P.assembly_bytes += h->asm_bytes;
+        h->P.sor_sweeps += sw;
+        h->P.sor_bytes += bytes * sw;
+        h->P.n_sor_colour += small ? 1 : (int64_t)sw * h->ncol;
+        if (!small) h->launches += (int64_t)((sw + per_pass - 1) / per_pass) * h->g_pass_launches;
+    }
+    return nr.status;
+}
+
 int nriter_impl(fas_handle *h, int inc, fas_iter_report *rep, int cap, int *n_rep)
 {
+    if ((h->mode & FAS_MODE_GRAPH) && !(h->mode & FAS_MODE_SOR_TILES) && h->prof < 2)
+        return nriter_graph_impl(h, inc, rep, cap, n_rep);
     int nit = 0;
     bool l_conv = true;
     while (l_conv) {
@@ -1850,6 +2129,9 @@ int32_t fas_gpu_set_mode(fas_handle *h, uint32_t mode)
     if (!h) return FAS_E_ARG;
     h->mode = mode;
     h->C.tangent = (mode & FAS_MODE_TANGENT_CONSISTENT) ? 1 : 0;
+    // increment graphs hold the launches of the old mode
+    for (auto &g : h->inc_graphs) cudaGraphExecDestroy(g.second);
+    h->inc_graphs.clear();
     return 0;
 }
 

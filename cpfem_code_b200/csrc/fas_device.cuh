@@ -38,6 +38,8 @@ struct DevCtrl {
     int maxit;
     int tangent;                // 1: consistent tangent at the converged stress
     unsigned long long seed;
+    const int *nit_dev;         // set in a graph-launched NRITER: the Newton
+                                // iteration number is *nit_dev + 1
 };
 
 // Gauss-point state, structure of arrays: field[k * ngps + g].

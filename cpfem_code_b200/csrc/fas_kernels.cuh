@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(128) k_elem(MeshDev Mh, DevMat M, DevCtrl C, D
             ds[k] = G.ds[k * ng + g];
         }
         GpOut o;
-        rc = dstrss<NS>(M, C, G, g, Mh.le[e], del, r, st, ds, dt, inc, nit, o);
+        rc = dstrss<NS>(M, C, G, g, Mh.le[e], del, r, st, ds, dt, inc, C.nit_dev ? *C.nit_dev + 1 : nit, o);
         if (rc) {
             atomicMin(errkey, ((unsigned long long)e << 16) | (unsigned long long)rc);
             return;
@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(128) k_elemq(MeshDev Mh, DevMat M, DevCtrl C, 
             ds[k] = G.ds[k * ng + g];
         }
         GpOut o;
-        rc = dstrss<NS>(M, C, G, g, Mh.le[e], del, r, st, ds, dt, inc, nit, o);
+        rc = dstrss<NS>(M, C, G, g, Mh.le[e], del, r, st, ds, dt, inc, C.nit_dev ? *C.nit_dev + 1 : nit, o);
         if (rc) {
             atomicMin(errkey, key | (unsigned long long)rc);
             return;
@@ -423,7 +423,8 @@ __global__ void __launch_bounds__(128) k_elem_wc(MeshDev Mh, DevMat M, DevCtrl C
         ds[k] = G.ds[k * ng + g];
     }
     wc::GpOutW o;
-    const int rc = wc::dstrss_wc<NA>(M, C, G, g, Mh.le[e], del, r, st, ds, dt, inc, nit, o);
+    const int rc = wc::dstrss_wc<NA>(M, C, G, g, Mh.le[e], del, r, st, ds, dt, inc,
+                                     C.nit_dev ? *C.nit_dev + 1 : nit, o);
     if (rc) {
         if (lane == 0) atomicMin(errkey, ((unsigned long long)e << 16) | (unsigned long long)rc);
         return;
@@ -1595,6 +1596,124 @@ __global__ void k_nr_update(int ndof, double alp2, const double *ddx, double *x,
     const double xc = alp2 * ddx[i];
     x[i] = x[i] - xc;
     dx[i] = dx[i] - xc;
+}
+
+// ---------------------------------------------------------------- graph-launched NRITER
+// State of NRITER's loop when a whole increment runs as one CUDA graph
+// (FAS_MODE_GRAPH): the loop and the SOR sweeps inside it are conditional
+// while nodes whose conditions these kernels set on the device.
+struct NrDev {
+    int nit;        // Newton iterations done in this increment
+    int status;     // 0, or the first error: a FAFERR code or FAS_E_* < 0
+    double alp2;    // damping factor of the iteration just finished (0 after an error)
+};
+
+// Before the sweeps of a Newton iteration: sweep only when nothing has
+// failed so far in it (an element's FAFERR code, a bad boundary code, a
+// zero diagonal -- Stif_sol.f90:183-185 -- stop the reference before FACSLS).
+// `hlast` (when `has_last`), the condition of the FP32 solve's shorter
+// last cycle, starts cleared.
+__global__ void k_graph_sor_begin(const unsigned long long *ekey, const int *flags,
+                                  cudaGraphConditionalHandle hsor, cudaGraphConditionalHandle hlast,
+                                  int has_last)
+{
+    if (threadIdx.x == 0) {
+        cudaGraphSetConditional(hsor, (ekey[0] == ~0ull && ekey[1] == ~0ull && flags[0] == 0) ? 1u : 0u);
+        if (has_last) cudaGraphSetConditional(hlast, 0u);
+    }
+}
+
+// After a cycle of the FP32 solve (m sweeps, fold, FP64 residual): another
+// full cycle while not converged, no wait gave up and fewer than `full`
+// (the largest multiple of m within 1000) sweeps are done; the shorter
+// last cycle of the remaining sweeps when exactly `full` are done and
+// some remain.
+__global__ void k_sor_cycle_cond(const SorCtl *ctl, int full, int rest, cudaGraphConditionalHandle hsor,
+                                 cudaGraphConditionalHandle hlast)
+{
+    if (threadIdx.x != 0) return;
+    const volatile SorCtl *c = ctl;
+    const bool go = !c->conv && !c->fault;
+    cudaGraphSetConditional(hsor, (go && c->sweeps < full) ? 1u : 0u);
+    cudaGraphSetConditional(hlast, (go && c->sweeps == full && rest > 0) ? 1u : 0u);
+}
+
+// The stopping test of one sweep (k_sor_check) that also sets the sweep
+// loop's condition: another four sweeps while not converged, below maxitl
+// sweeps and no bounded wait gave up.
+__global__ void __launch_bounds__(1024) k_sor_check_cond(const double *part, int nblk, SorCtl *ctl, double tolerl,
+                                                         int maxitl, cudaGraphConditionalHandle hsor)
+{
+    pdl_launch_dependents();
+    pdl_wait();
+    if (!ctl->conv) sweep_test(part, nblk, ctl, tolerl);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const volatile SorCtl *c = ctl;
+        cudaGraphSetConditional(hsor, (!c->conv && c->sweeps < maxitl && !c->fault) ? 1u : 0u);
+    }
+}
+
+// The end of NRITER's loop body (Stif_sol.f90:46-75) on the device: the
+// norms' sfc, errdx, erddx, sdx and the damping factor alp2, the report line
+// of the iteration, the first error of the iteration (element key, boundary
+// codes, zero diagonal, SOR fault or 904), and the loop's condition:
+// another pass while sdx >= toler and nit < maxit and nothing failed.
+__global__ void k_nr_decide(const double *sums, int ngps, const unsigned long long *ekey, const int *flags,
+                            const SorCtl *ctl, double toler, double alpha, int maxit, double tolerl,
+                            NrDev *nr, fas_iter_report *rep, int cap, cudaGraphConditionalHandle hnr)
+{
+    if (threadIdx.x != 0) return;
+    const int nit = nr->nit + 1;
+    int status = 0;
+    if (ekey[0] != ~0ull)
+        status = (int)(ekey[0] & 0xFFFFull);
+    else if (flags[0])
+        status = FAS_E_ARG;
+    else if (ekey[1] != ~0ull)
+        status = 903;
+    else if (ctl->fault)
+        status = FAS_E_TIMEOUT;
+    else if (ctl->err > 10.0 * tolerl)
+        status = 904;
+    const double sfc = sqrt(sums[0]), errdx = sqrt(sums[1]), erddx = sqrt(sums[2]);
+    const double sdx = errdx == 0.0 ? toler : erddx / errdx;
+    // rounded like the host's 1 / (1 + alpha sdx): no fused multiply-add
+    const double alp2 = 1.0 / __dadd_rn(1.0, __dmul_rn(alpha, sdx));
+    if (nit <= cap && status == 0) {
+        fas_iter_report &r = rep[nit - 1];
+        r.nit = nit;
+        r.sor_sweeps = ctl->sweeps;
+        r.sdx = sdx;
+        r.sfc = sfc;
+        r.cp_err = sums[3] / (double)ngps;
+        r.alp2 = alp2;
+        r.sor_error = ctl->err;
+    }
+    nr->nit = nit;
+    nr->status = status;
+    nr->alp2 = status ? 0.0 : alp2;
+    cudaGraphSetConditional(hnr, (status == 0 && sdx >= toler && nit < maxit) ? 1u : 0u);
+}
+
+// NRITER's correction x, dx -= alp2 ddx with the device's alp2 (none after
+// an error: the reference stops before it).
+__global__ void k_nr_update_dev(int ndof, const NrDev *nr, const double *ddx, double *x, double *dx)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ndof || nr->status) return;
+    const double xc = nr->alp2 * ddx[i];
+    x[i] = x[i] - xc;
+    dx[i] = dx[i] - xc;
+}
+
+// NRITER's cumslip tail, skipped after an error.
+__global__ void k_cumslip_dev(DevGp G, int nsc, double tm, const NrDev *nr)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G.ngps || nr->status) return;
+    for (int k = 0; k < nsc; ++k)
+        G.cumslip[k * G.ngps + g] = G.cumslip[k * G.ngps + g] + (G.srate[k * G.ngps + g] * tm);
 }
 
 // UPDATE_NODE (src/fasolt/Fasolt3.f90:231-244)

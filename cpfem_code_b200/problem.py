@@ -111,6 +111,28 @@ class Problem:
     def copy(self) -> "Problem":
         return copy.deepcopy(self)
 
+    def first_points(self, n: int) -> "Problem":
+        """The first n points of a mesh-free point batch (nlmnt == 0), with
+        their state, as a batch of their own."""
+        if self.nlmnt != 0:
+            raise ValueError("first_points needs a mesh-free point batch")
+        n = min(int(n), self.ngps)
+        out = copy.copy(self)
+        out.ngps = n
+        out.le = self.le[:n].copy()
+        out.meta = dict(self.meta)
+        for name in ("eps", "dep", "st", "ep", "ds", "de", "rt", "dr", "sv", "dsv",
+                     "timestwinned", "twinsys", "srate", "cumslip"):
+            a = getattr(self, name)
+            if a is not None:
+                setattr(out, name, a[:n].copy())
+        for name in ("e", "ssang", "ab", "an", "ampar", "smatrx", "nss", "tiem", "x_spec", "f_spec",
+                     "x", "dx", "fc", "ddx"):
+            a = getattr(self, name)
+            if a is not None:
+                setattr(out, name, a.copy())
+        return out
+
     # ------------------------------------------------------------ descriptors
     def descriptors(self):
         """(mesh, matl, ctrl) ctypes descriptors pointing into this object."""

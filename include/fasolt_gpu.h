@@ -84,6 +84,23 @@ extern "C" {
                                      their neighbour tiles have finished the
                                      previous one (8-node bricks; other
                                      meshes keep one launch per colour)     */
+#define FAS_MODE_GRAPH      128u  /* fas_gpu_nriter as one CUDA graph per
+                                     increment: the Newton loop and the SOR
+                                     loop are conditional while nodes whose
+                                     conditions the device sets (sdx >=
+                                     toler and nit < maxit; not converged
+                                     and below 1000 sweeps), so the
+                                     increment runs with one launch and one
+                                     host read.  Same arithmetic and launch
+                                     shapes as the host-driven loop, so the
+                                     same results to the bit; combines with
+                                     FAS_MODE_SOR_FP32 (cycles of sweeps,
+                                     fold and residual as the loop body).
+                                     With FAS_MODE_SOR_TILES, and while
+                                     profiling with prof >= 2, the host loop
+                                     runs.  The graph of an increment is
+                                     built on its first call and kept until
+                                     the mode changes                       */
 
 /*
  * Mesh: the FAS_COM element and node tables.

@@ -119,4 +119,4 @@ def test_fp32_sor_refinement_20_node():
     o.download()
     per_point = np.abs(pg.st - po.st).max() / np.abs(po.st).max()
     macro = abs(pg.st[:, 0].mean() - po.st[:, 0].mean()) / abs(po.st[:, 0].mean())
-    assert per_point < 1e-4 and macro < 1e-5
+    assert per_point < 1e-5 and macro < 1e-6
