@@ -902,7 +902,7 @@ def run_case(args) -> int:
                  "tiles": abi.FAS_MODE_SOR_GRID | abi.FAS_MODE_SOR_TILES,
                  "tiles_fp32": abi.FAS_MODE_SOR_GRID | abi.FAS_MODE_SOR_TILES | abi.FAS_MODE_SOR_FP32,
                  "colour_fp32": abi.FAS_MODE_SOR_GRID | abi.FAS_MODE_SOR_FP32}
-        for n in (2, 4, 8, 12, 16, 20, 24, 32, 48):
+        for n in (2, 4, 8, 12, 16, 20, 24, 32, 40, 48, 64):
             p = generator.cube_config(n=n, ninc=1, grain=1, seed=n)
             row = {"n": n, "nodes": p.nnod}
             for tag, mode in paths.items():

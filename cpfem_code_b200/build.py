@@ -18,7 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "lib", "libfasgpu.so")
 SOURCES = ["fas_capi.cu"]
-DEPS = ["fas_capi.cu", "fas_kernels.cuh", "fas_sor_tiles.cuh", "fas_adjoint.cuh", "fas_device.cuh", "fas_flops.h", "fas_rng.h"]
+DEPS = ["fas_capi.cu", "fas_kernels.cuh", "fas_sor_tiles.cuh", "fas_device_warp.cuh", "fas_adjoint.cuh", "fas_device.cuh", "fas_flops.h", "fas_rng.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 TUNED = os.path.join(HERE, "tuned.json")
 
