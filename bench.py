@@ -430,9 +430,6 @@ def run_increments(g, prob, start, ninc_warm: int, ninc_timed: int):
     legs = [("plain", abi.FAS_MODE_PLAIN), ("tuned", TUNED_MODE),
             ("plain_consistent_tangent", abi.FAS_MODE_TANGENT_CONSISTENT),
             ("plain_graph", abi.FAS_MODE_GRAPH), ("tuned_graph", TUNED_MODE | abi.FAS_MODE_GRAPH)]
-    if WORKLOAD == "mixed32":
-        # the persistent phase-sorted queue for the constitutive passes
-        legs.append(("plain_cp_queue", abi.FAS_MODE_CP_QUEUE))
     for tag, mode in legs:
         t = s0.copy()
         g.upload(t)

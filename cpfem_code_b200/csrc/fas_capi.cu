@@ -173,6 +173,7 @@ struct fas_handle {
     bool sor_small = false;      // whole solve in one CTA (small meshes)
     int sor_nblk_tot = 0, sor_nblk_tot32 = 0, nr_nblk = 0;
     DVec<double> part_sor, part_nr, sums;
+    bool mixed_phases = false;   // GPs of materials with different slip-system counts
     DVec<unsigned long long> ekey;
     DVec<int> flags;
     DVec<SorCtl> sorctl;
@@ -892,10 +893,14 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
         }
         h->M.amax[m] = amx;
     }
+    int ns_used = 0;   // the slip-system count shared by every GP's material, or -1
     for (int g = 0; g < h->ngps; ++g) {
         const int mc = std::abs(h->h_gp_iel[g]);
         if (mc < 1 || mc > nm) return FAS_E_ARG;
+        const int ns = h->M.ns[mc - 1];
+        ns_used = ns_used == 0 ? ns : (ns_used == ns ? ns : -1);
     }
+    h->mixed_phases = ns_used < 0;
     h->ns_tmpl = h->maxns <= 12 ? 12 : (h->maxns <= 32 ? 32 : 60);
     h->nsvld = 3 + h->maxns;
     CKA(h->m_e.alloc(e.size()));
@@ -1122,14 +1127,15 @@ const int *work_order(fas_handle *h, int n, const int *gp_of)
 }
 
 // Grid of a constitutive pass over n items (for_each_item).  With the
-// queue (FAS_MODE_CP_QUEUE, or built in with FAS_CP_QUEUE=1): as many
+// queue (FAS_MODE_CP_QUEUE, meshes whose GPs' materials differ in their
+// slip-system counts, or built in with FAS_CP_QUEUE=1): as many
 // 128-thread CTAs as reside at once, at most one item per thread, and the
 // queue head zeroed; otherwise one thread per item.
 template <typename K> unsigned cp_grid(fas_handle *h, K kern, long long n, int **queue)
 {
     *queue = nullptr;
     const unsigned full = nblocks(n, 128);
-    if (!FAS_CP_QUEUE && !(h->mode & FAS_MODE_CP_QUEUE)) return full;
+    if (!FAS_CP_QUEUE && !(h->mode & FAS_MODE_CP_QUEUE) && !h->mixed_phases) return full;
     int occ = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 128, 0) != cudaSuccess || occ < 1) return full;
     if (!h->cp_queue.p && h->cp_queue.alloc(1) != cudaSuccess) return full;

@@ -77,7 +77,10 @@ extern "C" {
                                      whose warps take the next 32 GPs of the
                                      work-sorted (heaviest first) order from
                                      a device queue, instead of one thread
-                                     per GP in that order                   */
+                                     per GP in that order.  Meshes whose GPs'
+                                     materials differ in their slip-system
+                                     counts (mixed FCC/HCP) take the queue
+                                     without the flag                       */
 #define FAS_MODE_SOR_TILES   16u  /* grid-wide SOR as one persistent launch
                                      per solve: spatial tiles of rows, one
                                      per SM, that start each colour once
