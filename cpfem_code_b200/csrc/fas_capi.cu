@@ -174,6 +174,7 @@ struct fas_handle {
     int sor_nblk_tot = 0, sor_nblk_tot32 = 0, nr_nblk = 0;
     DVec<double> part_sor, part_nr, sums;
     bool mixed_phases = false;   // GPs of materials with different slip-system counts
+    size_t stage_bytes = 0;      // shared memory of the constitutive kernels' table copy
     DVec<unsigned long long> ekey;
     DVec<int> flags;
     DVec<SorCtl> sorctl;
@@ -870,6 +871,8 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
         sm((size_t)nm * MAXSS * MAXSS, 0.0);
     h->M = DevMat{};
     h->M.nmatl = nm;
+    h->M.tld = MAXSS;
+    h->M.sld = MAXSS * MAXSS;
     for (int m = 0; m < nm; ++m) {
         const int ns = T->nss[m];
         if (ns < 1 || ns > L) return FAS_E_ARG;
@@ -902,6 +905,12 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
     }
     h->mixed_phases = ns_used < 0;
     h->ns_tmpl = h->maxns <= 12 ? 12 : (h->maxns <= 32 ? 32 : 60);
+    // tables in shared memory (FAS_SMEM_TABLES builds) when they fit the
+    // default 48 KB of a launch
+    if (FAS_SMEM_TABLES && staged_doubles(nm, h->maxns) * 8 <= 48 * 1024) {
+        h->M.stage_t = h->maxns;
+        h->stage_bytes = (size_t)staged_doubles(nm, h->maxns) * 8;
+    }
     h->nsvld = 3 + h->maxns;
     CKA(h->m_e.alloc(e.size()));
     CKA(h->m_ssang.alloc(ssang.size()));
@@ -1137,7 +1146,8 @@ template <typename K> unsigned cp_grid(fas_handle *h, K kern, long long n, int *
     const unsigned full = nblocks(n, 128);
     if (!FAS_CP_QUEUE && !(h->mode & FAS_MODE_CP_QUEUE) && !h->mixed_phases) return full;
     int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 128, 0) != cudaSuccess || occ < 1) return full;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 128, h->stage_bytes) != cudaSuccess || occ < 1)
+        return full;
     if (!h->cp_queue.p && h->cp_queue.alloc(1) != cudaSuccess) return full;
     if (cudaMemsetAsync(h->cp_queue.p, 0, sizeof(int), h->stream) != cudaSuccess) return full;
     *queue = h->cp_queue.p;
@@ -1153,7 +1163,7 @@ template <int NS> int launch_elem(fas_handle *h, int inc, int nit)
             const int *order = work_order(h, (int)nit_items, h->gp_item.p);
             int *queue = nullptr;
             const unsigned grid = cp_grid(h, kern, nit_items, &queue);
-            kern<<<grid, 128, 0, h->stream>>>(h->mesh(), h->M, h->C, h->gp(), h->dnq.p, h->wfac, h->x.p, h->dx.p,
+            kern<<<grid, 128, h->stage_bytes, h->stream>>>(h->mesh(), h->M, h->C, h->gp(), h->dnq.p, h->wfac, h->x.p, h->dx.p,
                                               h->rec.p, h->h_tiem[inc - 1], inc, nit, h->ekey.p, order, queue);
         };
         if (h->nn == 20)
@@ -1167,7 +1177,7 @@ template <int NS> int launch_elem(fas_handle *h, int inc, int nit)
         const int *order = work_order(h, h->nlmnt, h->gpe.p);
         int *queue = nullptr;
         const unsigned grid = cp_grid(h, k_elem<NS>, h->nlmnt, &queue);
-        k_elem<NS><<<grid, 128, 0, h->stream>>>(
+        k_elem<NS><<<grid, 128, h->stage_bytes, h->stream>>>(
             h->mesh(), h->M, h->C, h->gp(), h->x.p, h->dx.p, h->rec.p, h->h_tiem[inc - 1], inc, nit, h->ekey.p,
             order, queue);
     }
@@ -2314,7 +2324,7 @@ int32_t fas_gpu_constitutive(fas_handle *h, int32_t inc, int32_t nit)
         if (thr) {
             int *queue = nullptr;
             const unsigned grid = cp_grid(h, k_points<12>, h->ngps, &queue);
-            k_points<12><<<grid, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order, queue);
+            k_points<12><<<grid, 128, h->stage_bytes, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order, queue);
         }
         else k_points_wc<12><<<nbw, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p);
         break;
@@ -2322,14 +2332,14 @@ int32_t fas_gpu_constitutive(fas_handle *h, int32_t inc, int32_t nit)
         if (thr) {
             int *queue = nullptr;
             const unsigned grid = cp_grid(h, k_points<32>, h->ngps, &queue);
-            k_points<32><<<grid, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order, queue);
+            k_points<32><<<grid, 128, h->stage_bytes, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order, queue);
         }
         else k_points_wc<32><<<nbw, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p);
         break;
     default: {
         int *queue = nullptr;
         const unsigned grid = cp_grid(h, k_points<60>, h->ngps, &queue);
-        k_points<60><<<grid, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order, queue);
+        k_points<60><<<grid, 128, h->stage_bytes, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order, queue);
         break;
     }
     }

@@ -31,6 +31,11 @@ struct DevMat {
     const double *sm;           // [nmatl][60*60], sm[i*ns+j] = smatrx(i,j)
     int twinlim;
     double twinprob;
+    int tld, sld;               // per-material strides: systems of the per-system tables
+                                // (MAXSS) and entries of sm (MAXSS^2); smaller in a
+                                // shared-memory copy (stage_tables)
+    int stage_t;                // > 0: constitutive kernels copy the tables into shared
+                                // memory at this system stride (FAS_SMEM_TABLES builds)
 };
 
 struct DevCtrl {
@@ -52,7 +57,51 @@ struct DevGp {
     double *erepmd, *ops;
 };
 
+#ifndef FAS_SMEM_TABLES
+#define FAS_SMEM_TABLES 0
+#endif
+#if FAS_SMEM_TABLES
+// the tables may sit in shared memory: a generic load
+__device__ __forceinline__ double ld_ro(const double *p) { return *p; }
+#else
 __device__ __forceinline__ double ld_ro(const double *p) { return __ldg(p); }
+#endif
+
+// Doubles of the shared-memory copy of nmatl materials' tables at a stride
+// of t systems: e, ssang, ab, an, ampar and sm.
+__host__ __device__ inline int staged_doubles(int nmatl, int t) { return nmatl * (9 + t * (13 + t)); }
+
+// Copies the tables into shared memory (every thread of the CTA takes part;
+// call before any thread leaves) and returns M with its pointers and strides
+// on the copy.
+__device__ __forceinline__ DevMat stage_tables(const DevMat &M, double *s)
+{
+    const int nm = M.nmatl, t = M.stage_t;
+    double *e = s, *ss = e + 9 * nm, *ab = ss + nm * t, *an = ab + 3 * nm * t, *amp = an + 3 * nm * t,
+           *sm = amp + 6 * nm * t;
+    for (int i = threadIdx.x; i < 9 * nm; i += blockDim.x) e[i] = M.e[i];
+    for (int i = threadIdx.x; i < nm * t; i += blockDim.x) ss[i] = M.ssang[(i / t) * MAXSS + i % t];
+    for (int i = threadIdx.x; i < 3 * nm * t; i += blockDim.x) {
+        const int m = i / (3 * t), r = i % (3 * t);
+        ab[i] = M.ab[(size_t)m * MAXSS * 3 + r];
+        an[i] = M.an[(size_t)m * MAXSS * 3 + r];
+    }
+    for (int i = threadIdx.x; i < 6 * nm * t; i += blockDim.x)
+        amp[i] = M.ampar[(size_t)(i / (6 * t)) * MAXSS * 6 + i % (6 * t)];
+    for (int i = threadIdx.x; i < nm * t * t; i += blockDim.x)
+        sm[i] = M.sm[(size_t)(i / (t * t)) * MAXSS * MAXSS + i % (t * t)];
+    __syncthreads();
+    DevMat S = M;
+    S.e = e;
+    S.ssang = ss;
+    S.ab = ab;
+    S.an = an;
+    S.ampar = amp;
+    S.sm = sm;
+    S.tld = t;
+    S.sld = t * t;
+    return S;
+}
 
 // FJ2VOM, src/fasolt/Sig_eps.f90:217-241
 __device__ __forceinline__ double fj2vom(bool stress, const double *x)
@@ -371,8 +420,8 @@ template <int NS> struct CpScratch {
 template <int NS>
 __device__ __forceinline__ void btmatrx(const DevMat &M, const double a[3][3], CpScratch<NS> &w)
 {
-    const double *ab = M.ab + (size_t)w.mc * MAXSS * 3;
-    const double *an = M.an + (size_t)w.mc * MAXSS * 3;
+    const double *ab = M.ab + (size_t)w.mc * M.tld * 3;
+    const double *an = M.an + (size_t)w.mc * M.tld * 3;
     for (int i = 0; i < w.ns; ++i) {
         double d0 = ld_ro(ab + 3 * i), d1 = ld_ro(ab + 3 * i + 1), d2 = ld_ro(ab + 3 * i + 2);
         double n0 = ld_ro(an + 3 * i), n1 = ld_ro(an + 3 * i + 1), n2 = ld_ro(an + 3 * i + 2);
@@ -411,8 +460,8 @@ template <int NS>
 __device__ __noinline__ void plastc(const DevMat &M, CpScratch<NS> &w, double dt)
 {
     const int ns = w.ns;
-    const double *amp = M.ampar + (size_t)w.mc * MAXSS * 6;
-    const double *sm = M.sm + (size_t)w.mc * MAXSS * MAXSS;
+    const double *amp = M.ampar + (size_t)w.mc * M.tld * 6;
+    const double *sm = M.sm + (size_t)w.mc * M.sld;
     double sumss = 0.0;
     for (int i = 0; i < ns; ++i) sumss = sumss + fabs(w.gam[i]);
     double gradh[NS];
@@ -448,8 +497,8 @@ __device__ __forceinline__ void slpini(const DevMat &M, CpScratch<NS> &w, const 
                                        const DevCtrl &C, int g, double dt, int inc, int nit,
                                        int cpit, int &twinsys, int timestwinned)
 {
-    const double *amp = M.ampar + (size_t)w.mc * MAXSS * 6;
-    const double *ssang = M.ssang + (size_t)w.mc * MAXSS;
+    const double *amp = M.ampar + (size_t)w.mc * M.tld * 6;
+    const double *ssang = M.ssang + (size_t)w.mc * M.tld;
     double gammax = 0.0;
     for (int i = 0; i < w.ns; ++i) {
         w.am[i] = ld_ro(amp + 6 * i);

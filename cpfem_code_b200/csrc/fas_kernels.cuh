@@ -117,6 +117,10 @@ __global__ void __launch_bounds__(128) k_elem(MeshDev Mh, DevMat M, DevCtrl C, D
                                               unsigned long long *errkey, const int *__restrict__ order,
                                               int *queue)
 {
+#if FAS_SMEM_TABLES
+    extern __shared__ double s_tables[];
+    if (M.stage_t > 0) M = stage_tables(M, s_tables);
+#endif
     for_each_item(Mh.nlmnt, order, queue, [&](int e) {
         if (Mh.lt[e] < 9) return;   // tie element: no Gauss point
         const int ne = Mh.nlmnt;
@@ -199,6 +203,10 @@ __global__ void __launch_bounds__(128) k_elemq(MeshDev Mh, DevMat M, DevCtrl C, 
                                                unsigned long long *errkey, const int *__restrict__ order,
                                                int *queue)
 {
+#if FAS_SMEM_TABLES
+    extern __shared__ double s_tables[];
+    if (M.stage_t > 0) M = stage_tables(M, s_tables);
+#endif
     using L = RecLayout<NN>;
     for_each_item(NPG * Mh.nlmnt, order, queue, [&](int t) {   // item e*NPG + gq
         const int e = t / NPG, gq = t - e * NPG;
@@ -337,6 +345,10 @@ __global__ void __launch_bounds__(128) k_points(DevMat M, DevCtrl C, DevGp G, co
                                                 unsigned long long *errkey, const int *__restrict__ order,
                                                 int *queue)
 {
+#if FAS_SMEM_TABLES
+    extern __shared__ double s_tables[];
+    if (M.stage_t > 0) M = stage_tables(M, s_tables);
+#endif
     for_each_item(G.ngps, order, queue, [&](int g) {
         const int ng = G.ngps;
         double de[6], r[3], st[6], ds[6];
