@@ -48,7 +48,8 @@ CASES = [((4, 4, 4), abi.FAS_MODE_PLAIN, 8),      # one-CTA solve
          ((8, 8, 8), abi.FAS_MODE_SOR_GRID, 8),   # colour kernels forced
          ((3, 3, 3), abi.FAS_MODE_PLAIN, 20),     # 81-slot rows, one CTA
          ((3, 3, 3), abi.FAS_MODE_SOR_GRID, 20),  # 81-slot colour kernels
-         ((12, 12, 12), abi.FAS_MODE_PLAIN, 20)]  # 81-slot colour kernels, 8,281 nodes
+         ((12, 12, 12), abi.FAS_MODE_PLAIN, 20),  # 81-slot colour kernels, 8,281 nodes
+         ((32, 32, 32), abi.FAS_MODE_PLAIN, 20)]  # the brick20_32 workload: the most partials benchmarked
 
 
 @pytest.mark.parametrize("n,mode,nodes", CASES)
