@@ -2084,12 +2084,24 @@ int replay_prepare(fas_handle *h, const fas_replay_desc *d, bool grad, ReplayDev
     return 0;
 }
 
+// CTA size of the replay kernels: 128 threads, halved (down to one warp)
+// while that leaves fewer than two CTAs per SM, so that a small GP count
+// still spreads its long serial threads over every SM.  Each GP is
+// independent, so the size changes no result.
+int replay_block(const fas_handle *h)
+{
+    int bs = 128;
+    while (bs > 32 && (long long)h->ngps < 2LL * h->nsm * bs) bs >>= 1;
+    return bs;
+}
+
 // The forward sweep; with rs > 0 it also records the last segment for
 // the reverse sweep.
 template <int NS>
 void launch_replay_fwd(fas_handle *h, const ReplayDev &H, const DevGp &G, int rs)
 {
-    k_replay_fwd<NS><<<nblocks(h->ngps, 128), 128, 0, h->stream>>>(h->M, h->C, G, h->gp_iel.p, h->st.p, H,
+    const int bs = replay_block(h);
+    k_replay_fwd<NS><<<nblocks(h->ngps, bs), bs, 0, h->stream>>>(h->M, h->C, G, h->gp_iel.p, h->st.p, H,
                                                                   h->rp.chk.p, rs > 0 ? h->rp.rec.p : nullptr,
                                                                   rs, h->rp.jg.p, h->rp.eq.p, h->ekey.p);
 }
@@ -2097,7 +2109,8 @@ void launch_replay_fwd(fas_handle *h, const ReplayDev &H, const DevGp &G, int rs
 template <int NS>
 void launch_replay_adj(fas_handle *h, const ReplayDev &H, const DevGp &G, int rs)
 {
-    k_replay_adj<NS><<<nblocks(h->ngps, 128), 128, 0, h->stream>>>(h->M, h->C, G, h->gp_iel.p, H, h->rp.chk.p,
+    const int bs = replay_block(h);
+    k_replay_adj<NS><<<nblocks(h->ngps, bs), bs, 0, h->stream>>>(h->M, h->C, G, h->gp_iel.p, H, h->rp.chk.p,
                                                                   h->rp.rec.p, rs, h->rp.jg.p, h->rp.gst.p,
                                                                   h->rp.gsv.p, h->rp.gp.p, h->ekey.p);
 }
