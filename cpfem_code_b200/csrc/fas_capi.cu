@@ -1140,13 +1140,25 @@ const int *work_order(fas_handle *h, int n, const int *gp_of)
 // slip-system counts, or built in with FAS_CP_QUEUE=1): as many
 // 128-thread CTAs as reside at once, at most one item per thread, and the
 // queue head zeroed; otherwise one thread per item.
-template <typename K> unsigned cp_grid(fas_handle *h, K kern, long long n, int **queue)
+// CTA size of a constitutive pass over n items: 128 threads, halved (down
+// to one warp) while that leaves fewer than two CTAs per SM, so that a
+// small mesh spreads its long serial threads over every SM.  Items are
+// independent, so the size changes no result.
+int cp_block(const fas_handle *h, long long n)
+{
+    int bs = 128;
+    while (bs > 32 && n < 2LL * h->nsm * bs) bs >>= 1;
+    return bs;
+}
+
+template <typename K> unsigned cp_grid(fas_handle *h, K kern, long long n, int **queue, int *bs)
 {
     *queue = nullptr;
-    const unsigned full = nblocks(n, 128);
+    *bs = cp_block(h, n);
+    const unsigned full = nblocks(n, *bs);
     if (!FAS_CP_QUEUE && !(h->mode & FAS_MODE_CP_QUEUE) && !h->mixed_phases) return full;
     int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 128, h->stage_bytes) != cudaSuccess || occ < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, *bs, h->stage_bytes) != cudaSuccess || occ < 1)
         return full;
     if (!h->cp_queue.p && h->cp_queue.alloc(1) != cudaSuccess) return full;
     if (cudaMemsetAsync(h->cp_queue.p, 0, sizeof(int), h->stream) != cudaSuccess) return full;
@@ -1161,9 +1173,9 @@ template <int NS> int launch_elem(fas_handle *h, int inc, int nit)
         auto go = [&](auto kern) {
             const long long nit_items = (long long)h->npg * h->nlmnt;
             const int *order = work_order(h, (int)nit_items, h->gp_item.p);
-            int *queue = nullptr;
-            const unsigned grid = cp_grid(h, kern, nit_items, &queue);
-            kern<<<grid, 128, h->stage_bytes, h->stream>>>(h->mesh(), h->M, h->C, h->gp(), h->dnq.p, h->wfac, h->x.p, h->dx.p,
+            int *queue = nullptr, bs = 128;
+            const unsigned grid = cp_grid(h, kern, nit_items, &queue, &bs);
+            kern<<<grid, bs, h->stage_bytes, h->stream>>>(h->mesh(), h->M, h->C, h->gp(), h->dnq.p, h->wfac, h->x.p, h->dx.p,
                                               h->rec.p, h->h_tiem[inc - 1], inc, nit, h->ekey.p, order, queue);
         };
         if (h->nn == 20)
@@ -1175,9 +1187,9 @@ template <int NS> int launch_elem(fas_handle *h, int inc, int nit)
     }
     else if (!(h->mode & FAS_MODE_CP_WARP)) {
         const int *order = work_order(h, h->nlmnt, h->gpe.p);
-        int *queue = nullptr;
-        const unsigned grid = cp_grid(h, k_elem<NS>, h->nlmnt, &queue);
-        k_elem<NS><<<grid, 128, h->stage_bytes, h->stream>>>(
+        int *queue = nullptr, bs = 128;
+        const unsigned grid = cp_grid(h, k_elem<NS>, h->nlmnt, &queue, &bs);
+        k_elem<NS><<<grid, bs, h->stage_bytes, h->stream>>>(
             h->mesh(), h->M, h->C, h->gp(), h->x.p, h->dx.p, h->rec.p, h->h_tiem[inc - 1], inc, nit, h->ekey.p,
             order, queue);
     }
@@ -2336,23 +2348,26 @@ int32_t fas_gpu_constitutive(fas_handle *h, int32_t inc, int32_t nit)
     case 12:
         if (thr) {
             int *queue = nullptr;
-            const unsigned grid = cp_grid(h, k_points<12>, h->ngps, &queue);
-            k_points<12><<<grid, 128, h->stage_bytes, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order, queue);
+            int bs = 128;
+            const unsigned grid = cp_grid(h, k_points<12>, h->ngps, &queue, &bs);
+            k_points<12><<<grid, bs, h->stage_bytes, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order, queue);
         }
         else k_points_wc<12><<<nbw, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p);
         break;
     case 32:
         if (thr) {
             int *queue = nullptr;
-            const unsigned grid = cp_grid(h, k_points<32>, h->ngps, &queue);
-            k_points<32><<<grid, 128, h->stage_bytes, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order, queue);
+            int bs = 128;
+            const unsigned grid = cp_grid(h, k_points<32>, h->ngps, &queue, &bs);
+            k_points<32><<<grid, bs, h->stage_bytes, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order, queue);
         }
         else k_points_wc<32><<<nbw, 128, 0, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p);
         break;
     default: {
         int *queue = nullptr;
-        const unsigned grid = cp_grid(h, k_points<60>, h->ngps, &queue);
-        k_points<60><<<grid, 128, h->stage_bytes, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order, queue);
+        int bs = 128;
+        const unsigned grid = cp_grid(h, k_points<60>, h->ngps, &queue, &bs);
+        k_points<60><<<grid, bs, h->stage_bytes, s>>>(h->M, h->C, h->gp(), h->gp_iel.p, h->chi_pts.p, dt, inc, nit, h->ekey.p, order, queue);
         break;
     }
     }
