@@ -68,3 +68,17 @@ def test_create_without_device_fails_loudly():
     with pytest.raises(abi.FasError) as ei:
         GpuSolver(p)
     assert ei.value.code == abi.FAS_E_NODEVICE
+
+
+def test_python_constants_match_header():
+    """Every FAS_MODE_*, FAS_E_* and FAS_MAX* value of the header equals its
+    name in cpfem_code_b200.abi."""
+    text = open(os.path.join(ROOT, "include", "fasolt_gpu.h")).read()
+    found = re.findall(r"^#define\s+(FAS_(?:MODE|E|MAX)\w*)\s+\(?(-?\d+)u?\)?", text, re.M)
+    assert len(found) >= 15
+    for name, val in found:
+        if hasattr(abi, name):
+            assert getattr(abi, name) == int(val), name
+    for name, _ in found:
+        if name.startswith("FAS_MODE_"):
+            assert hasattr(abi, name), f"{name} has no Python mirror"
