@@ -14,7 +14,10 @@ time it sets:
 * ``sor27f32``: ``FAS_TMA_ROWS32``, ``FAS_TMA_LPR32``, ``FAS_TMA_MINB32``
   (rows per chunk, lanes per row and the CTAs per SM the register budget
   must allow, of the tuned form's FP32-matrix colour kernel), timed by the
-  FP32 FACSLS of the 64^3 cube's first Newton iteration.
+  FP32 FACSLS of the 64^3 cube's first Newton iteration;
+* ``sor81f32``: ``FAS_TMA_ROWS81_32``, ``FAS_TMA_LPR81_32`` (the FP32-matrix
+  colour kernel of 81-slot rows), timed by the FP32 FACSLS of 32^3 20-node
+  bricks.
 
 The knobs act on different kernels, so library i carries candidate i of
 every knob (a knob with fewer candidates repeats its last one), and one
@@ -45,7 +48,9 @@ KNOBS = {
     "sor81": [dict(FAS_TMA_ROWS81=r, FAS_TMA_LPR81=l) for r, l in ((8, 16), (4, 16), (8, 8), (4, 32), (16, 8))],
     "cp": [dict(FAS_WORK_DESC=d, FAS_CP_QUEUE=q) for d, q in ((1, 1), (1, 0), (0, 1), (0, 0))],
     "sor27f32": [dict(FAS_TMA_ROWS32=r, FAS_TMA_LPR32=l, FAS_TMA_MINB32=m)
-                 for r, l, m in ((16, 4, 1), (8, 4, 1), (32, 4, 1), (16, 8, 1), (24, 4, 1), (16, 4, 6))],
+                 for r, l, m in ((24, 4, 1), (16, 4, 1), (32, 4, 1), (16, 8, 1), (8, 4, 1), (16, 4, 6))],
+    "sor81f32": [dict(FAS_TMA_ROWS81_32=r, FAS_TMA_LPR81_32=l)
+                 for r, l in ((4, 16), (8, 16), (8, 8), (4, 32), (2, 16), (16, 8))],
 }
 
 
@@ -142,9 +147,11 @@ def measure() -> dict:
         us27, sw27 = _solve_us(probs["cube64"])
         us81, sw81 = _solve_us(probs["brick20_32"])
         us32, sw32 = _solve_us(probs["cube64"], mode=1)   # FAS_MODE_SOR_FP32
+        us8132, sw8132 = _solve_us(probs["brick20_32"], mode=1)
         out[str(i)] = dict(defines=defines_of(i), cube64_sweep_us=us27, cube64_sweeps=sw27,
                            brick20_32_sweep_us=us81, brick20_32_sweeps=sw81,
                            cube64_fp32_sweep_us=us32, cube64_fp32_sweeps=sw32,
+                           brick20_32_fp32_sweep_us=us8132, brick20_32_fp32_sweeps=sw8132,
                            mixed32_cp_ms=_cp_ms(probs["mixed32"], False),
                            points_cp_ms=_cp_ms(probs["points"], True))
         print(json.dumps(out[str(i)]), flush=True)
@@ -164,13 +171,14 @@ def select(meas: dict | None = None, out: str = TUNED) -> dict:
         "sor27": lambda r: r["cube64_sweep_us"],
         "sor81": lambda r: r["brick20_32_sweep_us"],
         "sor27f32": lambda r: r["cube64_fp32_sweep_us"],
+        "sor81f32": lambda r: r.get("brick20_32_fp32_sweep_us", r["brick20_32_sweep_us"]),
         "cp": lambda r: math.sqrt(r["mixed32_cp_ms"] / rows[0]["mixed32_cp_ms"]
                                   * r["points_cp_ms"] / rows[0]["points_cp_ms"]),
     }
     # sweep counts do not depend on a launch shape; a candidate that changed
     # them would be wrong, not fast
-    for key in ("cube64_sweeps", "brick20_32_sweeps", "cube64_fp32_sweeps"):
-        assert len({r[key] for r in rows}) == 1, f"{key} differ between candidates"
+    for key in ("cube64_sweeps", "brick20_32_sweeps", "cube64_fp32_sweeps", "brick20_32_fp32_sweeps"):
+        assert len({r.get(key) for r in rows}) == 1, f"{key} differ between candidates"
     tuned = {"defines": {}, "measured": {}}
     for knob, cands in KNOBS.items():
         vals = [score[knob](rows[i]) for i in range(len(cands))]

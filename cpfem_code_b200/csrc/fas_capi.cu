@@ -469,7 +469,7 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
     for (int c = 0; c < h->ncol; ++c) {
         h->sor_boff32[c] = tot32;
         const int cps = h->slots == SLOTS ? tma_ctas_per_sm<SLOTS, TMA_LPR32, float>()
-                                          : tma_ctas_per_sm<SLOTS20, TMA_LPR81, float>();
+                                          : tma_ctas_per_sm<SLOTS20, TMA_LPR81_32, float>();
         const int rows = h->slots == SLOTS ? tma_rows<SLOTS, float>() : tma_rows<SLOTS20, float>();
         h->sor_nblk32[c] = (int)std::min<long long>(nblocks(h->col_start[c + 1] - h->col_start[c], rows),
                                                      (long long)h->nsm * cps);
@@ -728,7 +728,7 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
                             cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem_bytes<float, SLOTS>()));
     CK(cudaFuncSetAttribute(k_sor_colour_tma<double, SLOTS20, TMA_LPR81>,
                             cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem_bytes<double, SLOTS20>()));
-    CK(cudaFuncSetAttribute(k_sor_colour_tma<float, SLOTS20, TMA_LPR81>,
+    CK(cudaFuncSetAttribute(k_sor_colour_tma<float, SLOTS20, TMA_LPR81_32>,
                             cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem_bytes<float, SLOTS20>()));
     CK(cudaFuncSetAttribute(k_sor_tiles<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             tile_smem_bytes<double>()));
@@ -1325,8 +1325,9 @@ void launch_colour_kernel(fas_handle *h, int c, bool pdl, const T *blk, const do
             k<<<nblk, nt, tma_smem_bytes<T, SLOTS>(), h->stream>>>(
                 blk, h->bcol.p, p0, p1, rhs, sol, base, rdiag, ctl, part, boff, ntot);
     } else {
-        auto k = k_sor_colour_tma<T, SLOTS20, TMA_LPR81>;
-        const unsigned nt = tma_threads<TMA_LPR81, TMA_ROWS81>();
+        constexpr int LPR = tma_lpr<SLOTS20, T>();
+        auto k = k_sor_colour_tma<T, SLOTS20, LPR>;
+        const unsigned nt = tma_threads<LPR, tma_rows<SLOTS20, T>()>();
         if (pdl)
             launch_pdl(k, nblk, nt, tma_smem_bytes<T, SLOTS20>(), h->stream, blk, h->bcol.p, p0, p1,
                        rhs, sol, base, rdiag, ctl, part, boff, ntot);

@@ -1174,6 +1174,15 @@ constexpr int TMA_ROWS81 = FAS_TMA_ROWS81;   // rows per chunk of 81-slot rows
 #ifndef FAS_SOR32_ARITH
 #define FAS_SOR32_ARITH 1
 #endif
+// and so have the FP32 sweeps of 81-slot rows
+#ifndef FAS_TMA_ROWS81_32
+#define FAS_TMA_ROWS81_32 4
+#endif
+#ifndef FAS_TMA_LPR81_32
+#define FAS_TMA_LPR81_32 16
+#endif
+constexpr int TMA_ROWS81_32 = FAS_TMA_ROWS81_32;   // rows per chunk of FP32 81-slot rows
+constexpr int TMA_LPR81_32 = FAS_TMA_LPR81_32;     // lanes per row of FP32 81-slot rows
 constexpr int TMA_ROWS32 = FAS_TMA_ROWS32;   // rows per chunk of FP32 27-slot rows
 constexpr int TMA_LPR32 = FAS_TMA_LPR32;     // lanes per row of FP32 27-slot rows
 constexpr int TMA_MINB32 = FAS_TMA_MINB32;   // CTAs per SM the FP32 kernel's registers must allow
@@ -1188,8 +1197,16 @@ static_assert(TMA_THREADS % 32 == 0 && tma_threads<TMA_LPR81, TMA_ROWS81>() % 32
 // rows per chunk of the S-slot layout in value type T
 template <int S, typename T = double> __host__ __device__ constexpr int tma_rows()
 {
-    return S == SLOTS ? (sizeof(T) == 4 ? TMA_ROWS32 : TMA_ROWS) : TMA_ROWS81;
+    return S == SLOTS ? (sizeof(T) == 4 ? TMA_ROWS32 : TMA_ROWS) : (sizeof(T) == 4 ? TMA_ROWS81_32 : TMA_ROWS81);
 }
+// lanes per row of the S-slot layout in value type T
+template <int S, typename T = double> __host__ __device__ constexpr int tma_lpr()
+{
+    return S == SLOTS ? (sizeof(T) == 4 ? TMA_LPR32 : TMA_LPR) : (sizeof(T) == 4 ? TMA_LPR81_32 : TMA_LPR81);
+}
+static_assert(tma_threads<TMA_LPR81_32, TMA_ROWS81_32>() % 32 == 0 && (TMA_LPR81_32 & (TMA_LPR81_32 - 1)) == 0 &&
+                  TMA_LPR81_32 <= 32,
+              "whole warps per CTA");
 // minimum CTAs per SM the kernel's register budget must allow (1: no bound)
 template <int S, typename T> __host__ __device__ constexpr int tma_minb()
 {

@@ -57,7 +57,9 @@ extern "C" {
 /* ---- mode flags for fas_gpu_create / fas_gpu_set_mode ------------------ */
 #define FAS_MODE_PLAIN        0u  /* FP64 everywhere, reference tangent      */
 #define FAS_MODE_SOR_FP32     1u  /* SOR sweeps on an FP32 copy of the
-                                     matrix with FP64 residual refinement   */
+                                     matrix (FP32 products, FP64 point
+                                     update and stopping test) with an FP64
+                                     residual every 16 sweeps               */
 #define FAS_MODE_SOR_NATURAL  2u  /* (oracle only) natural-order SOR        */
 #define FAS_MODE_CP_WARP      8u  /* Gauss-point update with one warp per GP
                                      (lanes = slip systems) instead of one

@@ -18,7 +18,8 @@ def test_every_candidate_of_every_knob_is_built():
 def _fake(i, us27, us81, mixed, pts, sw=(252, 318)):
     return dict(defines=autotune.defines_of(i), cube64_sweep_us=us27, cube64_sweeps=sw[0],
                 brick20_32_sweep_us=us81, brick20_32_sweeps=sw[1], mixed32_cp_ms=mixed, points_cp_ms=pts,
-                cube64_fp32_sweep_us=us27 / 2, cube64_fp32_sweeps=sw[0])
+                cube64_fp32_sweep_us=us27 / 2, cube64_fp32_sweeps=sw[0],
+                brick20_32_fp32_sweep_us=us81 / 2, brick20_32_fp32_sweeps=sw[1])
 
 
 def test_select_takes_the_best_candidate_per_knob(tmp_path):
