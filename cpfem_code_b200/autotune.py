@@ -50,7 +50,7 @@ KNOBS = {
     "sor27f32": [dict(FAS_TMA_ROWS32=r, FAS_TMA_LPR32=l, FAS_TMA_MINB32=m)
                  for r, l, m in ((24, 4, 1), (16, 4, 1), (32, 4, 1), (16, 8, 1), (8, 4, 1), (16, 4, 6))],
     "sor81f32": [dict(FAS_TMA_ROWS81_32=r, FAS_TMA_LPR81_32=l)
-                 for r, l in ((4, 16), (8, 16), (8, 8), (4, 32), (2, 16), (16, 8))],
+                 for r, l in ((16, 8), (32, 8), (16, 4), (32, 4), (8, 4), (24, 8))],
 }
 
 
