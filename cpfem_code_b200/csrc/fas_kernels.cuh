@@ -1176,10 +1176,10 @@ constexpr int TMA_ROWS81 = FAS_TMA_ROWS81;   // rows per chunk of 81-slot rows
 #endif
 // and so have the FP32 sweeps of 81-slot rows
 #ifndef FAS_TMA_ROWS81_32
-#define FAS_TMA_ROWS81_32 4
+#define FAS_TMA_ROWS81_32 16
 #endif
 #ifndef FAS_TMA_LPR81_32
-#define FAS_TMA_LPR81_32 16
+#define FAS_TMA_LPR81_32 8
 #endif
 constexpr int TMA_ROWS81_32 = FAS_TMA_ROWS81_32;   // rows per chunk of FP32 81-slot rows
 constexpr int TMA_LPR81_32 = FAS_TMA_LPR81_32;     // lanes per row of FP32 81-slot rows

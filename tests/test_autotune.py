@@ -45,3 +45,17 @@ def test_build_reads_the_committed_choice():
     if d:
         for knob, cands in autotune.KNOBS.items():
             assert any(all(d[k] == v for k, v in c.items()) for c in cands), knob
+
+
+def test_select_skips_candidates_the_device_refused(tmp_path):
+    """A library whose combination the device refused (recorded with an
+    error) scores worst in every knob; the others are still ranked."""
+    meas = {str(i): _fake(i, 130 - i, 200 + i, 10 + i, 20 - i) for i in range(autotune.n_libs())}
+    last = str(autotune.n_libs() - 1)
+    meas[last] = dict(defines=autotune.defines_of(int(last)), error="fas_gpu_create: ABI error -3")
+    t = autotune.select(meas, str(tmp_path / "tuned.json"))
+    sor27 = autotune.KNOBS["sor27"]
+    # the refused library held sor27's last candidate (the best one otherwise)
+    best = sor27[min(len(sor27) - 1, autotune.n_libs() - 2)]
+    for k, v in best.items():
+        assert t["defines"][k] == v
