@@ -143,6 +143,7 @@ struct fas_handle {
     DVec<double> blk;
     DVec<float> blk32;           // FP32 copy for FAS_MODE_SOR_FP32
     DVec<double> sor_d, sor_r;   // correction and residual of the refinement
+    DVec<float> sor_d32;         // the correction rounded to FP32 (the FP32 sweeps' gathers)
     DVec<double> rdiag;          // reciprocals of the diagonal entries, row order
     DVec<int> work_order, work_hist;   // work-sorted constitutive launch order
     DVec<int> cp_queue;          // head of the constitutive pass's device queue
@@ -1212,6 +1213,7 @@ int ensure_fp32(fas_handle *h)
     const size_t nd3 = 3 * (size_t)h->nnod;
     CKA(h->blk32.alloc((size_t)brow_of(h->slots) * h->nnod));
     CKA(h->sor_d.alloc(nd3));
+    CKA(h->sor_d32.alloc(nd3));
     CKA(h->sor_r.alloc(nd3));
     CK(h->blk32.zero(h->stream));
     return 0;
@@ -1306,7 +1308,8 @@ void launch_pdl(void (*kern)(KArgs...), unsigned grid, unsigned block, size_t sm
 // slots), with programmatic serialisation when `pdl` is set.
 template <typename T>
 void launch_colour_kernel(fas_handle *h, int c, bool pdl, const T *blk, const double *rhs, double *sol,
-                          const double *base, const double *rdiag, SorCtl *ctl, double *part)
+                          const double *base, const double *rdiag, SorCtl *ctl, double *part,
+                          float *sol32 = nullptr)
 {
     const int p0 = h->col_start[c], p1 = h->col_start[c + 1];
     if (p1 <= p0) return;
@@ -1320,20 +1323,20 @@ void launch_colour_kernel(fas_handle *h, int c, bool pdl, const T *blk, const do
         const unsigned nt = tma_threads<LPR, tma_rows<SLOTS, T>()>();
         if (pdl)
             launch_pdl(k, nblk, nt, tma_smem_bytes<T, SLOTS>(), h->stream, blk, h->bcol.p, p0,
-                       p1, rhs, sol, base, rdiag, ctl, part, boff, ntot);
+                       p1, rhs, sol, base, rdiag, ctl, part, boff, ntot, sol32);
         else
             k<<<nblk, nt, tma_smem_bytes<T, SLOTS>(), h->stream>>>(
-                blk, h->bcol.p, p0, p1, rhs, sol, base, rdiag, ctl, part, boff, ntot);
+                blk, h->bcol.p, p0, p1, rhs, sol, base, rdiag, ctl, part, boff, ntot, sol32);
     } else {
         constexpr int LPR = tma_lpr<SLOTS20, T>();
         auto k = k_sor_colour_tma<T, SLOTS20, LPR>;
         const unsigned nt = tma_threads<LPR, tma_rows<SLOTS20, T>()>();
         if (pdl)
             launch_pdl(k, nblk, nt, tma_smem_bytes<T, SLOTS20>(), h->stream, blk, h->bcol.p, p0, p1,
-                       rhs, sol, base, rdiag, ctl, part, boff, ntot);
+                       rhs, sol, base, rdiag, ctl, part, boff, ntot, sol32);
         else
             k<<<nblk, nt, tma_smem_bytes<T, SLOTS20>(), h->stream>>>(
-                blk, h->bcol.p, p0, p1, rhs, sol, base, rdiag, ctl, part, boff, ntot);
+                blk, h->bcol.p, p0, p1, rhs, sol, base, rdiag, ctl, part, boff, ntot, sol32);
     }
 }
 
@@ -1354,7 +1357,7 @@ void launch_colour(fas_handle *h, int c, bool fp32)
 {
     if (fp32)
         launch_colour_kernel<float>(h, c, true, h->blk32.p, h->sor_r.p, h->sor_d.p, h->ddx.p, nullptr,
-                                    h->sorctl.p, h->part_sor.p);
+                                    h->sorctl.p, h->part_sor.p, h->sor_d32.p);
     else
         launch_colour_kernel<double>(h, c, true, h->blk.p, h->rhs.p, h->ddx.p, nullptr,
                                      FAS_SOR_RCP ? h->rdiag.p : nullptr, h->sorctl.p, h->part_sor.p);
@@ -1399,7 +1402,7 @@ void launch_fp32_cycle(fas_handle *h, const BlockDev &B, double tolerl, int swee
         for (int c = 0; c < h->ncol; ++c) launch_colour(h, c, true);
         launch_check(h, tolerl, true);
     }
-    k_fold<<<nblocks((long long)nd3, 256), 256, 0, h->stream>>>((int)nd3, h->ddx.p, h->sor_d.p);
+    k_fold<<<nblocks((long long)nd3, 256), 256, 0, h->stream>>>((int)nd3, h->ddx.p, h->sor_d.p, h->sor_d32.p);
     k_residual<<<rblk, 256, 0, h->stream>>>(B, h->rhs.p, h->ddx.p, h->sor_r.p, h->sorctl.p);
 }
 
@@ -1494,6 +1497,7 @@ int facsls_tiles(fas_handle *h, const BlockDev &B, double tolerl, bool fp32)
     // x (= ddx) starts at 0, so the first residual is rhs itself
     CK(cudaMemcpyAsync(h->sor_r.p, h->rhs.p, nd3 * sizeof(double), cudaMemcpyDeviceToDevice, s));
     CK(cudaMemsetAsync(h->sor_d.p, 0, nd3 * sizeof(double), s));
+        CK(cudaMemsetAsync(h->sor_d32.p, 0, nd3 * sizeof(float), s));
     const int m = h->refine_every;
     const unsigned rblk = (unsigned)std::min<long long>(nblocks(rows, 8), (long long)h->nsm * 8);
     int done = 0, outer_per_chunk = 1;
@@ -1506,7 +1510,7 @@ int facsls_tiles(fas_handle *h, const BlockDev &B, double tolerl, bool fp32)
             sp.end();
             keep(h, sp);
             if (rc) return rc;
-            k_fold<<<nblocks((long long)nd3, 256), 256, 0, s>>>((int)nd3, h->ddx.p, h->sor_d.p);
+            k_fold<<<nblocks((long long)nd3, 256), 256, 0, s>>>((int)nd3, h->ddx.p, h->sor_d.p, h->sor_d32.p);
             LAUNCHED(h);
             k_residual<<<rblk, 256, 0, s>>>(B, h->rhs.p, h->ddx.p, h->sor_r.p, h->sorctl.p);
             LAUNCHED(h);
@@ -1563,6 +1567,7 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
         // x (= ddx) starts at 0, so the first residual is rhs itself
         CK(cudaMemcpyAsync(h->sor_r.p, h->rhs.p, nd3 * sizeof(double), cudaMemcpyDeviceToDevice, s));
         CK(cudaMemsetAsync(h->sor_d.p, 0, nd3 * sizeof(double), s));
+        CK(cudaMemsetAsync(h->sor_d32.p, 0, nd3 * sizeof(float), s));
         const int m = h->refine_every;
         const unsigned rblk = (unsigned)std::min<long long>(nblocks(h->nnod, 8), (long long)h->nsm * 8);
         const bool graph32 = h->prof < 2 && ensure_fp32_graph(h, B, tolerl) == 0;
@@ -1589,7 +1594,7 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
                     LAUNCHED(h);
                 }
                 done += k;
-                k_fold<<<nblocks((long long)nd3, 256), 256, 0, s>>>((int)nd3, h->ddx.p, h->sor_d.p);
+                k_fold<<<nblocks((long long)nd3, 256), 256, 0, s>>>((int)nd3, h->ddx.p, h->sor_d.p, h->sor_d32.p);
                 LAUNCHED(h);
                 k_residual<<<rblk, 256, 0, s>>>(B, h->rhs.p, h->ddx.p, h->sor_r.p, h->sorctl.p);
                 LAUNCHED(h);
@@ -1806,6 +1811,7 @@ int capture_nr_body(fas_handle *h, int inc, cudaGraphConditionalHandle hnr)
     if (fp32) {
         CK(cudaMemcpyAsync(h->sor_r.p, h->rhs.p, nd3 * sizeof(double), cudaMemcpyDeviceToDevice, s));
         CK(cudaMemsetAsync(h->sor_d.p, 0, nd3 * sizeof(double), s));
+        CK(cudaMemsetAsync(h->sor_d32.p, 0, nd3 * sizeof(float), s));
     }
     cudaGraphConditionalHandle hsor, hlast = 0;
     if (int r = make_condition(s, 0, false, &hsor)) return r;

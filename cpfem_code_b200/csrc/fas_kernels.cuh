@@ -26,6 +26,8 @@
 // the increment commit, twin reorientation, ELASEPS and the exports.
 #pragma once
 
+#include <type_traits>
+
 #include "fas_device.cuh"
 #include "fas_device_warp.cuh"
 
@@ -1241,17 +1243,32 @@ static_assert(TMA_CTAS_PER_SM >= 1 && tma_ctas_per_sm<SLOTS20, TMA_LPR81>() >= 1
 // Operands of one chunk row for one lane, gathered before its point
 // update: the solution at the lane's slots (x0, x1, x2) and, on the row's
 // first lane, the right-hand side and reciprocal diagonal of the row's node (r).
-template <int SPL> struct SorOps {
-    double x0[SPL], x1[SPL], x2[SPL], r[6];
+template <int SPL, typename XT = double> struct SorOps {
+    XT x0[SPL], x1[SPL], x2[SPL];
+    double r[6];
 };
+// The FP32 sweeps' form: the slots' values from the FP32 mirror of the
+// correction (exactly the values the FP32 products round them to), and the
+// row node's own old values in FP64 for the point update.
+template <int SPL> struct SorOps<SPL, float> {
+    float x0[SPL], x1[SPL], x2[SPL];
+    double r[6], own[3];
+};
+
+__device__ __forceinline__ float ld_keep_f32(const float *ptr, uint64_t pol)
+{
+    float v;
+    asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(ptr), "l"(pol));
+    return v;
+}
 
 // Gather of lane q of chunk row `row` from a landed stage's column ids.
 // r0 is the chunk's first row and nrow its row count.
-template <int S, int LPR>
+template <int S, int LPR, typename XT = double>
 __device__ __forceinline__ void sor_gather(const int *stage_cols, int r0, int nrow, int row, int q,
                                            const double *sol, const double *__restrict__ rhs,
                                            const double *__restrict__ rdiag, uint64_t keep_pol,
-                                           SorOps<(S + LPR - 1) / LPR> &g)
+                                           SorOps<(S + LPR - 1) / LPR, XT> &g, const float *sol32 = nullptr)
 {
     constexpr int SPL = (S + LPR - 1) / LPR, CR = crow_of(S);
     const bool live = row < nrow;
@@ -1262,12 +1279,23 @@ __device__ __forceinline__ void sor_gather(const int *stage_cols, int r0, int nr
         const int sl = q + LPR * j;
         const bool on = sl < ns;
         const int m = on ? cols[sl] : 0;
-        g.x0[j] = on ? ld_keep(sol + 3 * m, keep_pol) : 0.0;
-        g.x1[j] = on ? ld_keep(sol + 3 * m + 1, keep_pol) : 0.0;
-        g.x2[j] = on ? ld_keep(sol + 3 * m + 2, keep_pol) : 0.0;
+        if constexpr (sizeof(XT) == 4) {
+            g.x0[j] = on ? ld_keep_f32(sol32 + 3 * m, keep_pol) : 0.f;
+            g.x1[j] = on ? ld_keep_f32(sol32 + 3 * m + 1, keep_pol) : 0.f;
+            g.x2[j] = on ? ld_keep_f32(sol32 + 3 * m + 2, keep_pol) : 0.f;
+        } else {
+            g.x0[j] = on ? ld_keep(sol + 3 * m, keep_pol) : 0.0;
+            g.x1[j] = on ? ld_keep(sol + 3 * m + 1, keep_pol) : 0.0;
+            g.x2[j] = on ? ld_keep(sol + 3 * m + 2, keep_pol) : 0.0;
+        }
     }
     const bool own = live && q == 0;
     const int n = cols[0];
+    if constexpr (sizeof(XT) == 4) {
+        g.own[0] = own ? ld_keep(sol + 3 * n, keep_pol) : 0.0;
+        g.own[1] = own ? ld_keep(sol + 3 * n + 1, keep_pol) : 0.0;
+        g.own[2] = own ? ld_keep(sol + 3 * n + 2, keep_pol) : 0.0;
+    }
     g.r[0] = own ? ld_keep(rhs + 3 * n, keep_pol) : 0.0;
     g.r[1] = own ? ld_keep(rhs + 3 * n + 1, keep_pol) : 0.0;
     g.r[2] = own ? ld_keep(rhs + 3 * n + 2, keep_pol) : 0.0;
@@ -1285,12 +1313,15 @@ __device__ __forceinline__ void sor_gather(const int *stage_cols, int r0, int nr
 // the first lane updates x, y and z in turn (omega = 1.2), stores them and
 // adds |x_new - x_old|^2 to v0 and |x_new + base|^2 to v1.  With `rcp` the
 // quotients come from the gathered reciprocal diagonal.
-template <typename T, int S, int LPR, int ROWS>
+// With FP32 gathers (XT = float) the row's own old values come from g.own,
+// and the new values also go, rounded, to the mirror sol32.
+template <typename T, int S, int LPR, int ROWS, typename XT = double>
 __device__ __forceinline__ void sor_update(const unsigned char *stage, int nrow, int row, int q,
-                                           const SorOps<(S + LPR - 1) / LPR> &g, bool rcp,
+                                           const SorOps<(S + LPR - 1) / LPR, XT> &g, bool rcp,
                                            const double *__restrict__ base, double *sol, double &v0,
-                                           double &v1)
+                                           double &v1, float *sol32 = nullptr)
 {
+    static_assert(sizeof(XT) == 8 || (sizeof(T) == 4 && FAS_SOR32_ARITH), "FP32 gathers feed FP32 products only");
     constexpr int SPL = (S + LPR - 1) / LPR, BR = brow_of(S), CR = crow_of(S);
     constexpr int VB = ROWS * BR * (int)sizeof(T);
     const bool live = row < nrow;
@@ -1339,7 +1370,16 @@ __device__ __forceinline__ void sor_update(const unsigned char *stage, int nrow,
         double D[9];
 #pragma unroll
         for (int qq = 0; qq < 9; ++qq) D[qq] = (double)vals[qq * S];
-        const double o0 = g.x0[0], o1 = g.x1[0], o2 = g.x2[0];
+        double o0, o1, o2;
+        if constexpr (sizeof(XT) == 4) {
+            o0 = g.own[0];
+            o1 = g.own[1];
+            o2 = g.own[2];
+        } else {
+            o0 = g.x0[0];
+            o1 = g.x1[0];
+            o2 = g.x2[0];
+        }
         double x0 = o0, x1 = o1, x2 = o2;
         double t;
         if (rcp) {
@@ -1371,6 +1411,11 @@ __device__ __forceinline__ void sor_update(const unsigned char *stage, int nrow,
         sol[3 * n] = x0;
         sol[3 * n + 1] = x1;
         sol[3 * n + 2] = x2;
+        if constexpr (sizeof(XT) == 4) {
+            sol32[3 * n] = (float)x0;
+            sol32[3 * n + 1] = (float)x1;
+            sol32[3 * n + 2] = (float)x2;
+        }
         v0 += (x0 - o0) * (x0 - o0) + (x1 - o1) * (x1 - o1) + (x2 - o2) * (x2 - o2);
         if (base) {
             x0 += base[3 * n];
@@ -1401,11 +1446,15 @@ __global__ void __launch_bounds__(tma_rows<S, T>() * LPR, tma_minb<S, T>()) k_so
                                                                 const double *__restrict__ rhs, double *sol,
                                                                 const double *__restrict__ base,
                                                                 const double *__restrict__ rdiag, SorCtl *ctl,
-                                                                double *part, int boff, int nblk_tot)
+                                                                double *part, int boff, int nblk_tot,
+                                                                float *sol32)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int s_pre, s_post;
     constexpr int BR = brow_of(S), CR = crow_of(S);
+    // FP32 sweeps with FP32 products gather from the correction's FP32
+    // mirror sol32 (kept equal to the correction rounded to FP32)
+    using XT = std::conditional_t<sizeof(T) == 4 && FAS_SOR32_ARITH, float, double>;
     static_assert((BR * sizeof(T)) % 16 == 0 && (CR * 4) % 16 == 0, "bulk copies move 16-byte multiples");
     constexpr int SPL = (S + LPR - 1) / LPR;   // slots per lane
     constexpr int ROWS = tma_rows<S, T>();
@@ -1457,11 +1506,11 @@ __global__ void __launch_bounds__(tma_rows<S, T>() * LPR, tma_minb<S, T>()) k_so
     // to chunk k + j.  No row of a colour reads a value written by another
     // row of the same colour, so the gathers of the next TMA_PD chunks are
     // in flight while chunk k is computed.
-    SorOps<SPL> g[TMA_PD + 1] = {};
-    auto gather = [&](int kk, SorOps<SPL> &o) {
+    SorOps<SPL, XT> g[TMA_PD + 1] = {};
+    auto gather = [&](int kk, SorOps<SPL, XT> &o) {
         const int r0 = p0 + (blockIdx.x + kk * gridDim.x) * ROWS;
-        sor_gather<S, LPR>(reinterpret_cast<const int *>(smem + (kk % TMA_STAGES) * SB + VB), r0,
-                           min(ROWS, p1 - r0), row, q, sol, rhs, rdiag, keep_pol, o);
+        sor_gather<S, LPR, XT>(reinterpret_cast<const int *>(smem + (kk % TMA_STAGES) * SB + VB), r0,
+                               min(ROWS, p1 - r0), row, q, sol, rhs, rdiag, keep_pol, o, sol32);
     };
     // chunks [0, waited) have landed; chunks [0, min(myn, k + TMA_STAGES))
     // have been issued when iteration k starts
@@ -1491,7 +1540,8 @@ __global__ void __launch_bounds__(tma_rows<S, T>() * LPR, tma_minb<S, T>()) k_so
         }
         const int st = k % TMA_STAGES;
         const int nrow = min(ROWS, p1 - (p0 + (int)(blockIdx.x + k * gridDim.x) * ROWS));
-        sor_update<T, S, LPR, ROWS>(smem + st * SB, nrow, row, q, g[0], rdiag != nullptr, base, sol, v0, v1);
+        sor_update<T, S, LPR, ROWS, XT>(smem + st * SB, nrow, row, q, g[0], rdiag != nullptr, base, sol, v0, v1,
+                                        sol32);
         __syncthreads();   // every row of this stage is done
         if (threadIdx.x == 0 && k + TMA_STAGES < myn) {
             fence_proxy_async();
@@ -1603,13 +1653,14 @@ __global__ void __launch_bounds__(256) k_residual(BlockDev B, const double *__re
     }
 }
 
-// x += d, d = 0 (end of one refinement step).
-__global__ void k_fold(int ndof, double *x, double *d)
+// x += d, d = 0 and its FP32 mirror d32 = 0 (end of one refinement step).
+__global__ void k_fold(int ndof, double *x, double *d, float *d32)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ndof) return;
     x[i] += d[i];
     d[i] = 0.0;
+    if (d32) d32[i] = 0.f;
 }
 
 // End of one sweep: error = sum(dx^2) / sum(x^2) (Stif_sol.f90:206-210).
