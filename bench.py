@@ -429,7 +429,8 @@ def run_increments(g, prob, start, ninc_warm: int, ninc_timed: int):
     out, ends = {}, {}
     legs = [("plain", abi.FAS_MODE_PLAIN), ("tuned", TUNED_MODE),
             ("plain_consistent_tangent", abi.FAS_MODE_TANGENT_CONSISTENT),
-            ("plain_graph", abi.FAS_MODE_GRAPH), ("tuned_graph", TUNED_MODE | abi.FAS_MODE_GRAPH)]
+            ("plain_graph", abi.FAS_MODE_GRAPH), ("tuned_graph", TUNED_MODE | abi.FAS_MODE_GRAPH),
+            ("tuned_sym", TUNED_MODE | abi.FAS_MODE_SOR_SYM)]
     for tag, mode in legs:
         t = s0.copy()
         g.upload(t)
@@ -466,6 +467,11 @@ def run_increments(g, prob, start, ninc_warm: int, ninc_timed: int):
     out["tuned_graph"]["mode"] = "the tuned form with each increment's NRITER as one CUDA graph"
     out["tuned_graph"]["same_result_as_tuned"] = all(
         np.array_equal(getattr(ends["tuned_graph"], k), getattr(ends["tuned"], k)) for k in _state_arrays(s0))
+    out["tuned_sym"]["mode"] = ("the tuned form on symmetric FP32 rows (each off-diagonal block streamed once, "
+                                "transposed products pushed by vector atomic adds); no effect on 20-node rows")
+    out["speedup_tuned_sym_vs_plain_s_per_increment"] = (out["plain"]["s_per_increment"]
+                                                         / out["tuned_sym"]["s_per_increment"])
+    out["tuned_sym_vs_plain_error"] = stress_errors(ends["tuned_sym"], ends["plain"])
     return out, s0, ends["plain"]
 
 
@@ -588,7 +594,8 @@ def run_gpu(args):
                           f"({sum(r['sor_sweeps'] for r in reps_c)} SOR sweeps) by the C++ restatement, "
                           f"{secs:.1f} s"}
             errs = {}
-            for tag, mode in (("plain", abi.FAS_MODE_PLAIN), ("tuned", TUNED_MODE)):
+            for tag, mode in (("plain", abi.FAS_MODE_PLAIN), ("tuned", TUNED_MODE),
+                              ("tuned_sym", TUNED_MODE | abi.FAS_MODE_SOR_SYM)):
                 q = prob.copy()
                 _, rg = timed_steps(g, start, CPU_STEPS, mode, level=0)
                 g.download(q)
@@ -621,10 +628,12 @@ def rooflines(g, start, prob) -> dict:
     pk = peaks()
     out = {}
     kernels = {"sor": "k_sor_colour_tma<double,27,4>", "sor_fp32": "k_sor_colour_tma<float,27,4>",
-               "sor_tiles": "k_sor_tiles<double>", "sor_fp32_tiles": "k_sor_tiles<float>"}
+               "sor_tiles": "k_sor_tiles<double>", "sor_fp32_tiles": "k_sor_tiles<float>",
+               "sor_fp32_sym": "k_sor_colour_tma<float,14,8,true>"}
     for tag, mode in (("sor", abi.FAS_MODE_PLAIN), ("sor_fp32", abi.FAS_MODE_SOR_FP32),
                       ("sor_tiles", abi.FAS_MODE_SOR_TILES),
-                      ("sor_fp32_tiles", abi.FAS_MODE_SOR_FP32 | abi.FAS_MODE_SOR_TILES)):
+                      ("sor_fp32_tiles", abi.FAS_MODE_SOR_FP32 | abi.FAS_MODE_SOR_TILES),
+                      ("sor_fp32_sym", abi.FAS_MODE_SOR_FP32 | abi.FAS_MODE_SOR_SYM)):
         g.upload(start)
         g.set_mode(mode)
         g.update_node()
@@ -871,7 +880,7 @@ def run_case(args) -> int:
     * ``--case points``: ``--reps`` DSTRSS passes over ``--points`` points;
     * ``--case sweeps``: microseconds per sweep of the first FACSLS of n^3
       cubes on every solve path (one CTA, colour kernels, tiles; FP64 and
-      FP32), one JSON line per size.
+      FP32, and FP32 on symmetric rows), one JSON line per size.
     """
     from cpfem_code_b200 import GpuSolver, ReplayHistory, generator
     if args.case == "facsls":
@@ -898,7 +907,8 @@ def run_case(args) -> int:
         paths = {"one_cta": 0, "colour": abi.FAS_MODE_SOR_GRID,
                  "tiles": abi.FAS_MODE_SOR_GRID | abi.FAS_MODE_SOR_TILES,
                  "tiles_fp32": abi.FAS_MODE_SOR_GRID | abi.FAS_MODE_SOR_TILES | abi.FAS_MODE_SOR_FP32,
-                 "colour_fp32": abi.FAS_MODE_SOR_GRID | abi.FAS_MODE_SOR_FP32}
+                 "colour_fp32": abi.FAS_MODE_SOR_GRID | abi.FAS_MODE_SOR_FP32,
+                 "colour_fp32_sym": abi.FAS_MODE_SOR_GRID | abi.FAS_MODE_SOR_FP32 | abi.FAS_MODE_SOR_SYM}
         for n in (2, 4, 8, 12, 16, 20, 24, 32, 40, 48, 64):
             p = generator.cube_config(n=n, ninc=1, grain=1, seed=n)
             row = {"n": n, "nodes": p.nnod}

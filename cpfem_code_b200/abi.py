@@ -36,6 +36,7 @@ FAS_MODE_SOR_TILES = 16
 FAS_MODE_TANGENT_CONSISTENT = 32
 FAS_MODE_CP_QUEUE = 64
 FAS_MODE_GRAPH = 128
+FAS_MODE_SOR_SYM = 256
 
 #: FAFERR codes the hot path raises, with the reference's meaning.
 FAFERR_TEXT = {

@@ -144,6 +144,16 @@ struct fas_handle {
     DVec<float> blk32;           // FP32 copy for FAS_MODE_SOR_FP32
     DVec<double> sor_d, sor_r;   // correction and residual of the refinement
     DVec<float> sor_d32;         // the correction rounded to FP32 (the FP32 sweeps' gathers)
+    // symmetric FP32 rows (FAS_MODE_SOR_SYM, 27-slot rows): the blocks each
+    // row stores (bit s of sym_mask: slot s), the packed rows, and per node
+    // the accumulated transposed products of the blocks stored elsewhere
+    DVec<unsigned> sym_mask;
+    DVec<float> blk_sym, sor_acc;
+    DVec<int> bcol_sym;
+    int sym_state = 0;           // 0 not set up, 1 usable, -1 the pattern does not fit SLOTS_SYM
+    bool sym_on = false;         // the FP32 sweeps of this solve use the symmetric rows
+    std::vector<int> sor_boff_sym, sor_nblk_sym;
+    int sor_nblk_tot_sym = 0;
     DVec<double> rdiag;          // reciprocals of the diagonal entries, row order
     DVec<int> work_order, work_hist;   // work-sorted constitutive launch order
     DVec<int> cp_queue;          // head of the constitutive pass's device queue
@@ -166,6 +176,7 @@ struct fas_handle {
     int refine_every = 16;       // FP32 sweeps per FP64 residual
     cudaGraphExec_t sor_graph = nullptr;   // GRAPH_SWEEPS plain sweeps
     cudaGraphExec_t sor32_graph = nullptr; // one refinement cycle of the FP32 form
+    bool sor32_graph_sym = false;          // ... on the symmetric rows
     bool blk32_fresh = false;    // the last assembly wrote blk32
     // reductions and control
     std::vector<int> sor_boff, sor_nblk;       // FP64 colour grids and their partial offsets
@@ -477,7 +488,26 @@ int build_layout(fas_handle *h, const std::vector<double> &xyz)
         tot32 += h->sor_nblk32[c];
     }
     h->sor_nblk_tot32 = std::max(tot32, 1);
-    CKA(h->part_sor.alloc((size_t)2 * std::max(h->sor_nblk_tot, h->sor_nblk_tot32)));
+    // symmetric FP32 rows (27-slot meshes): rings of their own size; one
+    // wave of the CTAs that reside per SM (their registers, not only the
+    // rings, bound that)
+    h->sor_boff_sym.assign(h->ncol, 0);
+    h->sor_nblk_sym.assign(h->ncol, 0);
+    int cps_sym = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &cps_sym, k_sor_colour_tma<float, SLOTS_SYM, TMA_LPR_SYM, true>, tma_threads<TMA_LPR_SYM, TMA_ROWS_SYM>(),
+        tma_smem_bytes<float, SLOTS_SYM>()));
+    cps_sym = std::max(1, std::min(cps_sym, tma_ctas_per_sm<SLOTS_SYM, TMA_LPR_SYM, float>()));
+    int tots = 0;
+    for (int c = 0; c < h->ncol; ++c) {
+        h->sor_boff_sym[c] = tots;
+        h->sor_nblk_sym[c] = (int)std::min<long long>(
+            nblocks(h->col_start[c + 1] - h->col_start[c], tma_rows<SLOTS_SYM, float>()), (long long)h->nsm * cps_sym);
+        tots += h->sor_nblk_sym[c];
+    }
+    h->sor_nblk_tot_sym = std::max(tots, 1);
+    CKA(h->part_sor.alloc((size_t)2 *
+                          std::max(std::max(h->sor_nblk_tot, h->sor_nblk_tot32), h->sor_nblk_tot_sym)));
     if (FAS_SOR_RCP) CKA(h->rdiag.alloc((size_t)3 * nn));
     CKA(h->d_cstart.alloc(h->ncol + 1));
     CK(h->d_cstart.put(h->col_start.data(), h->ncol + 1, s));
@@ -731,6 +761,8 @@ int create_impl(fas_handle *h, const fas_mesh_desc *Md, const fas_matl_desc *T, 
                             cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem_bytes<double, SLOTS20>()));
     CK(cudaFuncSetAttribute(k_sor_colour_tma<float, SLOTS20, TMA_LPR81_32>,
                             cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem_bytes<float, SLOTS20>()));
+    CK(cudaFuncSetAttribute(k_sor_colour_tma<float, SLOTS_SYM, TMA_LPR_SYM, true>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem_bytes<float, SLOTS_SYM>()));
     CK(cudaFuncSetAttribute(k_sor_tiles<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             tile_smem_bytes<double>()));
     CK(cudaFuncSetAttribute(k_sor_tiles<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1219,10 +1251,72 @@ int ensure_fp32(fas_handle *h)
     return 0;
 }
 
+// Symmetric FP32 rows (FAS_MODE_SOR_SYM with FAS_MODE_SOR_FP32, 27-slot
+// rows), set up once per handle since the pattern is fixed: every
+// off-diagonal block pair of the pattern is given to one of its two rows,
+// in ascending node order, to the row that stores fewer blocks so far (13
+// per row on the interior of a brick mesh).  A pattern that needs more than
+// SLOTS_SYM - 1 stored blocks in some row, or is not symmetric, leaves the
+// FP32 sweeps on the full FP32 rows (sym_state -1).
+int ensure_sym(fas_handle *h)
+{
+    if (h->sym_state || !(h->mode & FAS_MODE_SOR_SYM) || !(h->mode & FAS_MODE_SOR_FP32) || h->slots != SLOTS ||
+        h->point_mode)
+        return 0;
+    cudaStream_t s = h->stream;
+    const int R = h->nnod;
+    std::vector<int> bc((size_t)CROW * R), rowof(R);
+    CK(cudaMemcpyAsync(bc.data(), h->bcol.p, bc.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(rowof.data(), h->rowof.p, (size_t)R * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    std::vector<int> cnt(R, 0);
+    std::vector<unsigned> mask(R, 0u);
+    bool ok = true;
+    for (int a = 0; a < R && ok; ++a) {
+        const int r = rowof[a];
+        const int *ca = &bc[(size_t)r * CROW];
+        for (int sl = 1; sl < ca[SLOTS] && ok; ++sl) {
+            const int m = ca[sl];
+            if (m <= a) continue;
+            if (cnt[m] < cnt[a]) {
+                const int *cm = &bc[(size_t)rowof[m] * CROW];
+                int s2 = -1;
+                for (int t = 1; t < cm[SLOTS]; ++t)
+                    if (cm[t] == a) s2 = t;
+                if (s2 < 0) ok = false;
+                else {
+                    mask[rowof[m]] |= 1u << s2;
+                    ++cnt[m];
+                }
+            } else {
+                mask[r] |= 1u << sl;
+                ++cnt[a];
+            }
+        }
+    }
+    for (int a = 0; a < R && ok; ++a) ok = cnt[a] <= SLOTS_SYM - 1;
+    if (!ok) {
+        h->sym_state = -1;
+        return 0;
+    }
+    CKA(h->sym_mask.alloc(R));
+    CKA(h->blk_sym.alloc((size_t)brow_of(SLOTS_SYM) * R));
+    CKA(h->bcol_sym.alloc((size_t)crow_of(SLOTS_SYM) * R));
+    CKA(h->sor_acc.alloc((size_t)4 * R));
+    CK(h->sym_mask.put(mask.data(), R, s));
+    CK(h->blk_sym.zero(s));
+    CK(h->bcol_sym.zero(s));
+    CK(h->sor_acc.zero(s));
+    CK(cudaStreamSynchronize(s));
+    h->sym_state = 1;
+    return 0;
+}
+
 int elvals_impl(fas_handle *h, int inc, int nit, bool bc)
 {
     cudaStream_t s = h->stream;
     if (int rc = ensure_fp32(h)) return rc;
+    if (int rc = ensure_sym(h)) return rc;
     CK(cudaMemsetAsync(h->ekey.p, 0xFF, sizeof(unsigned long long), s));
     CK(cudaMemsetAsync(h->flags.p, 0, sizeof(int), s));
     int rc;
@@ -1323,20 +1417,20 @@ void launch_colour_kernel(fas_handle *h, int c, bool pdl, const T *blk, const do
         const unsigned nt = tma_threads<LPR, tma_rows<SLOTS, T>()>();
         if (pdl)
             launch_pdl(k, nblk, nt, tma_smem_bytes<T, SLOTS>(), h->stream, blk, h->bcol.p, p0,
-                       p1, rhs, sol, base, rdiag, ctl, part, boff, ntot, sol32);
+                       p1, rhs, sol, base, rdiag, ctl, part, boff, ntot, sol32, (float *)nullptr);
         else
             k<<<nblk, nt, tma_smem_bytes<T, SLOTS>(), h->stream>>>(
-                blk, h->bcol.p, p0, p1, rhs, sol, base, rdiag, ctl, part, boff, ntot, sol32);
+                blk, h->bcol.p, p0, p1, rhs, sol, base, rdiag, ctl, part, boff, ntot, sol32, nullptr);
     } else {
         constexpr int LPR = tma_lpr<SLOTS20, T>();
         auto k = k_sor_colour_tma<T, SLOTS20, LPR>;
         const unsigned nt = tma_threads<LPR, tma_rows<SLOTS20, T>()>();
         if (pdl)
             launch_pdl(k, nblk, nt, tma_smem_bytes<T, SLOTS20>(), h->stream, blk, h->bcol.p, p0, p1,
-                       rhs, sol, base, rdiag, ctl, part, boff, ntot, sol32);
+                       rhs, sol, base, rdiag, ctl, part, boff, ntot, sol32, (float *)nullptr);
         else
             k<<<nblk, nt, tma_smem_bytes<T, SLOTS20>(), h->stream>>>(
-                blk, h->bcol.p, p0, p1, rhs, sol, base, rdiag, ctl, part, boff, ntot, sol32);
+                blk, h->bcol.p, p0, p1, rhs, sol, base, rdiag, ctl, part, boff, ntot, sol32, nullptr);
     }
 }
 
@@ -1351,11 +1445,26 @@ void launch_sor_small(fas_handle *h, const BlockDev &B, SorCtl *ctl, double tole
                                                        tolerl, 1000);
 }
 
+// One colour phase of the symmetric FP32 rows on the refinement's
+// (residual, correction), with the iterate as base.
+void launch_sym_colour(fas_handle *h, int c)
+{
+    const int p0 = h->col_start[c], p1 = h->col_start[c + 1];
+    if (p1 <= p0) return;
+    auto k = k_sor_colour_tma<float, SLOTS_SYM, TMA_LPR_SYM, true>;
+    launch_pdl(k, h->sor_nblk_sym[c], tma_threads<TMA_LPR_SYM, TMA_ROWS_SYM>(), tma_smem_bytes<float, SLOTS_SYM>(),
+               h->stream, (const float *)h->blk_sym.p, (const int *)h->bcol_sym.p, p0, p1, (const double *)h->sor_r.p,
+               h->sor_d.p, (const double *)h->ddx.p, (const double *)nullptr, h->sorctl.p, h->part_sor.p,
+               h->sor_boff_sym[c], h->sor_nblk_tot_sym, h->sor_d32.p, h->sor_acc.p);
+}
+
 // One colour phase: FP64 blocks on (rhs, sol), or the FP32 copy on the
 // refinement's (residual, correction) with the iterate as base.
 void launch_colour(fas_handle *h, int c, bool fp32)
 {
-    if (fp32)
+    if (fp32 && h->sym_on)
+        launch_sym_colour(h, c);
+    else if (fp32)
         launch_colour_kernel<float>(h, c, true, h->blk32.p, h->sor_r.p, h->sor_d.p, h->ddx.p, nullptr,
                                     h->sorctl.p, h->part_sor.p, h->sor_d32.p);
     else
@@ -1365,8 +1474,28 @@ void launch_colour(fas_handle *h, int c, bool fp32)
 
 void launch_check(fas_handle *h, double tolerl, bool fp32 = false)
 {
-    launch_pdl(k_sor_check, 1, 1024, 0, h->stream, h->part_sor.p, fp32 ? h->sor_nblk_tot32 : h->sor_nblk_tot,
-               h->sorctl.p, tolerl);
+    launch_pdl(k_sor_check, 1, 1024, 0, h->stream, h->part_sor.p,
+               fp32 ? (h->sym_on ? h->sor_nblk_tot_sym : h->sor_nblk_tot32) : h->sor_nblk_tot, h->sorctl.p, tolerl);
+}
+
+// End of one refinement cycle of the FP32 form: x += d, d = 0, the FP32
+// mirror and (symmetric rows) the accumulators cleared.
+void launch_fold(fas_handle *h)
+{
+    const long long nd3 = 3LL * h->nnod, nacc = h->sym_on ? 4LL * h->nnod : 0;
+    k_fold<<<nblocks(std::max(nd3, nacc), 256), 256, 0, h->stream>>>((int)nd3, h->ddx.p, h->sor_d.p, h->sor_d32.p,
+                                                                      h->sor_acc.p, (int)nacc);
+}
+
+// Start of an FP32 solve: whether its sweeps take the symmetric rows, and
+// if so their packing from the assembled FP64 rows and zero accumulators
+// (the correction starts at zero).
+void sym_begin(fas_handle *h, const BlockDev &B)
+{
+    h->sym_on = h->sym_state == 1 && (h->mode & FAS_MODE_SOR_SYM) && (h->mode & FAS_MODE_SOR_FP32);
+    if (!h->sym_on) return;
+    k_sym_pack<<<nblocks(32LL * h->nnod, 256), 256, 0, h->stream>>>(B, h->sym_mask.p, h->blk_sym.p, h->bcol_sym.p);
+    cudaMemsetAsync(h->sor_acc.p, 0, (size_t)4 * h->nnod * sizeof(float), h->stream);
 }
 
 void launch_plain_sweep(fas_handle *h, const BlockDev &B, double tolerl)
@@ -1402,13 +1531,16 @@ void launch_fp32_cycle(fas_handle *h, const BlockDev &B, double tolerl, int swee
         for (int c = 0; c < h->ncol; ++c) launch_colour(h, c, true);
         launch_check(h, tolerl, true);
     }
-    k_fold<<<nblocks((long long)nd3, 256), 256, 0, h->stream>>>((int)nd3, h->ddx.p, h->sor_d.p, h->sor_d32.p);
+    launch_fold(h);
     k_residual<<<rblk, 256, 0, h->stream>>>(B, h->rhs.p, h->ddx.p, h->sor_r.p, h->sorctl.p);
 }
 
 int ensure_fp32_graph(fas_handle *h, const BlockDev &B, double tolerl)
 {
-    if (h->sor32_graph) return 0;
+    if (h->sor32_graph && h->sor32_graph_sym == h->sym_on) return 0;
+    if (h->sor32_graph) cudaGraphExecDestroy(h->sor32_graph);
+    h->sor32_graph = nullptr;
+    h->sor32_graph_sym = h->sym_on;
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     launch_fp32_cycle(h, B, tolerl, h->refine_every);
@@ -1563,11 +1695,14 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
         if (rc) return rc;
         done = 1000;
     }
+    h->sym_on = false;
     if (fp32 && !tiles) {
         // x (= ddx) starts at 0, so the first residual is rhs itself
         CK(cudaMemcpyAsync(h->sor_r.p, h->rhs.p, nd3 * sizeof(double), cudaMemcpyDeviceToDevice, s));
         CK(cudaMemsetAsync(h->sor_d.p, 0, nd3 * sizeof(double), s));
         CK(cudaMemsetAsync(h->sor_d32.p, 0, nd3 * sizeof(float), s));
+        sym_begin(h, B);
+        CK(cudaGetLastError());
         const int m = h->refine_every;
         const unsigned rblk = (unsigned)std::min<long long>(nblocks(h->nnod, 8), (long long)h->nsm * 8);
         const bool graph32 = h->prof < 2 && ensure_fp32_graph(h, B, tolerl) == 0;
@@ -1594,7 +1729,7 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
                     LAUNCHED(h);
                 }
                 done += k;
-                k_fold<<<nblocks((long long)nd3, 256), 256, 0, s>>>((int)nd3, h->ddx.p, h->sor_d.p, h->sor_d32.p);
+                launch_fold(h);
                 LAUNCHED(h);
                 k_residual<<<rblk, 256, 0, s>>>(B, h->rhs.p, h->ddx.p, h->sor_r.p, h->sorctl.p);
                 LAUNCHED(h);
@@ -1640,6 +1775,8 @@ int facsls_impl(fas_handle *h, int *sweeps, double *error)
         bytes = 0.0;
         for (double b : h->col_bytes32) bytes += b;
     }
+    if (fp32 && h->sym_on)   // symmetric rows as streamed: values and column ids
+        bytes = (double)h->nnod * (brow_of(SLOTS_SYM) + crow_of(SLOTS_SYM)) * 4.0;
     h->P.sor_bytes += bytes * nsw;
     if (sweeps) *sweeps = nsw;
     if (error) *error = h->hc->sor.err;
@@ -1808,10 +1945,13 @@ int capture_nr_body(fas_handle *h, int inc, cudaGraphConditionalHandle hnr)
     // FP32 copy, each closed by the fold and the FP64 residual
     const bool fp32 = !small && (h->mode & FAS_MODE_SOR_FP32) && h->blk32.p;
     const int m = h->refine_every, full = (1000 / m) * m, rest = 1000 - full;
+    h->sym_on = false;
     if (fp32) {
         CK(cudaMemcpyAsync(h->sor_r.p, h->rhs.p, nd3 * sizeof(double), cudaMemcpyDeviceToDevice, s));
         CK(cudaMemsetAsync(h->sor_d.p, 0, nd3 * sizeof(double), s));
         CK(cudaMemsetAsync(h->sor_d32.p, 0, nd3 * sizeof(float), s));
+        sym_begin(h, B);
+        CK(cudaGetLastError());
     }
     cudaGraphConditionalHandle hsor, hlast = 0;
     if (int r = make_condition(s, 0, false, &hsor)) return r;
@@ -2180,6 +2320,9 @@ int32_t fas_gpu_set_mode(fas_handle *h, uint32_t mode)
     // increment graphs hold the launches of the old mode
     for (auto &g : h->inc_graphs) cudaGraphExecDestroy(g.second);
     h->inc_graphs.clear();
+    // and so does the FP32 cycle's graph (full or symmetric rows)
+    if (h->sor32_graph) cudaGraphExecDestroy(h->sor32_graph);
+    h->sor32_graph = nullptr;
     return 0;
 }
 

@@ -1185,6 +1185,24 @@ constexpr int TMA_ROWS81 = FAS_TMA_ROWS81;   // rows per chunk of 81-slot rows
 #endif
 constexpr int TMA_ROWS81_32 = FAS_TMA_ROWS81_32;   // rows per chunk of FP32 81-slot rows
 constexpr int TMA_LPR81_32 = FAS_TMA_LPR81_32;     // lanes per row of FP32 81-slot rows
+// Symmetric FP32 rows (FAS_MODE_SOR_SYM) of 8-node meshes: the stiffness
+// matrix is symmetric (K_mn = K_nm^T: symmetric element tangents, penalty
+// terms on diagonal blocks only), so each off-diagonal block is stored once,
+// in the row of one of its two nodes.  A row holds its diagonal block and at
+// most SLOTS_SYM - 1 stored blocks (13 on the interior of a brick mesh):
+// 576 bytes of FP32 values and column ids against 1,088 for full FP32 rows.
+constexpr int SLOTS_SYM = 14;
+#ifndef FAS_TMA_ROWS_SYM
+#define FAS_TMA_ROWS_SYM 16
+#endif
+#ifndef FAS_TMA_LPR_SYM
+#define FAS_TMA_LPR_SYM 8   // us per 64^3 sweep: 16 x 8 121.6, 16 x 4 125.3, 32 x 8 125.9, 32 x 4 126.3
+#endif
+constexpr int TMA_ROWS_SYM = FAS_TMA_ROWS_SYM;   // rows per chunk of symmetric rows
+constexpr int TMA_LPR_SYM = FAS_TMA_LPR_SYM;     // lanes per row of symmetric rows
+static_assert(TMA_ROWS_SYM * TMA_LPR_SYM % 32 == 0 && (TMA_LPR_SYM & (TMA_LPR_SYM - 1)) == 0 &&
+                  TMA_LPR_SYM <= 32,
+              "whole warps per CTA");
 constexpr int TMA_ROWS32 = FAS_TMA_ROWS32;   // rows per chunk of FP32 27-slot rows
 constexpr int TMA_LPR32 = FAS_TMA_LPR32;     // lanes per row of FP32 27-slot rows
 constexpr int TMA_MINB32 = FAS_TMA_MINB32;   // CTAs per SM the FP32 kernel's registers must allow
@@ -1199,12 +1217,16 @@ static_assert(TMA_THREADS % 32 == 0 && tma_threads<TMA_LPR81, TMA_ROWS81>() % 32
 // rows per chunk of the S-slot layout in value type T
 template <int S, typename T = double> __host__ __device__ constexpr int tma_rows()
 {
-    return S == SLOTS ? (sizeof(T) == 4 ? TMA_ROWS32 : TMA_ROWS) : (sizeof(T) == 4 ? TMA_ROWS81_32 : TMA_ROWS81);
+    return S == SLOTS_SYM ? TMA_ROWS_SYM
+           : S == SLOTS   ? (sizeof(T) == 4 ? TMA_ROWS32 : TMA_ROWS)
+                          : (sizeof(T) == 4 ? TMA_ROWS81_32 : TMA_ROWS81);
 }
 // lanes per row of the S-slot layout in value type T
 template <int S, typename T = double> __host__ __device__ constexpr int tma_lpr()
 {
-    return S == SLOTS ? (sizeof(T) == 4 ? TMA_LPR32 : TMA_LPR) : (sizeof(T) == 4 ? TMA_LPR81_32 : TMA_LPR81);
+    return S == SLOTS_SYM ? TMA_LPR_SYM
+           : S == SLOTS   ? (sizeof(T) == 4 ? TMA_LPR32 : TMA_LPR)
+                          : (sizeof(T) == 4 ? TMA_LPR81_32 : TMA_LPR81);
 }
 static_assert(tma_threads<TMA_LPR81_32, TMA_ROWS81_32>() % 32 == 0 && (TMA_LPR81_32 & (TMA_LPR81_32 - 1)) == 0 &&
                   TMA_LPR81_32 <= 32,
@@ -1250,9 +1272,11 @@ template <int SPL, typename XT = double> struct SorOps {
 // The FP32 sweeps' form: the slots' values from the FP32 mirror of the
 // correction (exactly the values the FP32 products round them to), and the
 // row node's own old values in FP64 for the point update.
+// Symmetric rows add the row node's accumulated transposed products (acc).
 template <int SPL> struct SorOps<SPL, float> {
     float x0[SPL], x1[SPL], x2[SPL];
     double r[6], own[3];
+    float acc[3];
 };
 
 __device__ __forceinline__ float ld_keep_f32(const float *ptr, uint64_t pol)
@@ -1261,14 +1285,25 @@ __device__ __forceinline__ float ld_keep_f32(const float *ptr, uint64_t pol)
     asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(ptr), "l"(pol));
     return v;
 }
+__device__ __forceinline__ float4 ld_keep_f32x4(const float *ptr, uint64_t pol)
+{
+    float4 v;
+    asm volatile("ld.global.cg.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "l"(ptr), "l"(pol));
+    return v;
+}
 
 // Gather of lane q of chunk row `row` from a landed stage's column ids.
 // r0 is the chunk's first row and nrow its row count.
-template <int S, int LPR, typename XT = double>
+// With SYM (symmetric rows) the row's first lane also reads the row node's
+// accumulated transposed products acc[4 n .. 4 n + 2].
+template <int S, int LPR, typename XT = double, bool SYM = false>
 __device__ __forceinline__ void sor_gather(const int *stage_cols, int r0, int nrow, int row, int q,
                                            const double *sol, const double *__restrict__ rhs,
                                            const double *__restrict__ rdiag, uint64_t keep_pol,
-                                           SorOps<(S + LPR - 1) / LPR, XT> &g, const float *sol32 = nullptr)
+                                           SorOps<(S + LPR - 1) / LPR, XT> &g, const float *sol32 = nullptr,
+                                           const float *acc = nullptr)
 {
     constexpr int SPL = (S + LPR - 1) / LPR, CR = crow_of(S);
     const bool live = row < nrow;
@@ -1295,6 +1330,14 @@ __device__ __forceinline__ void sor_gather(const int *stage_cols, int r0, int nr
         g.own[0] = own ? ld_keep(sol + 3 * n, keep_pol) : 0.0;
         g.own[1] = own ? ld_keep(sol + 3 * n + 1, keep_pol) : 0.0;
         g.own[2] = own ? ld_keep(sol + 3 * n + 2, keep_pol) : 0.0;
+        if constexpr (SYM) {
+            const float4 a = own ? ld_keep_f32x4(acc + 4 * (size_t)n, keep_pol) : make_float4(0.f, 0.f, 0.f, 0.f);
+            g.acc[0] = a.x;
+            g.acc[1] = a.y;
+            g.acc[2] = a.z;
+        }
+    } else {
+        static_assert(!SYM, "symmetric rows are FP32 rows with FP32 gathers");
     }
     g.r[0] = own ? ld_keep(rhs + 3 * n, keep_pol) : 0.0;
     g.r[1] = own ? ld_keep(rhs + 3 * n + 1, keep_pol) : 0.0;
@@ -1315,11 +1358,17 @@ __device__ __forceinline__ void sor_gather(const int *stage_cols, int r0, int nr
 // quotients come from the gathered reciprocal diagonal.
 // With FP32 gathers (XT = float) the row's own old values come from g.own,
 // and the new values also go, rounded, to the mirror sol32.
-template <typename T, int S, int LPR, int ROWS, typename XT = double>
+// With SYM (symmetric rows) the row's sum also takes the accumulated
+// transposed products g.acc, and after the point update every lane pushes,
+// for each stored block K_nm of its slots, K_nm^T (x32_new - x32_old) of
+// the row node n into acc[4 m ..] of the column node m (one vector atomic
+// add per block): acc[4 m ..] then always holds the products of the blocks
+// stored in other rows with the current FP32 correction.
+template <typename T, int S, int LPR, int ROWS, typename XT = double, bool SYM = false>
 __device__ __forceinline__ void sor_update(const unsigned char *stage, int nrow, int row, int q,
                                            const SorOps<(S + LPR - 1) / LPR, XT> &g, bool rcp,
                                            const double *__restrict__ base, double *sol, double &v0,
-                                           double &v1, float *sol32 = nullptr)
+                                           double &v1, float *sol32 = nullptr, float *acc = nullptr)
 {
     static_assert(sizeof(XT) == 8 || (sizeof(T) == 4 && FAS_SOR32_ARITH), "FP32 gathers feed FP32 products only");
     constexpr int SPL = (S + LPR - 1) / LPR, BR = brow_of(S), CR = crow_of(S);
@@ -1329,6 +1378,8 @@ __device__ __forceinline__ void sor_update(const unsigned char *stage, int nrow,
     const int *cols = reinterpret_cast<const int *>(stage + VB) + (live ? row : 0) * CR;
     const int ns = live ? cols[S] : 0;
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    // symmetric rows keep the lane's blocks in registers for the push
+    float kb[SYM ? SPL : 1][9];
     if constexpr (sizeof(T) == 4 && FAS_SOR32_ARITH) {
         // FP32 products and lane sums of the FP32 blocks with the rounded
         // correction; the lanes' sums join in FP64
@@ -1336,7 +1387,14 @@ __device__ __forceinline__ void sor_update(const unsigned char *stage, int nrow,
 #pragma unroll
         for (int j = 0; j < SPL; ++j) {
             const int sl = q + LPR * j;
-            if (sl >= 1 && sl < ns) {
+            if constexpr (SYM) {
+#pragma unroll
+                for (int qq = 0; qq < 9; ++qq) kb[j][qq] = (sl >= 1 && sl < ns) ? vals[sl + qq * S] : 0.f;
+                const float y0 = g.x0[j], y1 = g.x1[j], y2 = g.x2[j];
+                f0 += kb[j][0] * y0 + kb[j][1] * y1 + kb[j][2] * y2;
+                f1 += kb[j][3] * y0 + kb[j][4] * y1 + kb[j][5] * y2;
+                f2 += kb[j][6] * y0 + kb[j][7] * y1 + kb[j][8] * y2;
+            } else if (sl >= 1 && sl < ns) {
                 const T *b = vals + sl;
                 const float y0 = (float)g.x0[j], y1 = (float)g.x1[j], y2 = (float)g.x2[j];
                 f0 += b[0 * S] * y0 + b[1 * S] * y1 + b[2 * S] * y2;
@@ -1365,8 +1423,14 @@ __device__ __forceinline__ void sor_update(const unsigned char *stage, int nrow,
         a1 += __shfl_xor_sync(0xffffffffu, a1, o);
         a2 += __shfl_xor_sync(0xffffffffu, a2, o);
     }
+    float e0 = 0.f, e1 = 0.f, e2 = 0.f;   // the FP32 change of the row node (SYM)
     if (live && q == 0) {
         const int n = cols[0];
+        if constexpr (SYM) {
+            a0 += (double)g.acc[0];
+            a1 += (double)g.acc[1];
+            a2 += (double)g.acc[2];
+        }
         double D[9];
 #pragma unroll
         for (int qq = 0; qq < 9; ++qq) D[qq] = (double)vals[qq * S];
@@ -1415,6 +1479,11 @@ __device__ __forceinline__ void sor_update(const unsigned char *stage, int nrow,
             sol32[3 * n] = (float)x0;
             sol32[3 * n + 1] = (float)x1;
             sol32[3 * n + 2] = (float)x2;
+            if constexpr (SYM) {   // the mirror held (float) of the old value
+                e0 = (float)x0 - (float)o0;
+                e1 = (float)x1 - (float)o1;
+                e2 = (float)x2 - (float)o2;
+            }
         }
         v0 += (x0 - o0) * (x0 - o0) + (x1 - o1) * (x1 - o1) + (x2 - o2) * (x2 - o2);
         if (base) {
@@ -1423,6 +1492,25 @@ __device__ __forceinline__ void sor_update(const unsigned char *stage, int nrow,
             x2 += base[3 * n + 2];
         }
         v1 += x0 * x0 + x1 * x1 + x2 * x2;
+    }
+    if constexpr (SYM) {
+        const int lead = (int)(threadIdx.x & 31u) & ~(LPR - 1);
+        e0 = __shfl_sync(0xffffffffu, e0, lead);
+        e1 = __shfl_sync(0xffffffffu, e1, lead);
+        e2 = __shfl_sync(0xffffffffu, e2, lead);
+        if (e0 != 0.f || e1 != 0.f || e2 != 0.f) {
+#pragma unroll
+            for (int j = 0; j < SPL; ++j) {
+                const int sl = q + LPR * j;
+                if (sl >= 1 && sl < ns) {
+                    const float *b = kb[j];
+                    const float t0 = b[0] * e0 + b[3] * e1 + b[6] * e2;
+                    const float t1 = b[1] * e0 + b[4] * e1 + b[7] * e2;
+                    const float t2 = b[2] * e0 + b[5] * e1 + b[8] * e2;
+                    atomicAdd(reinterpret_cast<float4 *>(acc + 4 * (size_t)cols[sl]), make_float4(t0, t1, t2, 0.f));
+                }
+            }
+        }
     }
 }
 
@@ -1440,15 +1528,22 @@ __device__ __forceinline__ void sor_update(const unsigned char *stage, int nrow,
 // computed: one L2 round trip per chunk is hidden.  Every mbarrier
 // wait is bounded; on a timeout the CTA waits (bounded) for its own copies
 // still in flight, raises ctl->fault and leaves.
-template <typename T, int S, int LPR>
+//
+// With SYM the rows are symmetric FP32 rows (SLOTS_SYM slots: the diagonal
+// and the blocks stored in this row) and acc holds, per node, the products
+// of the blocks stored in other rows with the current FP32 correction
+// (sor_update).  The rows of a colour push only into nodes of other
+// colours, so no row of a phase reads an accumulator the phase writes.
+template <typename T, int S, int LPR, bool SYM = false>
 __global__ void __launch_bounds__(tma_rows<S, T>() * LPR, tma_minb<S, T>()) k_sor_colour_tma(const T *__restrict__ blk,
                                                                 const int *__restrict__ bcol, int p0, int p1,
                                                                 const double *__restrict__ rhs, double *sol,
                                                                 const double *__restrict__ base,
                                                                 const double *__restrict__ rdiag, SorCtl *ctl,
                                                                 double *part, int boff, int nblk_tot,
-                                                                float *sol32)
+                                                                float *sol32, float *acc)
 {
+    static_assert(!SYM || (S == SLOTS_SYM && sizeof(T) == 4 && FAS_SOR32_ARITH), "symmetric rows: FP32 products");
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int s_pre, s_post;
     constexpr int BR = brow_of(S), CR = crow_of(S);
@@ -1509,8 +1604,8 @@ __global__ void __launch_bounds__(tma_rows<S, T>() * LPR, tma_minb<S, T>()) k_so
     SorOps<SPL, XT> g[TMA_PD + 1] = {};
     auto gather = [&](int kk, SorOps<SPL, XT> &o) {
         const int r0 = p0 + (blockIdx.x + kk * gridDim.x) * ROWS;
-        sor_gather<S, LPR, XT>(reinterpret_cast<const int *>(smem + (kk % TMA_STAGES) * SB + VB), r0,
-                               min(ROWS, p1 - r0), row, q, sol, rhs, rdiag, keep_pol, o, sol32);
+        sor_gather<S, LPR, XT, SYM>(reinterpret_cast<const int *>(smem + (kk % TMA_STAGES) * SB + VB), r0,
+                                    min(ROWS, p1 - r0), row, q, sol, rhs, rdiag, keep_pol, o, sol32, acc);
     };
     // chunks [0, waited) have landed; chunks [0, min(myn, k + TMA_STAGES))
     // have been issued when iteration k starts
@@ -1540,8 +1635,8 @@ __global__ void __launch_bounds__(tma_rows<S, T>() * LPR, tma_minb<S, T>()) k_so
         }
         const int st = k % TMA_STAGES;
         const int nrow = min(ROWS, p1 - (p0 + (int)(blockIdx.x + k * gridDim.x) * ROWS));
-        sor_update<T, S, LPR, ROWS, XT>(smem + st * SB, nrow, row, q, g[0], rdiag != nullptr, base, sol, v0, v1,
-                                        sol32);
+        sor_update<T, S, LPR, ROWS, XT, SYM>(smem + st * SB, nrow, row, q, g[0], rdiag != nullptr, base, sol, v0,
+                                             v1, sol32, acc);
         __syncthreads();   // every row of this stage is done
         if (threadIdx.x == 0 && k + TMA_STAGES < myn) {
             fence_proxy_async();
@@ -1653,14 +1748,44 @@ __global__ void __launch_bounds__(256) k_residual(BlockDev B, const double *__re
     }
 }
 
-// x += d, d = 0 and its FP32 mirror d32 = 0 (end of one refinement step).
-__global__ void k_fold(int ndof, double *x, double *d, float *d32)
+// x += d, d = 0 and its FP32 mirror d32 = 0 (end of one refinement step);
+// with symmetric rows also the nacc accumulator entries (the products of a
+// zero correction).
+__global__ void k_fold(int ndof, double *x, double *d, float *d32, float *acc = nullptr, int nacc = 0)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nacc) acc[i] = 0.f;
     if (i >= ndof) return;
     x[i] += d[i];
     d[i] = 0.0;
     if (d32) d32[i] = 0.f;
+}
+
+// Symmetric FP32 rows from the assembled FP64 rows (27-slot layout), one
+// warp per row, lane s on slot s: the diagonal block and the slots whose bit
+// is set in mask[row] (the blocks this row stores) are rounded to FP32 and
+// packed, in slot order, into a SLOTS_SYM-slot row with its column ids and
+// slot count.
+__global__ void k_sym_pack(BlockDev B, const unsigned *__restrict__ mask, float *__restrict__ bs,
+                           int *__restrict__ cs)
+{
+    constexpr int BRS = brow_of(SLOTS_SYM), CRS = crow_of(SLOTS_SYM);
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= B.R) return;
+    const int r = (int)w;
+    const int *cols = B.bcol + B.si(r, 0);
+    const int ns = cols[SLOTS];
+    const bool keep = lane < ns && (lane == 0 || ((mask[r] >> lane) & 1u));
+    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+    const int pos = __popc(bal & ((1u << lane) - 1u));
+    if (keep && pos < SLOTS_SYM) {
+#pragma unroll
+        for (int qq = 0; qq < 9; ++qq)
+            bs[(size_t)r * BRS + qq * SLOTS_SYM + pos] = (float)B.blk[B.bi(r, lane, qq)];
+        cs[(size_t)r * CRS + pos] = cols[lane];
+    }
+    if (lane == 0) cs[(size_t)r * CRS + SLOTS_SYM] = min(__popc(bal), SLOTS_SYM);
 }
 
 // End of one sweep: error = sum(dx^2) / sum(x^2) (Stif_sol.f90:206-210).

@@ -106,6 +106,22 @@ extern "C" {
                                      runs.  The graph of an increment is
                                      built on its first call and kept until
                                      the mode changes                       */
+#define FAS_MODE_SOR_SYM    256u  /* with FAS_MODE_SOR_FP32 on 8-node meshes:
+                                     the FP32 sweeps stream each off-diagonal
+                                     block once (K_mn = K_nm^T), from the
+                                     row of one of its two nodes, and push
+                                     its transposed product with each change
+                                     of that node into a per-node FP32
+                                     accumulator of the other (vector atomic
+                                     adds): 576 instead of 1,088 bytes per
+                                     row.  The same iteration as
+                                     FAS_MODE_SOR_FP32 to FP32 rounding, but
+                                     the order of the atomic adds varies, so
+                                     results are not bit-reproducible from
+                                     run to run.  No effect on 20-node or
+                                     quadratic meshes, nor on a pattern
+                                     whose rows would store more than 13
+                                     blocks                                 */
 
 /*
  * Mesh: the FAS_COM element and node tables.
