@@ -629,7 +629,7 @@ def rooflines(g, start, prob) -> dict:
     out = {}
     kernels = {"sor": "k_sor_colour_tma<double,27,4>", "sor_fp32": "k_sor_colour_tma<float,27,4>",
                "sor_tiles": "k_sor_tiles<double>", "sor_fp32_tiles": "k_sor_tiles<float>",
-               "sor_fp32_sym": "k_sor_colour_tma<float,14,8,true>"}
+               "sor_fp32_sym": "k_sor_colour_tma<float,15,8,true>"}
     for tag, mode in (("sor", abi.FAS_MODE_PLAIN), ("sor_fp32", abi.FAS_MODE_SOR_FP32),
                       ("sor_tiles", abi.FAS_MODE_SOR_TILES),
                       ("sor_fp32_tiles", abi.FAS_MODE_SOR_FP32 | abi.FAS_MODE_SOR_TILES),

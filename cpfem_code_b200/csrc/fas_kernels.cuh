@@ -1190,8 +1190,11 @@ constexpr int TMA_LPR81_32 = FAS_TMA_LPR81_32;     // lanes per row of FP32 81-s
 // terms on diagonal blocks only), so each off-diagonal block is stored once,
 // in the row of one of its two nodes.  A row holds its diagonal block and at
 // most SLOTS_SYM - 1 stored blocks (13 on the interior of a brick mesh):
-// 576 bytes of FP32 values and column ids against 1,088 for full FP32 rows.
-constexpr int SLOTS_SYM = 14;
+// 608 bytes of FP32 values and column ids against 1,088 for full FP32 rows.
+// 15 slots make a row 136 values long, 8 banks apart in shared memory, so
+// the four rows a warp serves with 8 lanes each read without bank conflicts
+// (14 slots, 128 values, put all four rows on the same banks).
+constexpr int SLOTS_SYM = 15;
 #ifndef FAS_TMA_ROWS_SYM
 #define FAS_TMA_ROWS_SYM 16
 #endif

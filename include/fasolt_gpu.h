@@ -113,14 +113,14 @@ extern "C" {
                                      its transposed product with each change
                                      of that node into a per-node FP32
                                      accumulator of the other (vector atomic
-                                     adds): 576 instead of 1,088 bytes per
+                                     adds): 608 instead of 1,088 bytes per
                                      row.  The same iteration as
                                      FAS_MODE_SOR_FP32 to FP32 rounding, but
                                      the order of the atomic adds varies, so
                                      results are not bit-reproducible from
                                      run to run.  No effect on 20-node or
                                      quadratic meshes, nor on a pattern
-                                     whose rows would store more than 13
+                                     whose rows would store more than 14
                                      blocks                                 */
 
 /*

@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 
 FP32 = abi.FAS_MODE_SOR_GRID | abi.FAS_MODE_SOR_FP32
 SYM = FP32 | abi.FAS_MODE_SOR_SYM
-SYM_ROW_BYTES = (128 + 16) * 4      # brow_of(14) FP32 values + crow_of(14) column ids
+SYM_ROW_BYTES = (136 + 16) * 4      # brow_of(15) FP32 values + crow_of(15) column ids
 
 
 def _assembled(p, mode):
@@ -40,7 +40,7 @@ def _bytes_per_sweep(g):
 def test_sym_facsls_matches_full_fp32_rows(n):
     """One FACSLS of the first Newton iteration: the symmetric rows' solution
     equals the full FP32 rows' to FP32-sweep rounding, with the same sweep
-    count to within two, and the sweeps stream 576 bytes per row."""
+    count to within two, and the sweeps stream 608 bytes per row."""
     p = generator.structured_cube(n=n, ninc=1, seed=3)
     a, b = _assembled(p, FP32), _assembled(p, SYM)
     try:
