@@ -833,6 +833,23 @@ def run_gpu_points(args, ws, rank, local, dist, dev):
     torch.cuda.synchronize()
     e2e = time.perf_counter() - t0
     te, work_e = reduce_max_sum(dist, e2e, float(prob.ngps * args.steps), dev)
+    # the batched persistent kernel on the same points: a grid of the CTAs
+    # that reside at once, every warp taking the next 32 points of the
+    # work-sorted order from a device queue (FAS_MODE_CP_QUEUE)
+    from cpfem_code_b200 import abi
+    g.set_mode(abi.FAS_MODE_CP_QUEUE)
+    for _ in range(args.warmup):
+        g.upload(start)
+        g.constitutive(1, 1)
+    qms = 0.0
+    for _ in range(args.steps):
+        g.upload(start)
+        g.profile(2)
+        g.constitutive(1, 1)
+        qms += g.profile(0)["ms_constitutive"]
+    qprob = start.copy()
+    g.download(qprob)
+    g.set_mode(abi.FAS_MODE_PLAIN)
     if rank == 0:
         fp = fp64_peak_tflops()
         ach = ops / (ms / 1e3 / args.steps) / 1e12
@@ -852,6 +869,12 @@ def run_gpu_points(args, ws, rank, local, dist, dev):
             "clocks": clk,
             "e2e": {"value": work_e / te, "unit": "GP-updates/s",
                     "h2d_bytes_per_step": moved_bytes(prob, 12), "d2h_bytes_per_step": moved_bytes(prob, 12)},
+            "persistent": {"value": prob.ngps * args.steps / (qms / 1e3), "unit": "GP-updates/s",
+                           "ms_per_pass": qms / args.steps, "plain_ms_per_pass": ms / args.steps,
+                           "same_result_as_plain": bool(np.array_equal(qprob.ds, prob.ds)
+                                                        and np.array_equal(qprob.dsv, prob.dsv)),
+                           "mode": "batched persistent kernel: resident CTAs only, warps take the next 32 "
+                                   "points of the work-sorted order from a device queue"},
         }
         if ws == 1 and not args.no_cpu:
             secs, pc = cpu_points(start, os.cpu_count() or 1)
