@@ -313,3 +313,36 @@ def test_20_node_brick_increment_matches_8_node():
         out[nodes] = p.st[:, 0].mean()
         assert np.isfinite(p.st).all()
     assert out[20] == pytest.approx(out[8], rel=2e-3)
+
+
+@pytest.mark.parametrize("nodes,inc_steps", [(8, 1), (20, 1), (8, 3)])
+def test_assembled_stiffness_is_symmetric(nodes, inc_steps):
+    """The checker's assembled stiffness (ELVALS + SUVALS) is symmetric:
+    K_ij = K_ji to rounding on the rows of free DOFs, and exactly where the
+    penalty terms sit (they touch diagonal entries only).  This holds in the
+    elastic first iteration and after plastic increments (the tangent chi
+    is symmetric), and is the property the device's symmetric FP32 rows
+    (FAS_MODE_SOR_SYM) rely on when they store each off-diagonal block once."""
+    from oracle import OracleSolver
+    p = generator.structured_cube(n=(4, 3, 3) if nodes == 8 else (2, 2, 2), ninc=inc_steps, seed=3,
+                                  nodes=nodes)
+    o = OracleSolver(p, 8, threads=4)
+    for inc in range(1, inc_steps):
+        o.increment(inc)
+    o.update_node()
+    o.elvals(inc_steps, 1)
+    o.suvals(inc_steps)
+    ld = 96 if nodes == 8 else 256       # columns per DOF row: 27 or 81 nodes x 3
+    IS, SS = o.pattern(ld), o.stiffness(ld)
+    n = 3 * p.nnod
+    K = np.zeros((n, n))
+    for r in range(n):
+        K[r, r] = SS[r, 0]
+        for k in range(1, IS[r, 0] + 1):
+            K[r, IS[r, k] - 1] = SS[r, k]
+    pen = np.diag(K) > 1e15
+    assert pen.any() and (~pen).any()
+    free = K[np.ix_(~pen, ~pen)]
+    assert np.abs(free - free.T).max() <= 1e-14 * np.abs(free).max()
+    off = K - np.diag(np.diag(K))
+    assert np.abs(off - off.T).max() <= 1e-14 * np.abs(free).max()
